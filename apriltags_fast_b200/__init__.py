@@ -1,0 +1,304 @@
+"""apriltags-b200: Python mirror of the AprilTag detector's C API.
+
+The detector itself is libapriltag_b200.so (sm_100a CUDA kernels behind the
+C ABI of include/apriltag_fast.h); this module binds it with ctypes and
+mirrors the reference's native API (fast/apriltag_fast.h:99-141):
+
+    det = Detector()                  # at_detector_create
+    det.add_family("tag36h11", 2)     # at_add_family(td, at_tag36h11(), 2)
+    dets = det.detect(image)          # at_detect; list of Detection
+    det.nquads                        # td->nquads
+
+There is no CPU path: loading fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libapriltag_b200.so")
+
+
+class Family(C.Structure):
+    """at_family (fast/apriltag_fast.h:24-36)."""
+
+    _fields_ = [
+        ("name", C.c_char * 32),
+        ("codes", C.POINTER(C.c_uint64)),
+        ("ncodes", C.c_int64),
+        ("nbits", C.c_int32),
+        ("h", C.c_int32),
+        ("width_at_border", C.c_int32),
+        ("total_width", C.c_int32),
+        ("reversed_border", C.c_bool),
+        ("bit_x", C.c_int32 * 64),
+        ("bit_y", C.c_int32 * 64),
+    ]
+
+
+class QuadThreshParams(C.Structure):
+    _fields_ = [
+        ("min_cluster_pixels", C.c_int32),
+        ("max_nmaxima", C.c_int32),
+        ("critical_rad", C.c_float),
+        ("cos_critical_rad", C.c_float),
+        ("max_line_fit_mse", C.c_float),
+        ("min_white_black_diff", C.c_int32),
+        ("deglitch", C.c_bool),
+    ]
+
+
+class CDetection(C.Structure):
+    """at_detection (fast/apriltag_fast.h:52-64), 168 bytes."""
+
+    _fields_ = [
+        ("family", C.c_int32),
+        ("id", C.c_int32),
+        ("hamming", C.c_int32),
+        ("decision_margin", C.c_float),
+        ("H", C.c_double * 9),
+        ("c", C.c_double * 2),
+        ("p", (C.c_double * 2) * 4),
+    ]
+
+
+class Timing(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("decimate", "blur", "threshold", "unionfind", "clusters", "fit_quads", "decode", "reconcile",
+                 "total")]
+
+
+class CDetector(C.Structure):
+    """at_detector (fast/apriltag_fast.h:73-96), 160 bytes."""
+
+    _fields_ = [
+        ("nthreads", C.c_int32),
+        ("quad_decimate", C.c_float),
+        ("quad_sigma", C.c_float),
+        ("refine_edges", C.c_bool),
+        ("decode_sharpening", C.c_double),
+        ("debug", C.c_bool),
+        ("qtp", QuadThreshParams),
+        ("detections", C.POINTER(CDetection)),
+        ("ndetections", C.c_int64),
+        ("nquads", C.c_int64),
+        ("timing", Timing),
+        ("internal", C.c_void_p),
+    ]
+
+
+class Frame(C.Structure):
+    _fields_ = [("pixels", C.c_void_p), ("width", C.c_int64), ("height", C.c_int64), ("stride", C.c_int64),
+                ("family_mask", C.c_uint32)]
+
+
+class FrameResult(C.Structure):
+    _fields_ = [("first", C.c_int64), ("count", C.c_int64), ("nquads", C.c_int64)]
+
+
+DIAG = {"quad_image": 0, "threshold": 1, "labels": 2, "points": 3, "clusters": 4, "quads": 5, "sizes": 6}
+QUAD_DTYPE = np.dtype([("p", np.float32, (4, 2)), ("reversed_border", np.int32), ("frame", np.int32)])
+
+FAMILY_NAMES = ("tag16h5", "tag25h9", "tag36h10", "tag36h11", "tagCircle21h7", "tagCircle49h12",
+                "tagCustom48h12", "tagStandard41h12", "tagStandard52h13")
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m apriltags_fast_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.at_detector_create.restype = C.POINTER(CDetector)
+        L.at_detector_destroy.argtypes = [C.POINTER(CDetector)]
+        L.at_add_family.argtypes = [C.POINTER(CDetector), C.POINTER(Family), C.c_int]
+        L.at_add_family.restype = C.c_bool
+        L.at_clear_families.argtypes = [C.POINTER(CDetector)]
+        L.at_family_name.argtypes = [C.POINTER(CDetector), C.POINTER(CDetection)]
+        L.at_family_name.restype = C.c_char_p
+        L.at_detect.argtypes = [C.POINTER(CDetector), C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
+        L.at_detect_batch.argtypes = [C.POINTER(CDetector), C.POINTER(Frame), C.c_int64, C.POINTER(FrameResult)]
+        L.at_shutdown.argtypes = [C.POINTER(CDetector)]
+        L.at_detector_last_error.argtypes = [C.POINTER(CDetector), C.POINTER(C.c_char_p)]
+        L.at_detector_last_error.restype = C.c_int
+        L.at_detector_diag.argtypes = [C.POINTER(CDetector), C.c_int, C.c_void_p, C.c_int64]
+        L.at_detector_diag.restype = C.c_int64
+        L.at_family_by_name.argtypes = [C.c_char_p]
+        L.at_family_by_name.restype = C.POINTER(Family)
+        for n in FAMILY_NAMES:
+            getattr(L, "at_" + n).restype = C.POINTER(Family)
+        _lib = L
+    return _lib
+
+
+def family(name: str) -> Family:
+    """A built-in family (at_family_by_name); KeyError if unknown."""
+    p = lib().at_family_by_name(name.encode())
+    if not p:
+        raise KeyError(f"no built-in family {name!r} (was the library built with the family tables?)")
+    return p.contents
+
+
+def family_codes(name: str) -> np.ndarray:
+    f = family(name)
+    return np.ctypeslib.as_array(f.codes, shape=(f.ncodes,)).copy()
+
+
+@dataclass
+class Detection:
+    family: int
+    id: int
+    hamming: int
+    decision_margin: float
+    H: tuple
+    c: tuple
+    p: tuple
+
+    def key(self) -> tuple:
+        return (self.family, self.id, self.hamming, self.decision_margin, self.H, self.c, self.p)
+
+
+def _detection(d: CDetection) -> Detection:
+    return Detection(int(d.family), int(d.id), int(d.hamming), float(d.decision_margin), tuple(d.H), tuple(d.c),
+                     tuple(tuple(r) for r in d.p))
+
+
+class Detector:
+    """Mirror of at_detector: the same parameters, the same defaults."""
+
+    def __init__(self, families=(), bits_corrected: int = 2, **params):
+        self._L = lib()
+        self._td = self._L.at_detector_create()
+        self._fams = []
+        for f in families:
+            self.add_family(f, bits_corrected)
+        for k, v in params.items():
+            self.set(k, v)
+
+    def set(self, name, value):
+        td = self._td.contents
+        if hasattr(td.qtp, name) and name not in ("detections",):
+            setattr(td.qtp, name, value)
+        elif name in ("nthreads", "quad_decimate", "quad_sigma", "refine_edges", "decode_sharpening", "debug"):
+            setattr(td, name, value)
+        else:
+            raise AttributeError(name)
+
+    @property
+    def params(self) -> CDetector:
+        return self._td.contents
+
+    def add_family(self, fam, bits_corrected: int = 2) -> bool:
+        f = family(fam) if isinstance(fam, str) else fam
+        ok = bool(self._L.at_add_family(self._td, C.byref(f), bits_corrected))
+        if ok:
+            self._fams.append(f)
+        return ok
+
+    def clear_families(self):
+        self._L.at_clear_families(self._td)
+        self._fams = []
+
+    def detect(self, img, stride: int | None = None) -> list[Detection]:
+        """Detect on a u8 image: a 2-D numpy array (host) or a uint8 CUDA
+        torch tensor (device memory, read in place)."""
+        ptr, w, h, s = _image_arg(img, stride)
+        self._L.at_detect(self._td, ptr, w, h, s)
+        self._check()
+        td = self._td.contents
+        return [_detection(td.detections[i]) for i in range(td.ndetections)]
+
+    def detect_batch(self, images, family_masks=None) -> list[list[Detection]]:
+        n = len(images)
+        frames = (Frame * max(n, 1))()
+        keep = []
+        for i, img in enumerate(images):
+            ptr, w, h, s = _image_arg(img, None)
+            keep.append(img)
+            frames[i] = Frame(ptr, w, h, s, 0 if family_masks is None else family_masks[i])
+        res = (FrameResult * max(n, 1))()
+        self._L.at_detect_batch(self._td, frames, n, res)
+        self._check()
+        td = self._td.contents
+        out = []
+        for i in range(n):
+            out.append([_detection(td.detections[res[i].first + k]) for k in range(res[i].count)])
+        self.last_batch_nquads = [int(res[i].nquads) for i in range(n)]
+        return out
+
+    def _check(self):
+        msg = C.c_char_p()
+        code = self._L.at_detector_last_error(self._td, C.byref(msg))
+        if code:
+            raise RuntimeError(f"apriltag_b200 error {code}: {msg.value.decode() if msg.value else ''}")
+
+    @property
+    def nquads(self) -> int:
+        return int(self._td.contents.nquads)
+
+    @property
+    def timing(self) -> dict:
+        t = self._td.contents.timing
+        return {n: getattr(t, n) for n, _ in Timing._fields_}
+
+    def diag(self, what: str) -> np.ndarray:
+        """An intermediate array of the last detection (frame 0), for
+        stage-by-stage checks: quad_image, threshold, labels, points,
+        clusters, quads or sizes."""
+        code = DIAG[what]
+        sizes = np.zeros(5, np.int64)
+        self._L.at_detector_diag(self._td, DIAG["sizes"], sizes.ctypes.data, 40)
+        if what == "sizes":
+            return sizes
+        nbytes = self._L.at_detector_diag(self._td, code, None, 0)
+        buf = np.zeros(max(int(nbytes), 0), np.uint8)
+        if nbytes > 0:
+            self._L.at_detector_diag(self._td, code, buf.ctypes.data, nbytes)
+        qw, qh = int(sizes[0]), int(sizes[1])
+        if what in ("quad_image", "threshold"):
+            return buf.reshape(qh, qw)
+        if what == "labels":
+            return buf.view(np.uint32).reshape(qh, qw)
+        if what == "points":
+            return buf.view(np.uint64)
+        if what == "clusters":
+            return buf.view(np.uint32)
+        return buf.view(QUAD_DTYPE)
+
+    def family_name(self, d: Detection) -> str:
+        return self._fams[d.family].name.decode()
+
+    def shutdown(self):
+        self._L.at_shutdown(self._td)
+
+    def close(self):
+        if getattr(self, "_td", None):
+            self._L.at_detector_destroy(self._td)
+            self._td = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _image_arg(img, stride):
+    if hasattr(img, "data_ptr") and getattr(img, "is_cuda", False):
+        assert img.dtype.__str__() == "torch.uint8" and img.dim() == 2
+        h, w = img.shape
+        return C.c_void_p(img.data_ptr()), w, h, int(img.stride(0))
+    a = np.asarray(img)
+    if a.dtype != np.uint8 or a.ndim != 2:
+        raise TypeError("image must be a 2-D uint8 array")
+    if not a.flags["C_CONTIGUOUS"] and a.strides[1] != 1:
+        a = np.ascontiguousarray(a)
+    h, w = a.shape
+    return C.c_void_p(a.ctypes.data), w, h, int(stride or a.strides[0])

@@ -1,0 +1,76 @@
+"""Build libapriltag_b200.so in-tree with nvcc for sm_100a.
+
+    python -m apriltags_fast_b200.build [--reference DIR]
+
+The tag family tables are extracted at build time from the AprilTag family
+files of the reference checkout (default: $APRILTAG_REFERENCE, else
+/root/reference) into _build/ (not committed). Without them the library
+still builds, and the at_tag*() accessors return NULL.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libapriltag_b200.so")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# every floating point operation rounded on its own, as the reference
+# (built with -ffp-contract=off) rounds it
+FP = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
+CUFLAGS = ARCH + FP + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+                       "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+SOURCES = ["at_kernels.cu", "at_detector.cu"]
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(reference: str | None = None, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    reference = reference or os.environ.get("APRILTAG_REFERENCE", "/root/reference")
+    headers = [os.path.join(CSRC, h) for h in ("at_gpu.h", "at_kernels.h")] + [
+        os.path.join(ROOT, "include", "apriltag_fast.h")]
+    objs = []
+    fam_c = os.path.join(BUILD, "at_families_data.c")
+    if os.path.isdir(reference) and os.path.exists(os.path.join(reference, "tag36h11.c")):
+        if force or not os.path.exists(fam_c):
+            _run([sys.executable, os.path.join(CSRC, "gen_families.py"), reference, fam_c])
+    if os.path.exists(fam_c):
+        fam_o = os.path.join(BUILD, "at_families_data.o")
+        if force or _newer(fam_o, [fam_c]):
+            _run(["gcc", "-O1", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c", fam_c, "-o", fam_o])
+        objs.append(fam_o)
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        if force or _newer(o, [s] + headers):
+            _run([NVCC] + CUFLAGS + ["-c", s, "-o", o])
+        objs.append(o)
+    if force or _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=None)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(a.reference, a.force))

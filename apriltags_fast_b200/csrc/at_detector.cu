@@ -1,0 +1,804 @@
+// The detector object and the C ABI (include/apriltag_fast.h).
+//
+// Host code only orchestrates: it sizes the device arenas, copies frames in,
+// launches the stage kernels (at_kernels.cu) on the detector's stream and
+// copies the detections out. Every computation of the detection path runs on
+// the GPU. Compiled with -ffp-contract=off for the few host-side constants
+// (blur taps, the low-pass taps, rotation cos/sin) that the reference takes
+// from libm.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cub/cub.cuh>
+#include <string>
+#include <vector>
+
+#include "apriltag_fast.h"
+#include "at_gpu.h"
+#include "at_kernels.h"
+
+static_assert(sizeof(at_detection) == 168, "at_detection layout");
+static_assert(sizeof(GpuDetection) == sizeof(at_detection), "detection layout");
+static_assert(sizeof(at_detector) == 160, "at_detector layout");
+static_assert(sizeof(at_family) == 584, "at_family layout");
+
+// Tables of the built-in families, generated at build time (gen_families.py);
+// a build without them links this empty list.
+extern "C" {
+extern const at_family *const at_builtin_families[] __attribute__((weak));
+}
+
+namespace {
+
+// A device buffer that only grows. Growing frees the old one (cudaFree
+// synchronises the device first).
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 4 + 4096;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Pinned host staging that only grows.
+struct HBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 4 + 4096;
+        cudaError_t e = cudaMallocHost(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+enum {
+    B_FRAMES, B_IMG, B_QIM, B_THR, B_TMPA, B_TMPB, B_TMAX, B_TMIN, B_LAB,
+    B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
+    B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
+    B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN,
+    B_CUB, B_ERR, B_NBUF
+};
+
+}  // namespace
+
+struct at_internal {
+    at_family families[AT_MAX_FAMILIES];
+    int bits[AT_MAX_FAMILIES];
+    int nfam = 0;
+    GpuFamily gfam[AT_MAX_FAMILIES];
+    std::vector<void *> fam_mem[AT_MAX_FAMILIES];
+    DBuf dfam;
+    bool fam_dirty = true;
+
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[12];
+    DBuf buf[B_NBUF];
+    HBuf h_frames, h_small, h_out;
+    std::vector<at_detection> dets;
+
+    int err = 0;
+    std::string msg;
+    // sizes of the last run (frame 0), for at_detector_diag
+    int64_t last_qw = 0, last_qh = 0, last_npts = 0, last_ncl = 0, last_nq = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Errors: a failed CUDA call ends the frame with no detections.
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            set_error(in, 1, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+            return false;                                                                   \
+        }                                                                                   \
+    } while (0)
+
+static void set_error(at_internal *in, int code, const std::string &m) {
+    in->err = code;
+    in->msg = m;
+    fprintf(stderr, "apriltag_b200: %s\n", m.c_str());
+}
+
+// ---------------------------------------------------------------------------
+// Families and their quick-decode tables (fast/decode.c:20-58), built on the
+// host once per at_add_family and kept on the device.
+
+static bool upload_family(at_internal *in, int i) {
+    const at_family *f = &in->families[i];
+    GpuFamily g;
+    memset(&g, 0, sizeof g);
+    g.nbits = f->nbits;
+    g.wab = f->width_at_border;
+    g.tw = f->total_width;
+    g.reversed_border = f->reversed_border ? 1 : 0;
+    g.chunk = (f->nbits + 3) / 4;
+    g.cap = (int64_t)1 << g.chunk;
+    g.ncodes = f->ncodes;
+    g.maxham = in->bits[i];
+    for (int k = 0; k < 64; k++) {
+        g.bit_x[k] = f->bit_x[k];
+        g.bit_y[k] = f->bit_y[k];
+    }
+    uint64_t mask = (uint64_t)g.cap - 1;
+    std::vector<uint32_t> off(4 * (g.cap + 1), 0);
+    std::vector<uint16_t> idx(4 * g.ncodes + 1);
+    std::vector<uint64_t> codes(4 * g.ncodes + 1);
+    for (int64_t c = 0; c < g.ncodes; c++)
+        for (int j = 0; j < 4; j++) off[j * (g.cap + 1) + ((f->codes[c] >> (j * g.chunk)) & mask) + 1]++;
+    for (int j = 0; j < 4; j++)
+        for (int64_t v = 0; v < g.cap; v++) off[j * (g.cap + 1) + v + 1] += off[j * (g.cap + 1) + v];
+    std::vector<uint32_t> cur(off);
+    for (int64_t c = 0; c < g.ncodes; c++)
+        for (int j = 0; j < 4; j++) {
+            int64_t b = j * (g.cap + 1) + ((f->codes[c] >> (j * g.chunk)) & mask);
+            int64_t e = j * g.ncodes + cur[b]++;
+            idx[e] = (uint16_t)c;
+            codes[e] = f->codes[c];
+        }
+    for (void *p : in->fam_mem[i]) cudaFree(p);
+    in->fam_mem[i].clear();
+    void *d_off, *d_idx, *d_codes;
+    CK(cudaMalloc(&d_off, off.size() * 4));
+    in->fam_mem[i].push_back(d_off);
+    CK(cudaMalloc(&d_idx, idx.size() * 2));
+    in->fam_mem[i].push_back(d_idx);
+    CK(cudaMalloc(&d_codes, codes.size() * 8));
+    in->fam_mem[i].push_back(d_codes);
+    CK(cudaMemcpy(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_idx, idx.data(), idx.size() * 2, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_codes, codes.data(), codes.size() * 8, cudaMemcpyHostToDevice));
+    g.off = (const uint32_t *)d_off;
+    g.idx = (const uint16_t *)d_idx;
+    g.codes = (const uint64_t *)d_codes;
+    in->gfam[i] = g;
+    in->fam_dirty = true;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side constants of the reference.
+
+// The quad image size (fast/image.c:6-20).
+static void quad_size(int64_t w, int64_t h, float f, int64_t *qw, int64_t *qh) {
+    if (!(f > 1.0f)) {
+        *qw = w;
+        *qh = h;
+    } else if (f == 1.5f) {
+        *qw = w / 3 * 2;
+        *qh = h / 3 * 2;
+    } else if ((int64_t)f == 2) {
+        *qw = w / 2;
+        *qh = h / 2;
+    } else {
+        int64_t k = (int64_t)f;
+        *qw = 1 + (w - 1) / k;
+        *qh = 1 + (h - 1) / k;
+    }
+}
+
+// Blur taps (fast/image.c:108-118, 476-482): 0 when nothing is filtered.
+static int blur_taps(float qsigma, BlurTaps *t) {
+    if (qsigma == 0.0f) return 0;
+    int64_t n = (int64_t)(4.0f * fabsf(qsigma));
+    if ((n & 1) == 0) n++;
+    if (n <= 1) return 0;
+    if (n > 63) return -1;
+    double sigma = fabsf(qsigma);
+    double dk[64], acc = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        double x = (double)(i - n / 2) / sigma;
+        dk[i] = exp(-0.5 * (x * x));
+    }
+    for (int64_t i = 0; i < n; i++) acc += dk[i];
+    t->n = (int)n;
+    for (int64_t i = 0; i < n; i++) t->k[i] = (uint8_t)(dk[i] / acc * 255.0);
+    return (int)n;
+}
+
+static void gpu_params(const at_detector *td, const at_internal *in, bool decode_blurred, GpuParams *p) {
+    memset(p, 0, sizeof *p);
+    p->quad_decimate = td->quad_decimate;
+    p->min_cluster_pixels = td->qtp.min_cluster_pixels;
+    p->max_nmaxima = td->qtp.max_nmaxima;
+    p->min_white_black_diff = td->qtp.min_white_black_diff;
+    // min_tag_width (fast/detector.c:67-81)
+    int32_t mtw = 1000000;
+    bool normal = false, reversed = false;
+    for (int i = 0; i < in->nfam; i++) {
+        if (in->families[i].width_at_border < mtw) mtw = in->families[i].width_at_border;
+        normal = normal || !in->families[i].reversed_border;
+        reversed = reversed || in->families[i].reversed_border;
+    }
+    if (td->quad_decimate > 1.0f) mtw = (int32_t)((float)mtw / td->quad_decimate);
+    if (mtw < 3) mtw = 3;
+    p->tag_width = mtw;
+    p->normal_border = normal;
+    p->reversed_border = reversed;
+    p->refine_edges = td->refine_edges ? 1 : 0;
+    p->decode_blurred = decode_blurred ? 1 : 0;
+    p->nfam = in->nfam;
+    p->max_dot = (double)td->qtp.cos_critical_rad;
+    p->max_mse = (double)td->qtp.max_line_fit_mse;
+    p->decode_sharpening = td->decode_sharpening;
+    for (int i = 0; i < 7; i++) p->qsm[i] = (float)exp(-(double)((i - 3) * (i - 3)) / 2.0);
+    for (int r = 0; r < 4; r++) {
+        double th = (double)r * M_PI / 2.0;
+        p->rot_cs[r][0] = cos(th);
+        p->rot_cs[r][1] = sin(th);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The pipeline over a batch of frames.
+
+static int bits_for(uint64_t n) {
+    int b = 1;
+    while (b < 63 && ((uint64_t)1 << b) < n) b++;
+    return b;
+}
+
+template <class F> static bool cub_call(at_internal *in, F &&f) {
+    size_t bytes = 0;
+    CK(f(nullptr, bytes));
+    CK(in->buf[B_CUB].ensure(bytes));
+    CK(f(in->buf[B_CUB].p, bytes));
+    return true;
+}
+
+static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *res) {
+    at_internal *in = td->in;
+    cudaStream_t st = in->stream;
+    CK(cudaSetDevice(in->device));
+    if (td->qtp.max_nmaxima > AT_MAX_NMAXIMA || td->qtp.max_nmaxima < 0) {
+        set_error(in, 2, "max_nmaxima above the supported " + std::to_string(AT_MAX_NMAXIMA));
+        return false;
+    }
+    BlurTaps taps;
+    memset(&taps, 0, sizeof taps);
+    int ntaps = blur_taps(td->quad_sigma, &taps);
+    if (ntaps < 0) {
+        set_error(in, 2, "quad_sigma too large (blur kernel above 63 taps)");
+        return false;
+    }
+    const bool decimated = td->quad_decimate > 1.0f;
+    GpuParams prm;
+    gpu_params(td, in, ntaps > 1 && !decimated, &prm);
+
+    // frame layout
+    std::vector<FrameDesc> fd(n);
+    int64_t img = 0, qpx = 0, nodes = 0, rows = 0, tiles = 0;
+    uint32_t all = in->nfam >= 32 ? 0xffffffffu : ((1u << in->nfam) - 1u);
+    for (int64_t i = 0; i < n; i++) {
+        FrameDesc &f = fd[i];
+        memset(&f, 0, sizeof f);
+        const at_frame &fr = frames[i];
+        bool live = in->nfam > 0 && fr.width >= 8 && fr.height >= 8;
+        int64_t qw = 0, qh = 0;
+        if (live) quad_size(fr.width, fr.height, td->quad_decimate, &qw, &qh);
+        if (qw < 4 || qh < 4) live = false;
+        f.w = live ? (int32_t)fr.width : 0;
+        f.h = live ? (int32_t)fr.height : 0;
+        f.qw = live ? (int32_t)qw : 0;
+        f.qh = live ? (int32_t)qh : 0;
+        f.img_off = img;
+        f.q_off = qpx;
+        f.node_off = nodes;
+        f.row0 = rows;
+        f.tile_off = tiles;
+        f.fam_mask = fr.family_mask ? (fr.family_mask & all) : all;
+        f.max_px = (int32_t)(2 * (2 * f.qw + 2 * f.qh));
+        img += (int64_t)f.w * f.h;
+        qpx += (int64_t)f.qw * f.qh;
+        nodes += (int64_t)f.qw * f.qh + f.qh;
+        rows += f.qh;
+        tiles += (int64_t)(f.qw / 4) * (f.qh / 4);
+    }
+    for (int64_t i = 0; i < n; i++) res[i] = at_frame_result{0, 0, 0};
+    in->dets.clear();
+    in->last_qw = n > 0 ? fd[0].qw : 0;
+    in->last_qh = n > 0 ? fd[0].qh : 0;
+    in->last_npts = in->last_ncl = in->last_nq = 0;
+    if (qpx == 0) return true;
+    if (nodes >= ((int64_t)1 << 32)) {
+        set_error(in, 2, "batch too large (union-find ids exceed 32 bits)");
+        return false;
+    }
+    const int nb = bits_for((uint64_t)nodes);
+    Launch L{st, (int)n, 0};
+    int64_t maxq = 0;
+    for (auto &f : fd) maxq = f.qw * (int64_t)f.qh > maxq ? f.qw * (int64_t)f.qh : maxq;
+    L.blocks_per_frame = (int)((maxq + 255) / 256 < 148 * 4 ? (maxq + 255) / 256 : 148 * 4);
+    if (L.blocks_per_frame < 1) L.blocks_per_frame = 1;
+
+    // arenas
+    DBuf *B = in->buf;
+    CK(B[B_FRAMES].ensure(n * sizeof(FrameDesc)));
+    CK(B[B_IMG].ensure(img));
+    CK(B[B_QIM].ensure(qpx));
+    CK(B[B_THR].ensure(qpx));
+    CK(B[B_TMPA].ensure(qpx));
+    CK(B[B_TMPB].ensure(qpx));
+    CK(B[B_TMAX].ensure(tiles + 1));
+    CK(B[B_TMIN].ensure(tiles + 1));
+    CK(B[B_LAB].ensure(qpx * 4));
+    CK(B[B_RSTART].ensure(nodes * 2));
+    CK(B[B_REND].ensure(nodes * 2));
+    CK(B[B_RV].ensure(nodes));
+    CK(B[B_PARENT].ensure(nodes * 4));
+    CK(B[B_PX].ensure(nodes * 4));
+    CK(B[B_ROWRUNS].ensure(rows * 4));
+    CK(B[B_ROWPTS].ensure((rows + 1) * 8));
+    CK(B[B_ROWOFF].ensure((rows + 1) * 8));
+    CK(B[B_ERR].ensure(4));
+    CK(in->h_frames.ensure(n * sizeof(FrameDesc)));
+    memcpy(in->h_frames.p, fd.data(), n * sizeof(FrameDesc));
+    const FrameDesc *dfr = B[B_FRAMES].as<FrameDesc>();
+
+    for (int k = 0; k < 12; k++) CK(cudaEventRecord(in->ev[k], st));  // keep all events valid
+    CK(cudaEventRecord(in->ev[0], st));
+    CK(cudaMemcpyAsync(B[B_FRAMES].p, in->h_frames.p, n * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(B[B_ERR].p, 0, 4, st));
+    for (int64_t i = 0; i < n; i++) {
+        if (fd[i].qw == 0) continue;
+        CK(cudaMemcpy2DAsync(B[B_IMG].as<uint8_t>() + fd[i].img_off, fd[i].w, frames[i].pixels, frames[i].stride,
+                             fd[i].w, fd[i].h, cudaMemcpyDefault, st));
+    }
+    uint8_t *qim = B[B_QIM].as<uint8_t>(), *thr = B[B_THR].as<uint8_t>();
+    launch_decimate(L, dfr, B[B_IMG].as<uint8_t>(), qim, td->quad_decimate);
+    CK(cudaEventRecord(in->ev[1], st));
+    if (ntaps > 1) launch_blur(L, dfr, qim, B[B_TMPA].as<uint8_t>(), B[B_TMPB].as<uint8_t>(), taps, td->quad_sigma < 0);
+    CK(cudaEventRecord(in->ev[2], st));
+    launch_threshold(L, dfr, qim, B[B_TMAX].as<uint8_t>(), B[B_TMIN].as<uint8_t>(), thr, td->qtp.min_white_black_diff);
+    if (td->qtp.deglitch) launch_deglitch(L, dfr, thr, B[B_TMPA].as<uint8_t>());
+    CK(cudaEventRecord(in->ev[3], st));
+    RunArrays runs{B[B_RSTART].as<uint16_t>(), B[B_REND].as<uint16_t>(), B[B_RV].as<uint8_t>(),
+                   B[B_PARENT].as<uint32_t>(), B[B_PX].as<uint32_t>()};
+    uint32_t *lab = B[B_LAB].as<uint32_t>();
+    launch_segment(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), lab, td->qtp.min_cluster_pixels);
+    CK(cudaEventRecord(in->ev[4], st));
+    CK(cudaGetLastError());
+
+    // boundary points
+    uint64_t *row_npts = B[B_ROWPTS].as<uint64_t>(), *row_off = B[B_ROWOFF].as<uint64_t>();
+    CK(cudaMemsetAsync(row_npts + rows, 0, 8, st));
+    launch_point_count(L, dfr, thr, lab, row_npts);
+    if (!cub_call(in, [&](void *t, size_t &b) {
+            return cub::DeviceScan::ExclusiveSum(t, b, row_npts, row_off, rows + 1, st);
+        }))
+        return false;
+    uint64_t npts = 0;
+    CK(cudaMemcpyAsync(&npts, row_off + rows, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int64_t ncl = 0, nq = 0;
+    std::vector<GpuQuad> hq;
+    std::vector<int64_t> qstart(n + 1, 0);
+    if (npts > 0) {
+        CK(B[B_KEY].ensure(npts * 8));
+        CK(B[B_VAL].ensure(npts * 8));
+        CK(B[B_KEY2].ensure(npts * 8));
+        CK(B[B_VAL2].ensure(npts * 8));
+        CK(B[B_HEAD].ensure(npts * 4));
+        CK(B[B_HSCAN].ensure(npts * 4));
+        launch_point_emit(L, dfr, thr, lab, row_off, B[B_KEY].as<uint64_t>(), B[B_VAL].as<uint64_t>(), nb);
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
+                                                       B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
+                                                       (int64_t)npts, 0, 2 * nb, st);
+            }))
+            return false;
+        const uint64_t *skey = B[B_KEY2].as<uint64_t>(), *spts = B[B_VAL2].as<uint64_t>();
+        uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
+        launch_cluster_heads(st, skey, npts, head);
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
+            }))
+            return false;
+        uint32_t last[2];
+        CK(cudaMemcpyAsync(&last[0], hscan + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&last[1], head + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ncl = (int64_t)last[0] + last[1];
+        CK(B[B_CSTART].ensure(ncl * 4));
+        CK(B[B_CFRAME].ensure(ncl * 4));
+        launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
+                              B[B_CFRAME].as<int32_t>());
+        CK(cudaEventRecord(in->ev[5], st));
+
+        // quads
+        const int sc[] = {B_SKEYS, B_SSKEY, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW,
+                          B_SERRS, B_SFILT, B_SMXE};
+        for (int b : sc) CK(B[b].ensure(npts * 8));
+        CK(B[B_SSVAL].ensure(npts * 4));
+        CK(B[B_SMXI].ensure(npts * 4));
+        CK(B[B_QUADS].ensure(ncl * sizeof(GpuQuad)));
+        CK(B[B_QOK].ensure(ncl * 4));
+        CK(B[B_QSCAN].ensure(ncl * 4));
+        FitScratch scr{B[B_SKEYS].as<uint64_t>(), B[B_SSKEY].as<uint64_t>(), B[B_SSVAL].as<uint32_t>(),
+                       B[B_SW].as<double>(),      B[B_SFX].as<double>(),    B[B_SFY].as<double>(),
+                       B[B_SMX].as<double>(),     B[B_SMY].as<double>(),    B[B_SMXX].as<double>(),
+                       B[B_SMXY].as<double>(),    B[B_SMYY].as<double>(),   B[B_SMW].as<double>(),
+                       B[B_SERRS].as<double>(),   B[B_SFILT].as<double>(),  B[B_SMXE].as<double>(),
+                       B[B_SMXI].as<int32_t>()};
+        uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
+        launch_fit_quads(st, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
+                         (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
+        CK(cudaGetLastError());
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
+            }))
+            return false;
+        CK(cudaMemcpyAsync(&last[0], qscan + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&last[1], qok + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        nq = (int64_t)last[0] + last[1];
+        if (nq > 0) {
+            CK(B[B_QUADSC].ensure(nq * sizeof(GpuQuad)));
+            launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>());
+            hq.resize(nq);
+            CK(cudaMemcpyAsync(hq.data(), B[B_QUADSC].p, nq * sizeof(GpuQuad), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+    }
+    CK(cudaEventRecord(in->ev[6], st));
+    in->last_npts = (int64_t)npts;
+    in->last_ncl = ncl;
+    in->last_nq = nq;
+    // quads are in cluster order, so grouped by frame
+    for (int64_t i = 0, f = 0; f <= n; f++) {
+        while (i < nq && hq[i].frame < f) i++;
+        qstart[f] = i;
+    }
+    for (int64_t f = 0; f < n; f++) res[f].nquads = qstart[f + 1] - qstart[f];
+    if (nq > 0) {
+        // decode
+        if (in->fam_dirty) {
+            CK(in->dfam.ensure(sizeof(GpuFamily) * AT_MAX_FAMILIES));
+            CK(cudaMemcpyAsync(in->dfam.p, in->gfam, sizeof(GpuFamily) * AT_MAX_FAMILIES, cudaMemcpyHostToDevice, st));
+            in->fam_dirty = false;
+        }
+        const int64_t nd = nq * in->nfam;
+        CK(B[B_DETS].ensure(nd * sizeof(GpuDetection)));
+        CK(B[B_DETOK].ensure(nd * 4));
+        CK(B[B_OUT].ensure(nd * sizeof(GpuDetection)));
+        CK(B[B_QSTART].ensure((n + 1) * 8));
+        CK(B[B_OUTOFF].ensure((n + 1) * 8));
+        CK(B[B_OUTN].ensure((n + 1) * 8));
+        CK(in->h_small.ensure((3 * n + 3) * 8));
+        int64_t *hs = in->h_small.as<int64_t>();
+        for (int64_t f = 0; f <= n; f++) {
+            hs[f] = qstart[f];
+            hs[n + 1 + f] = qstart[f] * in->nfam;
+        }
+        CK(cudaMemcpyAsync(B[B_QSTART].p, hs, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(B[B_OUTOFF].p, hs + n + 1, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+        launch_decode(st, dfr, prm, in->dfam.as<GpuFamily>(), B[B_IMG].as<uint8_t>(), qim, B[B_QUADSC].as<GpuQuad>(),
+                      nq, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
+        CK(cudaEventRecord(in->ev[7], st));
+        launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
+                        B[B_DETOK].as<uint32_t>(), B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
+                        B[B_OUTN].as<int64_t>());
+        CK(cudaGetLastError());
+        CK(in->h_out.ensure(nd * sizeof(GpuDetection)));
+        CK(cudaMemcpyAsync(hs + 2 * n + 2, B[B_OUTN].p, n * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(in->h_out.p, B[B_OUT].p, nd * sizeof(GpuDetection), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(in->ev[8], st));
+        uint32_t derr = 0;
+        CK(cudaMemcpyAsync(&derr, B[B_ERR].p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (derr) {
+            set_error(in, 3, "device check failed (code " + std::to_string(derr) + ")");
+            return false;
+        }
+        const GpuDetection *ho = in->h_out.as<GpuDetection>();
+        for (int64_t f = 0; f < n; f++) {
+            int64_t cnt = hs[2 * n + 2 + f];
+            res[f].first = (int64_t)in->dets.size();
+            res[f].count = cnt;
+            const GpuDetection *src = ho + qstart[f] * in->nfam;
+            for (int64_t k = 0; k < cnt; k++) {
+                at_detection d;
+                memcpy(&d, &src[k], sizeof d);
+                in->dets.push_back(d);
+            }
+        }
+    } else {
+        CK(cudaEventRecord(in->ev[7], st));
+        CK(cudaEventRecord(in->ev[8], st));
+        CK(cudaStreamSynchronize(st));
+    }
+    // stage times from the events (at_timing, fast/apriltag_fast.h:67-69)
+    auto dt = [&](int a, int b) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, in->ev[a], in->ev[b]);
+        return (double)ms * 1e-3;
+    };
+    memset(&td->timing, 0, sizeof td->timing);
+    td->timing.decimate = dt(0, 1);
+    td->timing.blur = dt(1, 2);
+    td->timing.threshold = dt(2, 3);
+    td->timing.unionfind = dt(3, 4);
+    if (npts > 0) {
+        td->timing.clusters = dt(4, 5);
+        td->timing.fit_quads = dt(5, 6);
+    } else {
+        td->timing.clusters = dt(4, 6);
+    }
+    td->timing.decode = dt(6, 7);
+    td->timing.reconcile = dt(7, 8);
+    td->timing.total = dt(0, 8);
+    if (td->debug && n == 1 && fd[0].qw > 0) {
+        std::vector<uint8_t> h((size_t)fd[0].qw * fd[0].qh);
+        CK(cudaMemcpy(h.data(), qim, h.size(), cudaMemcpyDeviceToHost));
+        at_write_pgm("debug_preprocess.pnm", h.data(), fd[0].qw, fd[0].qh);
+        CK(cudaMemcpy(h.data(), thr, h.size(), cudaMemcpyDeviceToHost));
+        at_write_pgm("debug_threshold.pnm", h.data(), fd[0].qw, fd[0].qh);
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// The C ABI.
+
+extern "C" {
+
+at_detector *at_detector_create(void) {
+    at_detector *td = (at_detector *)calloc(1, sizeof *td);
+    at_internal *in = new at_internal();
+    if (!td) abort();
+    td->nthreads = 1;
+    td->quad_decimate = 2.0f;
+    td->quad_sigma = 0.0f;
+    td->refine_edges = true;
+    td->decode_sharpening = 0.25;
+    td->debug = false;
+    td->qtp.min_cluster_pixels = 24;
+    td->qtp.max_nmaxima = 10;
+    td->qtp.critical_rad = 0.0f;
+    td->qtp.cos_critical_rad = (float)cos(10.0 * M_PI / 180.0);
+    td->qtp.max_line_fit_mse = 10.0f;
+    td->qtp.min_white_black_diff = 5;
+    td->qtp.deglitch = false;
+    td->in = in;
+    if (cudaGetDevice(&in->device) != cudaSuccess || cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        fprintf(stderr, "apriltag_b200: no usable CUDA device\n");
+        abort();
+    }
+    for (int k = 0; k < 12; k++) cudaEventCreate(&in->ev[k]);
+    return td;
+}
+
+static void release_arenas(at_internal *in) {
+    for (int b = 0; b < B_NBUF; b++) in->buf[b].release();
+    in->h_frames.release();
+    in->h_small.release();
+    in->h_out.release();
+}
+
+void at_shutdown(at_detector *td) {
+    if (!td) return;
+    cudaStreamSynchronize(td->in->stream);
+    release_arenas(td->in);
+}
+
+void at_detector_destroy(at_detector *td) {
+    if (!td) return;
+    at_internal *in = td->in;
+    cudaStreamSynchronize(in->stream);
+    release_arenas(in);
+    for (int i = 0; i < AT_MAX_FAMILIES; i++)
+        for (void *p : in->fam_mem[i]) cudaFree(p);
+    in->dfam.release();
+    for (int k = 0; k < 12; k++) cudaEventDestroy(in->ev[k]);
+    cudaStreamDestroy(in->stream);
+    delete in;
+    free(td);
+}
+
+bool at_add_family(at_detector *td, const at_family *fam, int bits_corrected) {
+    at_internal *in = td->in;
+    if (bits_corrected < 0 || bits_corrected > 3) return false;
+    if (in->nfam == AT_MAX_FAMILIES) return false;
+    if (fam->ncodes >= 65536 || fam->nbits <= 0 || fam->nbits > 64) return false;
+    if (fam->total_width > AT_MAX_TW || fam->width_at_border > AT_MAX_TW || fam->width_at_border < 1) {
+        set_error(in, 2, "family total_width above the supported 16");
+        return false;
+    }
+    // every bit must land in the total_width x total_width grid that the
+    // sampler fills (fast/decode.c:340-361)
+    int32_t minc = (fam->width_at_border - fam->total_width) / 2;
+    for (int k = 0; k < fam->nbits; k++)
+        if (fam->bit_x[k] - minc < 0 || fam->bit_x[k] - minc >= fam->total_width || fam->bit_y[k] - minc < 0 ||
+            fam->bit_y[k] - minc >= fam->total_width) {
+            set_error(in, 2, "family bit position outside the tag grid");
+            return false;
+        }
+    int i = in->nfam;
+    in->families[i] = *fam;
+    in->bits[i] = bits_corrected;
+    if (!upload_family(in, i)) return false;
+    in->nfam++;
+    return true;
+}
+
+void at_clear_families(at_detector *td) {
+    td->in->nfam = 0;
+    td->in->fam_dirty = true;
+}
+
+const char *at_family_name(const at_detector *td, const at_detection *d) { return td->in->families[d->family].name; }
+
+void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *results) {
+    at_internal *in = td->in;
+    in->err = 0;
+    in->msg.clear();
+    td->ndetections = 0;
+    td->nquads = 0;
+    if (!run_batch(td, frames, n, results)) {
+        in->dets.clear();
+        for (int64_t i = 0; i < n; i++) results[i] = at_frame_result{0, 0, 0};
+    }
+    td->detections = in->dets.data();
+    td->ndetections = (int64_t)in->dets.size();
+    int64_t nq = 0;
+    for (int64_t i = 0; i < n; i++) nq += results[i].nquads;
+    td->nquads = nq;
+}
+
+void at_detect(at_detector *td, const uint8_t *pixels, int64_t width, int64_t height, int64_t stride) {
+    at_frame f{pixels, width, height, stride, 0};
+    at_frame_result r;
+    at_detect_batch(td, &f, 1, &r);
+}
+
+int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap) {
+    at_internal *in = td->in;
+    const DBuf *B = in->buf;
+    const void *src = nullptr;
+    int64_t bytes = 0;
+    int64_t sizes[5] = {in->last_qw, in->last_qh, in->last_npts, in->last_ncl, in->last_nq};
+    switch (what) {
+    case AT_DIAG_QUAD_IMAGE: src = B[B_QIM].p, bytes = in->last_qw * in->last_qh; break;
+    case AT_DIAG_THRESHOLD: src = B[B_THR].p, bytes = in->last_qw * in->last_qh; break;
+    case AT_DIAG_LABELS: src = B[B_LAB].p, bytes = 4 * in->last_qw * in->last_qh; break;
+    case AT_DIAG_POINTS: src = B[B_VAL2].p, bytes = 8 * in->last_npts; break;
+    case AT_DIAG_CLUSTERS: src = B[B_CSTART].p, bytes = 4 * in->last_ncl; break;
+    case AT_DIAG_QUADS: src = B[B_QUADSC].p, bytes = (int64_t)sizeof(GpuQuad) * in->last_nq; break;
+    case AT_DIAG_SIZES:
+        memcpy(dst, sizes, (size_t)(cap < 40 ? cap : 40));
+        return 40;
+    default: return -1;
+    }
+    int64_t n = bytes < cap ? bytes : cap;
+    if (n > 0 && src && cudaMemcpy(dst, src, (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return bytes;
+}
+
+int at_detector_last_error(const at_detector *td, const char **message) {
+    if (message) *message = td->in->msg.c_str();
+    return td->in->err;
+}
+
+// Built-in families (fast/families.c:44-78).
+static const at_family *builtin(const char *name) {
+    if (!at_builtin_families) return nullptr;
+    for (int i = 0; at_builtin_families[i]; i++)
+        if (!strcmp(at_builtin_families[i]->name, name)) return at_builtin_families[i];
+    return nullptr;
+}
+const at_family *at_family_by_name(const char *name) { return builtin(name); }
+const at_family *at_tag16h5(void) { return builtin("tag16h5"); }
+const at_family *at_tag25h9(void) { return builtin("tag25h9"); }
+const at_family *at_tag36h10(void) { return builtin("tag36h10"); }
+const at_family *at_tag36h11(void) { return builtin("tag36h11"); }
+const at_family *at_tagCircle21h7(void) { return builtin("tagCircle21h7"); }
+const at_family *at_tagCircle49h12(void) { return builtin("tagCircle49h12"); }
+const at_family *at_tagCustom48h12(void) { return builtin("tagCustom48h12"); }
+const at_family *at_tagStandard41h12(void) { return builtin("tagStandard41h12"); }
+const at_family *at_tagStandard52h13(void) { return builtin("tagStandard52h13"); }
+
+// PNM files, as the reference reads them (fast/image.c:204-266): binary PGM
+// or PPM with maxval 255; color becomes (r + 2g + b) / 4.
+static void pnm_skip(const uint8_t *d, int64_t n, int64_t *at) {
+    while (*at < n) {
+        uint8_t c = d[*at];
+        if (c == '#') {
+            while (*at < n && d[*at] != '\n') (*at)++;
+        } else if (c == ' ' || c == '\n' || c == '\r' || c == '\t') {
+            (*at)++;
+        } else {
+            return;
+        }
+    }
+}
+static int64_t pnm_int(const uint8_t *d, int64_t n, int64_t *at) {
+    pnm_skip(d, n, at);
+    int64_t v = 0;
+    while (*at < n && d[*at] >= '0' && d[*at] <= '9') v = v * 10 + (d[(*at)++] - '0');
+    return v;
+}
+
+bool at_read_pnm_into(const char *path, int64_t *width, int64_t *height, uint8_t **pixels, int64_t *cap) {
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return false;
+    std::vector<uint8_t> d;
+    bool ok = false;
+    if (fseek(fp, 0, SEEK_END) == 0) {
+        long len = ftell(fp);
+        if (len > 0 && fseek(fp, 0, SEEK_SET) == 0) {
+            d.resize(len);
+            ok = fread(d.data(), 1, len, fp) == (size_t)len;
+        }
+    }
+    fclose(fp);
+    if (!ok || d.size() < 2 || d[0] != 'P' || (d[1] != '5' && d[1] != '6')) return false;
+    int64_t n = (int64_t)d.size(), at = 2;
+    int64_t w = pnm_int(d.data(), n, &at), h = pnm_int(d.data(), n, &at), mv = pnm_int(d.data(), n, &at);
+    at++;
+    if (w <= 0 || h <= 0 || mv != 255) return false;
+    int64_t ch = d[1] == '5' ? 1 : 3;
+    if (n - at < w * h * ch) return false;
+    if (!*pixels || *cap < w * h) {
+        uint8_t *px = (uint8_t *)aligned_alloc(64, (size_t)(w * h + 63) / 64 * 64);
+        if (!px) return false;
+        free(*pixels);
+        *pixels = px;
+        *cap = w * h;
+    }
+    if (ch == 1) {
+        memcpy(*pixels, d.data() + at, w * h);
+    } else {
+        for (int64_t i = 0; i < w * h; i++) {
+            int r = d[at + 3 * i], g = d[at + 3 * i + 1], b = d[at + 3 * i + 2];
+            (*pixels)[i] = (uint8_t)((r + g + g + b) / 4);
+        }
+    }
+    *width = w;
+    *height = h;
+    return true;
+}
+
+bool at_read_pnm(const char *path, int64_t *width, int64_t *height, uint8_t **pixels) {
+    int64_t cap = 0;
+    *pixels = nullptr;
+    return at_read_pnm_into(path, width, height, pixels, &cap);
+}
+
+bool at_write_pgm(const char *path, const uint8_t *pixels, int64_t width, int64_t height) {
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return false;
+    fprintf(fp, "P5\n%lld %lld\n255\n", (long long)width, (long long)height);
+    bool ok = fwrite(pixels, 1, (size_t)(width * height), fp) == (size_t)(width * height);
+    return fclose(fp) == 0 && ok;
+}
+
+}  // extern "C"

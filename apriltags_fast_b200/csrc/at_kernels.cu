@@ -1,0 +1,1784 @@
+// The sm_100a kernels of the AprilTag detection path.
+//
+// Every kernel takes a batch of frames (FrameDesc array) and works on all
+// of them at once: blockIdx.y is the frame, blockIdx.x strides over the
+// frame's rows, pixels or items. Compiled with --fmad=false, -prec-div and
+// -prec-sqrt: each floating point operation is rounded on its own, as the
+// reference (built with -ffp-contract=off) rounds it, so the results are
+// bit-identical. Each kernel names the reference lines it follows.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "at_gpu.h"
+#include "at_kernels.h"
+
+// ---------------------------------------------------------------------------
+// Small helpers.
+
+__device__ __forceinline__ int64_t dmin(int64_t a, int64_t b) { return a < b ? a : b; }
+__device__ __forceinline__ int64_t dmax(int64_t a, int64_t b) { return a > b ? a : b; }
+
+// C's (int) of a double on x86-64: truncation, INT_MIN out of range or NaN
+// (fast/decode.c:8-11).
+__device__ __forceinline__ int64_t c_int(double x) {
+    if (x > -2147483649.0 && x < 2147483648.0) return (int64_t)x;
+    return -2147483648LL;
+}
+
+#define FRAME_LOOP_BEGIN(n_items)                                                               \
+    const FrameDesc fd = frames[blockIdx.y];                                                   \
+    for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < (n_items);          \
+         it += (int64_t)gridDim.x * blockDim.x) {
+#define FRAME_LOOP_END }
+
+// ---------------------------------------------------------------------------
+// 1. Decimation (fast/image.c:6-88). One thread per quad-image pixel.
+
+__global__ void k_decimate(const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t n = (int64_t)f.qw * f.qh;
+    const uint8_t *src = img + f.img_off;
+    uint8_t *out = qim + f.q_off;
+    const int64_t stride = f.w;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t y = i / f.qw, x = i - y * f.qw;
+        uint8_t o;
+        if (factor == 1.5f) {
+            // 3x3 weights over 9; output pixel (2k+dx, 2m+dy) from input
+            // block (3k.., 3m..) (fast/image.c:50-62)
+            int64_t k = x >> 1, m = y >> 1;
+            const uint8_t *r0 = src + (3 * m) * stride + 3 * k, *r1 = r0 + stride, *r2 = r1 + stride;
+            int e = r1[1];
+            int v;
+            if ((y & 1) == 0)
+                v = (x & 1) == 0 ? 4 * r0[0] + 2 * r0[1] + 2 * r1[0] + e : 4 * r0[2] + 2 * r0[1] + 2 * r1[2] + e;
+            else
+                v = (x & 1) == 0 ? 4 * r2[0] + 2 * r1[0] + 2 * r2[1] + e : 4 * r2[2] + 2 * r1[2] + 2 * r2[1] + e;
+            o = (uint8_t)(v / 9);
+        } else if (factor > 1.0f) {
+            int64_t k = (int64_t)factor;
+            if (k == 2) {
+                // 2x2 box; the part of the row below the largest multiple of
+                // 32 rounds twice (the C library's AVX2 path), the rest once
+                // (fast/image.c:26-46)
+                const uint8_t *r0 = src + 2 * y * stride + 2 * x, *r1 = r0 + stride;
+                int a = r0[0], b = r0[1], c = r1[0], d = r1[1];
+                if (x < f.qw - f.qw % 32)
+                    o = (uint8_t)((((a + c + 1) >> 1) + ((b + d + 1) >> 1) + 1) >> 1);
+                else
+                    o = (uint8_t)((a + b + c + d + 2) >> 2);
+            } else {
+                o = src[y * k * stride + x * k];
+            }
+        } else {
+            o = src[y * stride + x];
+        }
+        out[i] = o;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Blur / sharpen of the quad image (fast/image.c:93-173). The taps are
+// integers made on the host. A separable pass: `dir` 0 filters rows, 1
+// columns. The line's first nk/2 outputs and its tail copy the input; the
+// wide variant (images of 65536 pixels or more) filters one more output.
+
+__global__ void k_blur_pass(const FrameDesc *frames, const uint8_t *in, uint8_t *out, BlurTaps taps, int dir) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t n = (int64_t)f.qw * f.qh;
+    const bool wide = n >= 65536;
+    const int nk = taps.n, r = nk / 2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t y = i / f.qw, x = i - y * f.qw;
+        int64_t len = dir == 0 ? f.qw : f.qh, pos = dir == 0 ? x : y, step = dir == 0 ? 1 : f.qw;
+        const uint8_t *line = in + f.q_off + (dir == 0 ? y * f.qw : x);
+        int64_t m = wide ? len - nk + 1 : len - nk;
+        uint8_t v;
+        if (pos >= r && pos - r < m) {
+            uint32_t acc = 0;
+            for (int j = 0; j < nk; j++) acc += (uint32_t)taps.k[j] * line[(pos - r + j) * step];
+            v = (uint8_t)(acc >> 8);
+        } else {
+            v = line[pos * step];
+        }
+        out[f.q_off + i] = v;
+    }
+}
+
+// sharpen: im = clamp(2 * orig - blurred) (fast/image.c:484-489); else copy
+__global__ void k_blur_finish(const FrameDesc *frames, const uint8_t *blurred, uint8_t *qim, int sharpen) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t n = (int64_t)f.qw * f.qh;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t b = blurred[f.q_off + i];
+        if (sharpen) {
+            int v = 2 * (int)qim[f.q_off + i] - b;
+            qim[f.q_off + i] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        } else {
+            qim[f.q_off + i] = b;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Adaptive threshold (fast/threshold.c:15-161). First each 4x4 tile's
+// max and min, then per pixel the max and min of its tile's 3x3 tile
+// neighbourhood (cells outside the grid left out).
+
+__global__ void k_tile_minmax(const FrameDesc *frames, const uint8_t *qim, uint8_t *tmax, uint8_t *tmin) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t tw = f.qw / 4, th = f.qh / 4, n = tw * th;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t ty = i / tw, tx = i - ty * tw;
+        const uint8_t *p = qim + f.q_off + 4 * ty * f.qw + 4 * tx;
+        uint32_t hi = 0, lo = 255;
+#pragma unroll
+        for (int dy = 0; dy < 4; dy++) {
+            // byte loads: rows of odd widths are not 4-byte aligned
+            const uint8_t *r = p + dy * f.qw;
+            hi = max(hi, (uint32_t)max(max(r[0], r[1]), max(r[2], r[3])));
+            lo = min(lo, (uint32_t)min(min(r[0], r[1]), min(r[2], r[3])));
+        }
+        tmax[f.tile_off + i] = (uint8_t)hi;
+        tmin[f.tile_off + i] = (uint8_t)lo;
+    }
+}
+
+// Pixels right of the last whole tile column use that column and are never
+// 127; rows below the last whole tile row use that row and are never 127
+// (fast/threshold.c:85-91, 144-148).
+__global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const uint8_t *tmax, const uint8_t *tmin,
+                            uint8_t *thr, int32_t diff) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t tw = f.qw / 4, th = f.qh / 4, n = (int64_t)f.qw * f.qh;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t y = i / f.qw, x = i - y * f.qw;
+        int64_t ty = y >> 2, tx = x >> 2;
+        bool may_flat = true;
+        if (ty >= th) {
+            ty = th - 1;
+            may_flat = false;
+        }
+        if (tx >= tw) {
+            tx = tw - 1;
+            may_flat = false;
+        }
+        uint32_t hi = 0, lo = 255;
+        for (int64_t yy = dmax(ty - 1, 0); yy <= dmin(ty + 1, th - 1); yy++)
+            for (int64_t xx = dmax(tx - 1, 0); xx <= dmin(tx + 1, tw - 1); xx++) {
+                hi = max(hi, (uint32_t)tmax[f.tile_off + yy * tw + xx]);
+                lo = min(lo, (uint32_t)tmin[f.tile_off + yy * tw + xx]);
+            }
+        uint32_t t = lo + (hi - lo) / 2;
+        uint8_t v = qim[f.q_off + i] > t ? 255 : 0;
+        thr[f.q_off + i] = may_flat && (int32_t)(hi - lo) < diff ? 127 : v;
+    }
+}
+
+// Deglitch (fast/threshold.c:173-193): 3x3 dilate into tmp (its border
+// zero), then 3x3 erode back; the image border keeps its values.
+__global__ void k_morph(const FrameDesc *frames, const uint8_t *in, uint8_t *out, int dilate) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t n = (int64_t)f.qw * f.qh;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t y = i / f.qw, x = i - y * f.qw;
+        bool border = x == 0 || y == 0 || x == f.qw - 1 || y == f.qh - 1;
+        if (border) {
+            if (dilate) out[f.q_off + i] = 0;
+            continue;
+        }
+        uint32_t m = dilate ? 0 : 255;
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                uint32_t v = in[f.q_off + (y + dy) * f.qw + x + dx];
+                m = dilate ? max(m, v) : min(m, v);
+            }
+        out[f.q_off + i] = (uint8_t)m;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. Runs (fast/threshold.c:210-283). One warp per row: the run starts of
+// 32 columns at a time by ballot; runs of 127 are not kept. Each run gets
+// union-find node node_off + y*qw + i, initialised as its own root.
+
+__global__ void k_runs(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int64_t y = warp; y < f.qh; y += nwarps) {
+        const uint8_t *t = thr + f.q_off + y * f.qw;
+        const int64_t base = f.node_off + y * f.qw;
+        const int64_t xmax = f.qw - 2;
+        int64_t count = 0, open = -1;
+        for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
+            int64_t x = x0 + lane;
+            bool valid = x <= xmax;
+            uint8_t v = valid ? t[x] : 0;
+            bool start = valid && (x == 0 || t[x - 1] != v);
+            uint32_t S = __ballot_sync(0xffffffffu, start);
+            uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
+            if (start) {
+                uint32_t below = S & lt;
+                int64_t prev_slot;
+                if (below) {
+                    int pl = 31 - __clz(below);
+                    prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
+                } else {
+                    prev_slot = open;
+                }
+                if (prev_slot >= 0) runs.end[base + prev_slot] = (uint16_t)(x - 1);
+                if (v != 127) {
+                    int64_t s = base + count + __popc(N & lt);
+                    runs.start[s] = (uint16_t)x;
+                    runs.v[s] = v;
+                    runs.parent[s] = (uint32_t)s;
+                    runs.px[s] = 0;
+                }
+            }
+            if (S) {
+                int ls = 31 - __clz(S);
+                open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
+            }
+            count += __popc(N);
+        }
+        if (lane == 0) {
+            if (open >= 0) runs.end[base + open] = (uint16_t)xmax;
+            row_nruns[f.row0 + y] = (uint32_t)count;
+            int64_t vn = f.node_off + (int64_t)f.qw * f.qh + y;
+            runs.parent[vn] = (uint32_t)vn;
+            runs.px[vn] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 5. Connected components over runs (fast/unionfind.c:89-196): the same
+// pairs of runs join as in the reference; lock-free union that links the
+// larger root under the smaller, so every component's root is its smallest
+// node id (the label the cluster order is defined by).
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t *par, uint32_t x) {
+    volatile uint32_t *p = par;
+    uint32_t px = p[x];
+    while (px != x) {
+        uint32_t ppx = p[px];
+        if (ppx != px) p[x] = ppx;  // path halving: only ever an ancestor
+        x = px;
+        px = p[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_unite(uint32_t *par, uint32_t a, uint32_t b) {
+    for (;;) {
+        a = uf_find(par, a);
+        b = uf_find(par, b);
+        if (a == b) return;
+        if (a < b) {
+            uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(par + a, a, b) == a) return;
+    }
+}
+
+__device__ __forceinline__ bool runs_touch(int64_t a0, int64_t a1, int64_t b0, int64_t b1, uint8_t v) {
+    if (dmax(dmax(a0, b0), 1) <= dmin(a1, b1)) return true;
+    if (v != 255) return false;
+    if (dmax(dmax(a0, b0 + 1), 1) <= dmin(a1, b1 + 1)) return true;
+    return dmax(dmax(a0, b0 - 1), 1) <= dmin(a1, b1 - 1);
+}
+
+__global__ void k_union(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, const uint32_t *row_nruns) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t y = 1 + warp; y < f.qh; y += nwarps) {
+        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
+        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
+        for (int64_t i = lane; i < ncur; i += 32) {
+            int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
+            uint8_t v = runs.v[cur + i];
+            // the first run above with end + 1 >= a0 (unionfind.c:124)
+            int64_t lo = 0, hi = nprev;
+            while (lo < hi) {
+                int64_t mid = (lo + hi) >> 1;
+                if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            for (int64_t k = lo; k < nprev && (int64_t)runs.start[prev + k] <= a1 + 1; k++) {
+                if (runs.v[prev + k] != v) continue;
+                if (runs_touch(a0, a1, runs.start[prev + k], runs.end[prev + k], v))
+                    uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + k));
+            }
+        }
+        if (lane == 0 && ncur > 0) {
+            // a white run ending at w-2 joins pixel (w-1, y-1) when that is
+            // white and (w-2, y-1) is not (unionfind.c:89-97)
+            int64_t last = cur + ncur - 1;
+            const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
+            if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
+                uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
+        }
+    }
+}
+
+// Every node points at its root; each root sums its component's pixels.
+__global__ void k_flatten(const FrameDesc *frames, RunArrays runs, const uint32_t *row_nruns) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t y = warp; y < f.qh; y += nwarps) {
+        const int64_t base = f.node_off + y * f.qw;
+        const int64_t n = row_nruns[f.row0 + y];
+        for (int64_t i = lane; i <= n; i += 32) {
+            int64_t node = i < n ? base + i : f.node_off + (int64_t)f.qw * f.qh + y;
+            uint32_t r = uf_find(runs.parent, (uint32_t)node);
+            runs.parent[node] = r;
+            uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
+            atomicAdd(runs.px + r, px);
+        }
+    }
+}
+
+// Per pixel: its component's label if the component has at least
+// min_cluster_pixels pixels, else AT_NOK (no run: 127, or too small).
+__global__ void k_labels(const FrameDesc *frames, const RunArrays runs, const uint32_t *row_nruns, uint32_t *lab,
+                         int32_t min_px) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t n = (int64_t)f.qw * f.qh;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t y = i / f.qw, x = i - y * f.qw;
+        int64_t node = -1;
+        if (x == f.qw - 1) {
+            node = f.node_off + (int64_t)f.qw * f.qh + y;
+        } else {
+            const int64_t base = f.node_off + y * f.qw;
+            int64_t lo = 0, hi = row_nruns[f.row0 + y];
+            while (lo < hi) {  // the first run with start > x
+                int64_t mid = (lo + hi) >> 1;
+                if ((int64_t)runs.start[base + mid] <= x)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (lo > 0 && (int64_t)runs.end[base + lo - 1] >= x) node = base + lo - 1;
+        }
+        uint32_t l = AT_NOK;
+        if (node >= 0) {
+            uint32_t r = runs.parent[node];
+            if ((int64_t)runs.px[r] >= min_px) l = r;
+        }
+        lab[f.q_off + i] = l;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 6. Boundary points (fast/clusters.c:144-252). Pixel (x, y), y in
+// 1..qh-2, against (1,0), (0,1), (-1,1), (1,1): a point where one pixel is
+// 0 and the other 255 and both labels are not AT_NOK. The (-1,1) point is
+// left out when the pixel to the left gave its (1,1) point, except at x=1;
+// x = 0 gives only (1,0). Points are emitted in (y, x, neighbour) order.
+
+__device__ __forceinline__ uint32_t point_mask(const uint8_t *a, const uint8_t *b, const uint32_t *la,
+                                               const uint32_t *lb, int64_t x, int64_t qw) {
+    if (x >= qw - 1) return 0;
+    if (x == 0) return ((a[0] ^ a[1]) == 255 && la[0] != AT_NOK && la[1] != AT_NOK) ? 1u : 0u;
+    if (la[x] == AT_NOK) return 0;
+    uint8_t v = a[x];
+    uint32_t c10 = (v ^ a[x + 1]) == 255 && la[x + 1] != AT_NOK;
+    uint32_t c01 = (v ^ b[x]) == 255 && lb[x] != AT_NOK;
+    uint32_t cm1 = (v ^ b[x - 1]) == 255 && lb[x - 1] != AT_NOK;
+    uint32_t c11 = (v ^ b[x + 1]) == 255 && lb[x + 1] != AT_NOK;
+    uint32_t left11 = x > 1 && (a[x - 1] ^ b[x]) == 255 && la[x - 1] != AT_NOK && lb[x] != AT_NOK;
+    return c10 | c01 << 1 | (cm1 & (left11 ^ 1u)) << 2 | c11 << 3;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim <= 1024).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total, uint32_t *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) sh[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += t;
+        }
+        if (lane < nw) sh[lane] = s;
+    }
+    __syncthreads();
+    uint32_t off = wid > 0 ? sh[wid - 1] : 0;
+    *total = sh[nw - 1];
+    return off + incl - v;
+}
+
+__global__ void k_point_count(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, uint64_t *row_npts) {
+    __shared__ uint32_t sh[32];
+    const FrameDesc f = frames[blockIdx.y];
+    for (int64_t y = blockIdx.x; y < f.qh; y += gridDim.x) {
+        uint32_t cnt = 0;
+        if (y >= 1 && y + 1 < f.qh) {
+            const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;
+            const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+            for (int64_t x = threadIdx.x; x < f.qw; x += blockDim.x) cnt += __popc(point_mask(a, b, la, lb, x, f.qw));
+        }
+        uint32_t total;
+        block_excl_scan(cnt, &total, sh);
+        if (threadIdx.x == 0) row_npts[f.row0 + y] = total;
+    }
+}
+
+// The cluster key of a point: (larger label, smaller label) packed as
+// larger << nb | smaller, nb = bits of the largest node id.
+__global__ void k_point_emit(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                             const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb) {
+    __shared__ uint32_t sh[32];
+    const FrameDesc f = frames[blockIdx.y];
+    for (int64_t y = 1 + blockIdx.x; y + 1 < f.qh; y += gridDim.x) {
+        const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;
+        const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+        uint64_t out = row_pt_off[f.row0 + y];
+        for (int64_t x0 = 0; x0 < f.qw; x0 += blockDim.x) {
+            int64_t x = x0 + threadIdx.x;
+            uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
+            uint32_t total;
+            uint32_t off = block_excl_scan(__popc(m), &total, sh);
+            uint64_t o = out + off;
+            int g = a[x < f.qw ? x : 0] == 0 ? 255 : -255;
+            for (int j = 0; j < 4; j++) {
+                if (!(m >> j & 1u)) continue;
+                int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0;
+                int dy = j == 0 ? 0 : 1;
+                uint32_t l0 = la[x], l1 = dy ? lb[x + dx] : la[x + dx];
+                uint64_t hi = l0 > l1 ? l0 : l1, lo = l0 > l1 ? l1 : l0;
+                uint64_t px = (uint64_t)(2 * x + dx), py = (uint64_t)(2 * y + dy);
+                uint64_t gx = (uint16_t)(int16_t)(dx * g), gy = (uint16_t)(int16_t)(dy * g);
+                pt_key[o] = hi << nb | lo;
+                pt_val[o] = px | py << 16 | gx << 32 | gy << 48;
+                o++;
+            }
+            out += total;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 7. Clusters: after the stable sort by key, each run of equal keys is a
+// cluster (points in emission order).
+
+__global__ void k_cluster_heads(const uint64_t *key, int64_t n, uint32_t *head) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        head[i] = i == 0 || key[i] != key[i - 1];
+}
+
+__global__ void k_cluster_starts(const uint64_t *key, const uint32_t *head, const uint32_t *head_scan, int64_t n,
+                                 int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!head[i]) continue;
+        uint32_t c = head_scan[i];
+        cstart[c] = (uint32_t)i;
+        int64_t node = (int64_t)(key[i] >> nb);
+        int lo = 0, hi = nframes - 1;  // the frame whose node range holds node
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (frames[mid].node_off <= node)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        cframe[c] = lo;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 8. Quad fitting, one block per cluster (fast/quads.c:429-1160).
+
+__device__ __forceinline__ uint32_t f32_bits(float f) { return __float_as_uint(f); }
+
+// The angle key (fast/quads.c:429-453): quadrant + slope in f32, as
+// order-preserving bits, above the complemented point index.
+__device__ __forceinline__ uint64_t angle_key(float dx, float dy, uint32_t idx) {
+    float quadrant = dy > 0.0f ? (dx > 0.0f ? 65536.0f : 131072.0f) : (dx > 0.0f ? 0.0f : -65536.0f);
+    float fx = dx, fy = dy;
+    if (dy < 0.0f) {
+        fx = __uint_as_float(f32_bits(dx) ^ 0x80000000u);
+        fy = __uint_as_float(f32_bits(dy) ^ 0x80000000u);
+    }
+    float ndx = fx, ndy = fy;
+    if (fx < 0.0f) {
+        ndx = fy;
+        ndy = -fx;
+    }
+    float slope = __fadd_rn(quadrant, __fdiv_rn(ndy, ndx));
+    uint32_t b = f32_bits(slope);
+    uint32_t s = (uint32_t)((int32_t)b >> 31);
+    return (uint64_t)(b ^ (s | 0x80000000u)) << 32 | (uint32_t)~idx;
+}
+
+// The leaf of the reference's angle sort holding position p of n
+// (fast/quads.c:181-237): cut in four while half the range has more than
+// 5 keys, then in two down to 5 or fewer. Returns start << 8 | length.
+__device__ __forceinline__ uint32_t leaf_of(int64_t n, int64_t p) {
+    int64_t lo = 0, sz = n;
+    while (sz / 2 > 5) {
+        int64_t half = sz / 2, q1 = half / 2, q3 = half + (sz - half) / 2;
+        int64_t r = p - lo;
+        if (r < q1) {
+            sz = q1;
+        } else if (r < half) {
+            lo += q1;
+            sz = half - q1;
+        } else if (r < q3) {
+            lo += half;
+            sz = q3 - half;
+        } else {
+            lo += q3;
+            sz = sz - q3;
+        }
+    }
+    while (sz > 5) {
+        int64_t half = sz / 2;
+        if (p - lo >= half) {
+            lo += half;
+            sz -= half;
+        } else {
+            sz = half;
+        }
+    }
+    return (uint32_t)(lo << 8 | sz);
+}
+
+// The leaf networks of the reference (fast/quads.c:56-85): compare-exchange
+// on the upper 32 bits only.
+__device__ __forceinline__ void leaf_network(uint64_t *k, int n) {
+#define CX(a, b)                                      \
+    if ((k[a] >> 32) > (k[b] >> 32)) {                \
+        uint64_t t_ = k[a];                           \
+        k[a] = k[b];                                  \
+        k[b] = t_;                                    \
+    }
+    if (n == 2) {
+        CX(0, 1)
+    } else if (n == 3) {
+        CX(0, 1) CX(1, 2) CX(0, 1)
+    } else if (n == 4) {
+        CX(0, 1) CX(2, 3) CX(0, 2) CX(1, 3) CX(1, 2)
+    } else if (n == 5) {
+        CX(0, 1) CX(3, 4) CX(1, 2) CX(0, 1) CX(0, 3) CX(2, 4) CX(1, 2) CX(2, 3) CX(1, 2)
+    }
+#undef CX
+}
+
+// Sort (key, val) pairs ascending by key, in place, n items (any n): a
+// bitonic network with every comparator ascending; partners past n act as
+// +infinity and are skipped.
+__device__ void block_sort_pairs(uint64_t *key, uint32_t *val, int64_t n) {
+    int64_t P = 1;
+    while (P < n) P <<= 1;
+    for (int64_t k = 2; k <= P; k <<= 1) {
+        for (int64_t j = k >> 1; j > 0; j >>= 1) {
+            for (int64_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                // comparator t of this step: i < p
+                int64_t i, p;
+                if (j == (k >> 1)) {
+                    int64_t blk = t / j, off = t % j;
+                    i = blk * k + off;
+                    p = blk * k + k - 1 - off;
+                } else {
+                    int64_t blk = t / j, off = t % j;
+                    i = blk * 2 * j + off;
+                    p = i + j;
+                }
+                if (p < n && key[p] < key[i]) {
+                    uint64_t tk = key[i];
+                    key[i] = key[p];
+                    key[p] = tk;
+                    uint32_t tv = val[i];
+                    val[i] = val[p];
+                    val[p] = tv;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+struct MSum {
+    double x, y, xx, xy, yy, w;
+};
+
+struct Moments {
+    const double *mx, *my, *mxx, *mxy, *myy, *mw;
+};
+
+// Moments of sorted points i0..i1, wrapping past the end, summed in the
+// reference's forms (fast/quads.c:539-569, 658-700, 885-921).
+__device__ __forceinline__ MSum seg_moments(const Moments &a, int64_t sz, int64_t i0, int64_t i1) {
+    MSum s;
+    if (i0 <= i1) {
+        s.x = a.mx[i1];
+        s.y = a.my[i1];
+        s.xx = a.mxx[i1];
+        s.xy = a.mxy[i1];
+        s.yy = a.myy[i1];
+        s.w = a.mw[i1];
+        if (i0 > 0) {
+            s.x = s.x - a.mx[i0 - 1];
+            s.y = s.y - a.my[i0 - 1];
+            s.xx = s.xx - a.mxx[i0 - 1];
+            s.xy = s.xy - a.mxy[i0 - 1];
+            s.yy = s.yy - a.myy[i0 - 1];
+            s.w = s.w - a.mw[i0 - 1];
+        }
+    } else {
+        s.x = (a.mx[sz - 1] - a.mx[i0 - 1]) + a.mx[i1];
+        s.y = (a.my[sz - 1] - a.my[i0 - 1]) + a.my[i1];
+        s.xx = (a.mxx[sz - 1] - a.mxx[i0 - 1]) + a.mxx[i1];
+        s.xy = (a.mxy[sz - 1] - a.mxy[i0 - 1]) + a.mxy[i1];
+        s.yy = (a.myy[sz - 1] - a.myy[i0 - 1]) + a.myy[i1];
+        s.w = (a.mw[sz - 1] - a.mw[i0 - 1]) + a.mw[i1];
+    }
+    return s;
+}
+
+// The error of a window of nn points (fast/quads.c:604-653).
+__device__ __forceinline__ double window_error(MSum s, double nn) {
+    double ex = s.x / s.w, ey = s.y / s.w;
+    double cxx = s.xx / s.w - ex * ex;
+    double cxy = s.xy / s.w - ex * ey;
+    double cyy = s.yy / s.w - ey * ey;
+    double d = cxx - cyy;
+    double root = (double)__fsqrt_rn((float)(d * d + 4.0 * (cxy * cxy)));
+    return nn * (0.5 * (cxx + cyy - root));
+}
+
+// The line of the moments: centroid, unit normal, smaller eigenvalue
+// (fast/quads.c:570-600, 756-783).
+__device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
+    double ex = s.x / s.w, ey = s.y / s.w;
+    double cxx = s.xx / s.w - ex * ex;
+    double cxy = s.xy / s.w - ex * ey;
+    double cyy = s.yy / s.w - ey * ey;
+    double root = (double)__fsqrt_rn((float)((cxx - cyy) * (cxx - cyy) + 4.0 * cxy * cxy));
+    double eig_small = 0.5 * (cxx + cyy - root);
+    double eig = 0.5 * (cxx + cyy + root);
+    double nx1 = cxx - eig, ny1 = cxy, m1 = nx1 * nx1 + ny1 * ny1;
+    double nx2 = cxy, ny2 = cyy - eig, m2 = nx2 * nx2 + ny2 * ny2;
+    double nx = nx2, ny = ny2, m = m2;
+    if (m1 > m2) {
+        nx = nx1;
+        ny = ny1;
+        m = m1;
+    }
+    double len = (double)__fsqrt_rn((float)m);
+    lp[0] = ex;
+    lp[1] = ey;
+    lp[2] = 0.0;
+    lp[3] = 0.0;
+    if (!(fabs(len) < 1e-12)) {
+        lp[2] = nx / len;
+        lp[3] = ny / len;
+    }
+    *mse = eig_small;
+}
+
+// The k-th largest (0-based) of v[0..n) by quickselect; v is reordered.
+__device__ double kth_largest(double *v, int64_t n, int64_t k) {
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        double pivot = v[(lo + hi) / 2];
+        int64_t i = lo, j = hi;
+        while (i <= j) {
+            while (v[i] > pivot) i++;
+            while (v[j] < pivot) j--;
+            if (i <= j) {
+                double t = v[i];
+                v[i] = v[j];
+                v[j] = t;
+                i++;
+                j--;
+            }
+        }
+        if (k <= j)
+            hi = j;
+        else if (k >= i)
+            lo = i;
+        else
+            break;
+    }
+    return v[k];
+}
+
+#define FIT_SORT_CAP 2048
+
+__global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *frames, GpuParams prm,
+                                                                 const uint8_t *qim, const uint64_t *pts,
+                                                                 const uint32_t *cstart, const int32_t *cframe,
+                                                                 int64_t nclusters, int64_t npoints, FitScratch scr,
+                                                                 GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
+    __shared__ uint64_t s_key[FIT_SORT_CAP];
+    __shared__ uint32_t s_val[FIT_SORT_CAP];
+    __shared__ float s_lane[8];
+    __shared__ int s_rev;
+    __shared__ uint32_t s_bb[4][AT_FIT_THREADS / 32];
+    __shared__ uint32_t s_scan[32];
+    __shared__ int64_t s_nm;
+    __shared__ int s_ok;
+    __shared__ double s_perr[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pmse[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA],
+        s_pnx[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pny[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA];
+    const int tid = threadIdx.x;
+
+    for (int64_t c = blockIdx.x; c < nclusters; c += gridDim.x) {
+        const int64_t s0 = cstart[c];
+        const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
+        const FrameDesc f = frames[cframe[c]];
+        if (tid == 0) quad_ok[c] = 0;
+        if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
+        if (sz > 65535) {
+            if (tid == 0) atomicOr(err, AT_ERR_CLUSTER_TOO_BIG);
+            continue;
+        }
+        const uint64_t *P = pts + s0;
+        // bounding box (fast/quads.c:515-528)
+        uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
+        for (int64_t i = tid; i < sz; i += blockDim.x) {
+            uint32_t x = (uint32_t)(P[i] & 0xffff), y = (uint32_t)(P[i] >> 16 & 0xffff);
+            xmin = min(xmin, x);
+            xmax = max(xmax, x);
+            ymin = min(ymin, y);
+            ymax = max(ymax, y);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+            xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+            ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+            ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+        }
+        __syncthreads();
+        if ((tid & 31) == 0) {
+            s_bb[0][tid >> 5] = xmin;
+            s_bb[1][tid >> 5] = xmax;
+            s_bb[2][tid >> 5] = ymin;
+            s_bb[3][tid >> 5] = ymax;
+        }
+        __syncthreads();
+        for (int w = 0; w < AT_FIT_THREADS / 32; w++) {
+            xmin = min(xmin, s_bb[0][w]);
+            xmax = max(xmax, s_bb[1][w]);
+            ymin = min(ymin, s_bb[2][w]);
+            ymax = max(ymax, s_bb[3][w]);
+        }
+        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < prm.tag_width) continue;
+        const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
+        const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
+
+        // angle keys, and the dot product of offsets and gradients: 8 lanes
+        // over the whole groups of 8, then the rest (fast/quads.c:467-512)
+        uint64_t *keys = scr.keys + s0;
+        for (int64_t i = tid; i < sz; i += blockDim.x) {
+            float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
+            keys[i] = angle_key(dx, dy, (uint32_t)i);
+        }
+        const int64_t nv = sz - sz % 8;
+        if (tid < 8) {
+            float acc = 0.0f;
+            for (int64_t i = tid; i < nv; i += 8) {
+                float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
+                float gx = (float)(int16_t)(P[i] >> 32 & 0xffff), gy = (float)(int16_t)(P[i] >> 48);
+                acc = __fadd_rn(acc, __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy)));
+            }
+            s_lane[tid] = acc;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float dot = __fadd_rn(__fadd_rn(__fadd_rn(s_lane[0], s_lane[4]), __fadd_rn(s_lane[2], s_lane[6])),
+                                  __fadd_rn(__fadd_rn(s_lane[1], s_lane[5]), __fadd_rn(s_lane[3], s_lane[7])));
+            for (int64_t i = nv; i < sz; i++) {
+                float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
+                float gx = (float)(int16_t)(P[i] >> 32 & 0xffff), gy = (float)(int16_t)(P[i] >> 48);
+                dot = __fadd_rn(dot, __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy)));
+            }
+            int rev = dot < 0.0f;
+            int ok = 1;
+            if (!prm.reversed_border && rev) ok = 0;
+            if (!prm.normal_border && !rev) ok = 0;
+            s_ok = ok;
+            s_rev = rev;
+        }
+        __syncthreads();
+        if (!s_ok) continue;
+        const int rev = s_rev;
+
+        // The angle sort. The reference's merge sort keeps each leaf's
+        // "blocks" (a key larger than all before it in the leaf's network
+        // order, and the smaller keys after it) together and orders them by
+        // their first key. So: per leaf, the network order, each key's
+        // block head and its place in the leaf; then one sort by (head,
+        // place), packed into 64 bits as head's slope bits, 0xffff - head's
+        // index, and the place.
+        const bool in_smem = sz <= FIT_SORT_CAP;
+        uint64_t *sk = in_smem ? s_key : scr.skey + s0;
+        uint32_t *sv = in_smem ? s_val : scr.sval + s0;
+        for (int64_t p = tid; p < sz; p += blockDim.x) {
+            uint32_t lf = leaf_of(sz, p);
+            int64_t lo = lf >> 8, len = lf & 255;
+            if (p != lo) continue;
+            uint64_t k5[5];
+            for (int t = 0; t < len; t++) k5[t] = keys[lo + t];
+            leaf_network(k5, (int)len);
+            uint64_t head = 0;
+            for (int t = 0; t < len; t++) {
+                if (t == 0 || k5[t] > head) head = k5[t];
+                uint32_t hidx = ~(uint32_t)head;
+                sk[lo + t] = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 3 | (uint64_t)t;
+                sv[lo + t] = ~(uint32_t)k5[t];
+            }
+        }
+        __syncthreads();
+        block_sort_pairs(sk, sv, sz);
+
+        // cumulative weighted moments in angle order (fast/quads.c:968-1035):
+        // w = sqrt(gx^2 + gy^2) + 1 on the quad image, 1 at its border
+        double *wb = scr.w + s0, *fxb = scr.fx + s0, *fyb = scr.fy + s0;
+        const uint8_t *im = qim + f.q_off;
+        for (int64_t k = tid; k < sz; k += blockDim.x) {
+            uint32_t src = sv[k];
+            int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
+            int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
+            int32_t g2 = 0;
+            if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
+                int64_t cc = (int64_t)iy * f.qw + ix;
+                int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
+                int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
+                g2 = gx * gx + gy * gy;
+            }
+            wb[k] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
+            fxb[k] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
+            fyb[k] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+        }
+        __syncthreads();
+        double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
+        if (tid < 6) {
+            double s = 0.0;
+            double *out = M[tid];
+            for (int64_t k = 0; k < sz; k++) {
+                double w = wb[k], fx = fxb[k], fy = fyb[k], v;
+                switch (tid) {
+                case 0: v = __dmul_rn(w, fx); break;
+                case 1: v = __dmul_rn(w, fy); break;
+                case 2: v = __dmul_rn(__dmul_rn(w, fx), fx); break;
+                case 3: v = __dmul_rn(__dmul_rn(w, fx), fy); break;
+                case 4: v = __dmul_rn(__dmul_rn(w, fy), fy); break;
+                default: v = w; break;
+                }
+                s = __dadd_rn(s, v);
+                out[k] = s;
+            }
+        }
+        __syncthreads();
+        const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
+
+        // corner search (fast/quads.c:788-959)
+        const int64_t ksz = dmin(20, sz / 12);
+        if (ksz < 2) continue;
+        const double nn = (double)(2 * ksz + 1);
+        double *errs = scr.errs + s0, *filt = scr.filt + s0;
+        for (int64_t i = tid; i < sz; i += blockDim.x) {
+            int64_t i0 = i - ksz, i1 = i + ksz;
+            MSum s;
+            if (i0 < 0)
+                s = seg_moments(mo, sz, i0 + sz, i1);
+            else if (i1 < sz)
+                s = seg_moments(mo, sz, i0, i1);
+            else
+                s = seg_moments(mo, sz, i0, i1 - sz);
+            errs[i] = window_error(s, nn);
+        }
+        __syncthreads();
+        for (int64_t i = tid; i < sz; i += blockDim.x) {
+            double acc;
+            if (i >= 3 && i < sz - 3) {
+                acc = errs[i - 3] * prm.qsm[0];
+                for (int t = 1; t < 7; t++) acc = acc + errs[i - 3 + t] * prm.qsm[t];
+            } else {
+                acc = 0.0;
+                for (int t = 0; t < 7; t++) {
+                    int64_t j = i - 3 + t;
+                    if (j < 0) j += sz;
+                    if (j >= sz) j -= sz;
+                    acc = acc + errs[j] * prm.qsm[t];
+                }
+            }
+            filt[i] = acc;
+        }
+        __syncthreads();
+        // local maxima with wrap-around, compacted in index order
+        int32_t *mxi = scr.mxi + s0;
+        double *mxe = scr.mxe + s0;
+        int64_t nm_run = 0;
+        for (int64_t i0 = 0; i0 < sz; i0 += blockDim.x) {
+            int64_t i = i0 + tid;
+            uint32_t is_max = 0;
+            double e = 0.0;
+            if (i < sz) {
+                e = filt[i];
+                double l = filt[i == 0 ? sz - 1 : i - 1], r = filt[i + 1 == sz ? 0 : i + 1];
+                is_max = e > l && e > r;
+            }
+            uint32_t total;
+            uint32_t off = block_excl_scan(is_max, &total, s_scan);
+            if (is_max) {
+                mxi[nm_run + off] = (int32_t)i;
+                mxe[nm_run + off] = e;
+            }
+            nm_run += total;
+        }
+        __syncthreads();
+        int64_t nm = nm_run;
+        if (nm < 4) continue;
+        if (nm > prm.max_nmaxima) {
+            if (tid == 0) {
+                double *sel = filt;  // free now: a copy of the maxima's errors
+                for (int64_t i = 0; i < nm; i++) sel[i] = mxe[i];
+                double thresh = kth_largest(sel, nm, prm.max_nmaxima);
+                int64_t o = 0;
+                for (int64_t i = 0; i < nm; i++)
+                    if (mxe[i] > thresh) mxi[o++] = mxi[i];
+                s_nm = o;
+            }
+            __syncthreads();
+            nm = s_nm;
+        }
+        // line fits of pairs of maxima: (a, b), a < b, and the closing pair
+        // (b, a) wrapping around for b >= a + 3
+        for (int64_t t = tid; t < nm * nm; t += blockDim.x) {
+            int64_t p = t / nm, q = t - p * nm;
+            bool used = p < q || p >= q + 3;
+            if (!used) continue;
+            int64_t i0 = mxi[p], i1 = mxi[q];
+            MSum s = seg_moments(mo, sz, i0, i1);
+            double n = (double)(i0 <= i1 ? i1 - i0 + 1 : sz - i0 + i1 + 1);
+            double lp[4], mse;
+            line_of(s, lp, &mse);
+            s_perr[t] = n * mse;
+            s_pmse[t] = mse;
+            s_pnx[t] = lp[2];
+            s_pny[t] = lp[3];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const double inf = __longlong_as_double(0x7ff0000000000000ll);
+            double best = inf;
+            int64_t bi[4] = {0, 0, 0, 0};
+            for (int64_t m0 = 0; m0 < nm - 3; m0++)
+                for (int64_t m1 = m0 + 1; m1 < nm - 2; m1++) {
+                    int64_t p01 = m0 * nm + m1;
+                    if (s_pmse[p01] > prm.max_mse) continue;
+                    for (int64_t m2 = m1 + 1; m2 < nm - 1; m2++) {
+                        int64_t p12 = m1 * nm + m2;
+                        if (s_pmse[p12] > prm.max_mse) continue;
+                        double dot = s_pnx[p01] * s_pnx[p12] + s_pny[p01] * s_pny[p12];
+                        if (fabs(dot) > prm.max_dot) continue;
+                        double e012 = s_perr[p01] + s_perr[p12];
+                        for (int64_t m3 = m2 + 1; m3 < nm; m3++) {
+                            int64_t p23 = m2 * nm + m3, p30 = m3 * nm + m0;
+                            double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
+                            double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
+                            double e = e012 + e23 + e30;
+                            if (e < best) {
+                                best = e;
+                                bi[0] = mxi[m0];
+                                bi[1] = mxi[m1];
+                                bi[2] = mxi[m2];
+                                bi[3] = mxi[m3];
+                            }
+                        }
+                    }
+                }
+            bool ok = best != inf && best / (double)sz < prm.max_mse;
+            GpuQuad q;
+            q.reversed_border = rev;
+            q.frame = cframe[c];
+            double lines[4][4];
+            for (int i = 0; ok && i < 4; i++) {
+                double mse;
+                line_of(seg_moments(mo, sz, bi[i], bi[(i + 1) & 3]), lines[i], &mse);
+                if (mse > prm.max_mse) ok = false;
+            }
+            for (int i = 0; ok && i < 4; i++) {
+                int j = (i + 1) & 3;
+                double a00 = lines[i][3], a01 = -lines[j][3], a10 = -lines[i][2], a11 = lines[j][2];
+                double b0 = -lines[i][0] + lines[j][0], b1 = -lines[i][1] + lines[j][1];
+                double det = a00 * a11 - a10 * a01;
+                if (fabs(det) < 0.001) {
+                    ok = false;
+                    break;
+                }
+                double w00 = a11 / det, w01 = -a01 / det;
+                double l0 = w00 * b0 + w01 * b1;
+                q.p[i][0] = (float)(lines[i][0] + l0 * a00);
+                q.p[i][1] = (float)(lines[i][1] + l0 * a10);
+            }
+            if (ok) {
+                // area of triangles (0,1,2) and (2,3,0) by Heron (quads.c:1094-1110)
+                const int tri[2][4] = {{0, 1, 2, 0}, {2, 3, 0, 2}};
+                double area = 0.0;
+                for (int t = 0; t < 2; t++) {
+                    double len[3];
+                    for (int i = 0; i < 3; i++) {
+                        int ia = tri[t][i], ib = tri[t][i + 1];
+                        double ddx = (double)__fsub_rn(q.p[ib][0], q.p[ia][0]);
+                        double ddy = (double)__fsub_rn(q.p[ib][1], q.p[ia][1]);
+                        len[i] = sqrt(ddx * ddx + ddy * ddy);
+                    }
+                    double pp = (len[0] + len[1] + len[2]) / 2.0;
+                    area = area + sqrt(pp * (pp - len[0]) * (pp - len[1]) * (pp - len[2]));
+                }
+                if (area < 0.95 * (double)prm.tag_width * (double)prm.tag_width) ok = false;
+            }
+            for (int i = 0; ok && i < 4; i++) {
+                // convexity (quads.c:1112-1124)
+                int i0 = i, i1 = (i + 1) & 3, i2 = (i + 2) & 3;
+                double dx1 = (double)__fsub_rn(q.p[i1][0], q.p[i0][0]), dy1 = (double)__fsub_rn(q.p[i1][1], q.p[i0][1]);
+                double dx2 = (double)__fsub_rn(q.p[i2][0], q.p[i1][0]), dy2 = (double)__fsub_rn(q.p[i2][1], q.p[i1][1]);
+                double den = sqrt((dx1 * dx1 + dy1 * dy1) * (dx2 * dx2 + dy2 * dy2));
+                if (den == 0.0) {
+                    ok = false;
+                    break;
+                }
+                double cs = (dx1 * dx2 + dy1 * dy2) / den;
+                if ((cs > prm.max_dot || cs < -prm.max_dot) || dx1 * dy2 < dy1 * dx2) ok = false;
+            }
+            if (ok) {
+                quads[c] = q;
+                quad_ok[c] = 1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 9. Decoding, one block per quad (fast/decode.c, fast/detector.c:83-139).
+
+struct DView {
+    const uint8_t *im;
+    int64_t s, w, h;
+};
+
+__device__ __forceinline__ double bil_pair(double a, double b, const uint8_t *p, int64_t s) {
+    double na = 1.0 - a, nb = 1.0 - b;
+    return ((na * nb) * p[0] + (a * nb) * p[1]) + ((na * b) * p[s] + (a * b) * p[s + 1]);
+}
+__device__ __forceinline__ double bil_seq(double a, double b, const uint8_t *p, int64_t s) {
+    return (1.0 - a) * (1.0 - b) * p[0] + a * (1.0 - b) * p[1] + (1.0 - a) * b * p[s] + a * b * p[s + 1];
+}
+
+// One sample point of edge refinement (fast/decode.c:549-735): the
+// weighted mean step n0 along the normal, or false when no step counts.
+__device__ bool refine_sample(const DView &v, double x0, double y0, double nx, double ny, int64_t range,
+                              int64_t vsteps, int64_t nsteps, double *n0) {
+    const double wl = (double)(v.w - 1), hl = (double)(v.h - 1);
+    double ln[4] = {0.0, 0.0, 0.0, 0.0}, lc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t k = 0; k < vsteps; k++) {
+        double n = (double)-range + 0.25 * (double)k;
+        double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
+        double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
+        double wgt = 0.0;
+        if (x1 > -1.0 && x1 < wl && y1 > -1.0 && y1 < hl && x2 > -1.0 && x2 < wl && y2 > -1.0 && y2 < hl) {
+            double tx1 = trunc(x1), ty1 = trunc(y1), tx2 = trunc(x2), ty2 = trunc(y2);
+            double g1 = bil_pair(x1 - tx1, y1 - ty1, v.im + (int64_t)ty1 * v.s + (int64_t)tx1, v.s);
+            double g2 = bil_pair(x2 - tx2, y2 - ty2, v.im + (int64_t)ty2 * v.s + (int64_t)tx2, v.s);
+            double d = g2 - g1;
+            wgt = !(g1 < g2) ? d * d : 0.0;
+        }
+        ln[k & 3] = ln[k & 3] + wgt * n;
+        lc[k & 3] = lc[k & 3] + wgt;
+    }
+    double mn = 0.0 + ((ln[0] + ln[2]) + (ln[1] + ln[3]));
+    double mc = 0.0 + ((lc[0] + lc[2]) + (lc[1] + lc[3]));
+    for (int64_t k = vsteps; k < nsteps; k++) {
+        double n = (double)-range + 0.25 * (double)k;
+        double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
+        int64_t x1i = c_int(x1), y1i = c_int(y1);
+        if (x1i < 0 || x1i + 1 >= v.w || y1i < 0 || y1i + 1 >= v.h) continue;
+        double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
+        int64_t x2i = c_int(x2), y2i = c_int(y2);
+        if (x2i < 0 || x2i + 1 >= v.w || y2i < 0 || y2i + 1 >= v.h) continue;
+        double g1 = bil_seq(x1 - (double)x1i, y1 - (double)y1i, v.im + y1i * v.s + x1i, v.s);
+        double g2 = bil_seq(x2 - (double)x2i, y2 - (double)y2i, v.im + y2i * v.s + x2i, v.s);
+        if (g1 < g2) continue;
+        double wgt = (g2 - g1) * (g2 - g1);
+        mn = mn + wgt * n;
+        mc = mc + wgt;
+    }
+    if (mc == 0.0) return false;
+    *n0 = mn / mc;
+    return true;
+}
+
+// Correctly rounded f32 trig as the golden vectors need: the double
+// function, then one rounding (fast/decode.c:740-744).
+__device__ __forceinline__ float cr_atan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
+__device__ __forceinline__ float cr_cosf(float x) { return (float)cos((double)x); }
+__device__ __forceinline__ float cr_sinf(float x) { return (float)sin((double)x); }
+
+// Homography of 4 correspondences: 8x9 Gaussian elimination with partial
+// pivoting (fast/decode.c:114-165).
+__device__ bool homography(const double c[4][4], double H[9]) {
+    double a[8][9];
+    for (int r = 0; r < 8; r++)
+        for (int i = 0; i < 9; i++) a[r][i] = 0.0;
+    for (int i = 0; i < 4; i++) {
+        double x = c[i][0], y = c[i][1], X = c[i][2], Y = c[i][3];
+        a[2 * i][0] = x;
+        a[2 * i][1] = y;
+        a[2 * i][2] = 1.0;
+        a[2 * i][6] = -x * X;
+        a[2 * i][7] = -y * X;
+        a[2 * i][8] = X;
+        a[2 * i + 1][3] = x;
+        a[2 * i + 1][4] = y;
+        a[2 * i + 1][5] = 1.0;
+        a[2 * i + 1][6] = -x * Y;
+        a[2 * i + 1][7] = -y * Y;
+        a[2 * i + 1][8] = Y;
+    }
+    for (int col = 0; col < 8; col++) {
+        double best = 0.0;
+        int piv = -1;
+        for (int r = col; r < 8; r++)
+            if (fabs(a[r][col]) > best) {
+                best = fabs(a[r][col]);
+                piv = r;
+            }
+        if (piv < 0 || best < 1e-10) return false;
+        if (piv != col)
+            for (int i = col; i < 9; i++) {
+                double t = a[col][i];
+                a[col][i] = a[piv][i];
+                a[piv][i] = t;
+            }
+        for (int r = col + 1; r < 8; r++) {
+            double fct = a[r][col] / a[col][col];
+            a[r][col] = 0.0;
+            for (int i = col + 1; i < 9; i++) a[r][i] = a[r][i] - fct * a[col][i];
+        }
+    }
+    for (int col = 7; col >= 0; col--) {
+        double s = 0.0;
+        for (int i = col + 1; i < 8; i++) s = s + a[col][i] * a[i][8];
+        a[col][8] = (a[col][8] - s) / a[col][col];
+    }
+    for (int i = 0; i < 8; i++) H[i] = a[i][8];
+    H[8] = 1.0;
+    return true;
+}
+
+// Invertibility as the C library's PLU decomposition decides it
+// (fast/decode.c:168-196).
+__device__ bool invertible3(const double m[9]) {
+    double lu[9];
+    for (int i = 0; i < 9; i++) lu[i] = m[i];
+    for (int j = 0; j < 3; j++) {
+        for (int i = 0; i < 3; i++) {
+            int kmax = i < j ? i : j;
+            double acc = 0.0;
+            for (int k = 0; k < kmax; k++) acc = acc + lu[i * 3 + k] * lu[k * 3 + j];
+            lu[i * 3 + j] = lu[i * 3 + j] - acc;
+        }
+        int p = j;
+        for (int i = j + 1; i < 3; i++)
+            if (fabs(lu[i * 3 + j]) > fabs(lu[p * 3 + j])) p = i;
+        if (p != j)
+            for (int k = 0; k < 3; k++) {
+                double t = lu[p * 3 + k];
+                lu[p * 3 + k] = lu[j * 3 + k];
+                lu[j * 3 + k] = t;
+            }
+        double d = lu[j * 3 + j];
+        if (fabs(d) < 1e-8) return false;
+        if (d != 0.0) {
+            double inv = 1.0 / d;
+            for (int i = j + 1; i < 3; i++) lu[i * 3 + j] = lu[i * 3 + j] * inv;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void project(const double H[9], double x, double y, double *ox, double *oy) {
+    double xx = H[0] * x + H[1] * y + H[2];
+    double yy = H[3] * x + H[4] * y + H[5];
+    double zz = H[6] * x + H[7] * y + H[8];
+    *ox = xx / zz;
+    *oy = yy / zz;
+}
+
+struct GrayModel {
+    double a[9], b[3], c[3];
+};
+
+// mat33_sym_solve as the C library does it (fast/decode.c:241-265).
+__device__ void gm_solve(GrayModel *g) {
+    const double *a = g->a;
+    double L0 = sqrt(a[0]);
+    double L3 = a[1] / L0;
+    double L6 = a[2] / L0;
+    double L4 = sqrt(a[4] - L3 * L3);
+    double L7 = (a[5] - L3 * L6) / L4;
+    double L8 = sqrt(a[8] - L6 * L6 - L7 * L7);
+    double M0 = 1.0 / L0;
+    double M3 = -L3 * M0 / L4;
+    double M4 = 1.0 / L4;
+    double M6 = (-L6 * M0 - L7 * M3) / L8;
+    double M7 = -L7 * M4 / L8;
+    double M8 = 1.0 / L8;
+    const double *b = g->b;
+    double t0 = M0 * b[0];
+    double t1 = M3 * b[0] + M4 * b[1];
+    double t2 = M6 * b[0] + M7 * b[1] + M8 * b[2];
+    g->c[0] = M0 * t0 + M3 * t1 + M6 * t2;
+    g->c[1] = M4 * t1 + M7 * t2;
+    g->c[2] = M8 * t2;
+}
+
+__device__ __forceinline__ double bilinear_at(const DView &v, double px, double py) {
+    int64_t x1 = c_int(floor(px - 0.5)), x2 = c_int(ceil(px - 0.5));
+    double x = px - 0.5 - (double)x1;
+    int64_t y1 = c_int(floor(py - 0.5)), y2 = c_int(ceil(py - 0.5));
+    double y = py - 0.5 - (double)y1;
+    if (x1 < 0 || x2 >= v.w || y1 < 0 || y2 >= v.h) return -1.0;
+    const uint8_t *r1 = v.im + y1 * v.s, *r2 = v.im + y2 * v.s;
+    return r1[x1] * (1.0 - x) * (1.0 - y) + r1[x2] * x * (1.0 - y) + r2[x1] * (1.0 - x) * y + r2[x2] * x * y;
+}
+
+__device__ __forceinline__ uint64_t rot90(uint64_t w0, int64_t nbits) {
+    int64_t p = nbits, l = 0;
+    if (nbits % 4 == 1) {
+        p = nbits - 1;
+        l = 1;
+    }
+    uint64_t w = ((w0 >> l) << (p / 4 + l)) | (w0 >> (3 * p / 4 + l) << l) | (w0 & (uint64_t)l);
+    return w & ((nbits >= 64) ? ~0ull : (((uint64_t)1 << nbits) - 1));
+}
+
+// The first code within maxham bits, by rotation, then chunk, then code
+// index (fast/decode.c:87-107). Returns id | hamming << 16 | rot << 24.
+__device__ uint32_t qd_lookup(const GpuFamily &F, uint64_t rcode) {
+    uint64_t mask = (uint64_t)F.cap - 1;
+    for (int r = 0; r < 4; r++) {
+        for (int j = 0; j < 4; j++) {
+            int64_t val = (int64_t)((rcode >> (j * F.chunk)) & mask);
+            int64_t ob = j * (F.cap + 1) + val;
+            int64_t base = j * F.ncodes;
+            for (int64_t e = base + F.off[ob]; e < base + F.off[ob + 1]; e++) {
+                int hd = __popcll(F.codes[e] ^ rcode);
+                if (hd <= F.maxham) return (uint32_t)F.idx[e] | (uint32_t)hd << 16 | (uint32_t)r << 24;
+            }
+        }
+        rcode = rot90(rcode, F.nbits);
+    }
+    return 65535u | 255u << 16;
+}
+
+__global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *frames, GpuParams prm,
+                                                              const GpuFamily *fams, const uint8_t *img,
+                                                              const uint8_t *qim, const GpuQuad *quads,
+                                                              int64_t nquads, GpuDetection *dets, uint32_t *det_ok) {
+    __shared__ float s_p[4][2];
+    __shared__ double s_lines[4][4];
+    __shared__ double s_bx[AT_DEC_THREADS], s_by[AT_DEC_THREADS];
+    __shared__ int s_bok[AT_DEC_THREADS];
+    __shared__ double s_H[9];
+    __shared__ int s_hok;
+    __shared__ double s_gx[8 * AT_MAX_TW], s_gy[8 * AT_MAX_TW], s_gv[8 * AT_MAX_TW];
+    __shared__ int s_gk[8 * AT_MAX_TW];
+    __shared__ double s_wc[3], s_bc[3];
+    __shared__ int s_pol;
+    __shared__ double s_vals[AT_MAX_TW * AT_MAX_TW], s_sharp[AT_MAX_TW * AT_MAX_TW];
+    const int tid = threadIdx.x;
+    for (int64_t qi = blockIdx.x; qi < nquads; qi += gridDim.x) {
+        const GpuQuad q = quads[qi];
+        const FrameDesc f = frames[q.frame];
+        DView v;
+        if (prm.decode_blurred)
+            v = DView{qim + f.q_off, (int64_t)f.qw, (int64_t)f.qw, (int64_t)f.qh};
+        else
+            v = DView{img + f.img_off, (int64_t)f.w, (int64_t)f.w, (int64_t)f.h};
+        if (tid < 8) {
+            float val = q.p[tid >> 1][tid & 1];
+            if (prm.quad_decimate > 1.0f) val = __fmul_rn(val, prm.quad_decimate);
+            s_p[tid >> 1][tid & 1] = val;
+        }
+        for (int fi = tid; fi < prm.nfam; fi += blockDim.x) det_ok[qi * prm.nfam + fi] = 0;
+        __syncthreads();
+        if (prm.refine_edges) {
+            // fast/decode.c:657-761
+            const int64_t range = (int64_t)__fadd_rn(prm.quad_decimate, 1.0f);
+            const int64_t nsteps = 2 * 4 * range + 1;
+            const int64_t vsteps = nsteps - nsteps % 4;
+            for (int edge = 0; edge < 4; edge++) {
+                int a = edge, b = (edge + 1) & 3;
+                double nx = (double)__fsub_rn(s_p[b][1], s_p[a][1]);
+                double ny = (double)__fadd_rn(-s_p[b][0], s_p[a][0]);
+                double mag = sqrt(nx * nx + ny * ny);
+                nx = nx / mag;
+                ny = ny / mag;
+                if (q.reversed_border) {
+                    nx = -nx;
+                    ny = -ny;
+                }
+                int64_t nsamples = dmax(16, c_int(mag / 8.0));
+                double mx = 0.0, my = 0.0, mxx = 0.0, mxy = 0.0, myy = 0.0, cnt = 0.0;
+                for (int64_t s0 = 0; s0 < nsamples; s0 += blockDim.x) {
+                    int64_t si = s0 + tid;
+                    if (si < nsamples) {
+                        double alpha = (1.0 + (double)si) / (double)(nsamples + 1);
+                        double x0 = alpha * (double)s_p[a][0] + (1.0 - alpha) * (double)s_p[b][0];
+                        double y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
+                        double n0;
+                        bool ok = refine_sample(v, x0, y0, nx, ny, range, vsteps, nsteps, &n0);
+                        s_bok[tid] = ok;
+                        if (ok) {
+                            s_bx[tid] = x0 + n0 * nx;
+                            s_by[tid] = y0 + n0 * ny;
+                        }
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        int64_t m = dmin((int64_t)blockDim.x, nsamples - s0);
+                        for (int64_t t = 0; t < m; t++) {
+                            if (!s_bok[t]) continue;
+                            double bx = s_bx[t], by = s_by[t];
+                            mx = mx + bx;
+                            my = my + by;
+                            mxx = mxx + bx * bx;
+                            mxy = mxy + bx * by;
+                            myy = myy + by * by;
+                            cnt = cnt + 1.0;
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (tid == 0) {
+                    double ex = mx / cnt, ey = my / cnt;
+                    double cxx = mxx / cnt - ex * ex, cxy = mxy / cnt - ex * ey, cyy = myy / cnt - ey * ey;
+                    double theta = 0.5 * (double)cr_atan2f((float)(-2.0 * cxy), (float)(cyy - cxx));
+                    s_lines[edge][0] = ex;
+                    s_lines[edge][1] = ey;
+                    s_lines[edge][2] = (double)cr_cosf((float)theta);
+                    s_lines[edge][3] = (double)cr_sinf((float)theta);
+                }
+            }
+            if (tid == 0) {
+                for (int i = 0; i < 4; i++) {
+                    int j = (i + 1) & 3;
+                    double a00 = s_lines[i][3], a01 = -s_lines[j][3], a10 = -s_lines[i][2], a11 = s_lines[j][2];
+                    double b0 = -s_lines[i][0] + s_lines[j][0], b1 = -s_lines[i][1] + s_lines[j][1];
+                    double det = a00 * a11 - a10 * a01;
+                    if (fabs(det) > 0.001) {
+                        double w00 = a11 / det, w01 = -a01 / det;
+                        double l0 = w00 * b0 + w01 * b1;
+                        s_p[j][0] = (float)(s_lines[i][0] + l0 * a00);
+                        s_p[j][1] = (float)(s_lines[i][1] + l0 * a10);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            double corr[4][4];
+            for (int i = 0; i < 4; i++) {
+                corr[i][0] = i == 0 || i == 3 ? -1.0 : 1.0;
+                corr[i][1] = i == 0 || i == 1 ? -1.0 : 1.0;
+                corr[i][2] = s_p[i][0];
+                corr[i][3] = s_p[i][1];
+            }
+            double H[9];
+            s_hok = homography(corr, H) && invertible3(H);
+            for (int i = 0; i < 9; i++) s_H[i] = H[i];
+        }
+        __syncthreads();
+        if (!s_hok) continue;
+        for (int fi = 0; fi < prm.nfam; fi++) {
+            const GpuFamily &F = fams[fi];
+            if (F.reversed_border != q.reversed_border) continue;
+            if (!(f.fam_mask >> fi & 1u)) continue;
+            // border gray models (fast/decode.c:291-337): 8 patterns x wab
+            const int32_t wab = F.wab;
+            const float wf = (float)wab;
+            for (int t = tid; t < 8 * wab; t += blockDim.x) {
+                int pi = t / wab, i = t - pi * wab;
+                float pat[5];
+                switch (pi) {
+                case 0: pat[0] = -0.5f, pat[1] = 0.5f, pat[2] = 0.0f, pat[3] = 1.0f; break;
+                case 1: pat[0] = 0.5f, pat[1] = 0.5f, pat[2] = 0.0f, pat[3] = 1.0f; break;
+                case 2: pat[0] = (float)(wab + 0.5), pat[1] = 0.5f, pat[2] = 0.0f, pat[3] = 1.0f; break;
+                case 3: pat[0] = (float)(wab - 0.5), pat[1] = 0.5f, pat[2] = 0.0f, pat[3] = 1.0f; break;
+                case 4: pat[0] = 0.5f, pat[1] = -0.5f, pat[2] = 1.0f, pat[3] = 0.0f; break;
+                case 5: pat[0] = 0.5f, pat[1] = 0.5f, pat[2] = 1.0f, pat[3] = 0.0f; break;
+                case 6: pat[0] = 0.5f, pat[1] = (float)(wab + 0.5), pat[2] = 1.0f, pat[3] = 0.0f; break;
+                default: pat[0] = 0.5f, pat[1] = (float)(wab - 0.5), pat[2] = 1.0f, pat[3] = 0.0f; break;
+                }
+                double tx01 = (double)__fdiv_rn(__fadd_rn(pat[0], __fmul_rn((float)i, pat[2])), wf);
+                double ty01 = (double)__fdiv_rn(__fadd_rn(pat[1], __fmul_rn((float)i, pat[3])), wf);
+                double tx = 2.0 * (tx01 - 0.5), ty = 2.0 * (ty01 - 0.5);
+                double zz = s_H[6] * tx + s_H[7] * ty + s_H[8];
+                double px = (s_H[0] * tx + s_H[1] * ty + s_H[2]) / zz;
+                double py = (s_H[3] * tx + s_H[4] * ty + s_H[5]) / zz;
+                int64_t ix = c_int(px), iy = c_int(py);
+                int keep = !(ix < 0 || iy < 0 || ix >= v.w || iy >= v.h);
+                s_gk[t] = keep;
+                s_gx[t] = tx;
+                s_gy[t] = ty;
+                s_gv[t] = keep ? (double)v.im[iy * v.s + ix] : 0.0;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                GrayModel gm[2];
+                for (int g = 0; g < 2; g++) {
+                    for (int i = 0; i < 9; i++) gm[g].a[i] = 0.0;
+                    for (int i = 0; i < 3; i++) gm[g].b[i] = 0.0;
+                }
+                for (int t = 0; t < 8 * wab; t++) {
+                    if (!s_gk[t]) continue;
+                    int pi = t / wab;
+                    GrayModel *g = &gm[(pi & 1) ? 1 : 0];  // even patterns white
+                    double x = s_gx[t], y = s_gy[t], val = s_gv[t];
+                    g->a[0] = g->a[0] + x * x;
+                    g->a[1] = g->a[1] + x * y;
+                    g->a[2] = g->a[2] + x;
+                    g->a[4] = g->a[4] + y * y;
+                    g->a[5] = g->a[5] + y;
+                    g->a[8] = g->a[8] + 1.0;
+                    g->b[0] = g->b[0] + x * val;
+                    g->b[1] = g->b[1] + y * val;
+                    g->b[2] = g->b[2] + val;
+                }
+                gm_solve(&gm[0]);
+                if (wab > 1) {
+                    gm_solve(&gm[1]);
+                } else {
+                    gm[1].c[0] = 0.0;
+                    gm[1].c[1] = 0.0;
+                    gm[1].c[2] = gm[1].b[2] / 4.0;
+                }
+                double wi = gm[0].c[0] * 0.0 + gm[0].c[1] * 0.0 + gm[0].c[2];
+                double bi = gm[1].c[0] * 0.0 + gm[1].c[1] * 0.0 + gm[1].c[2];
+                s_pol = (wi - bi < 0.0) == (F.reversed_border != 0);
+                for (int i = 0; i < 3; i++) {
+                    s_wc[i] = gm[0].c[i];
+                    s_bc[i] = gm[1].c[i];
+                }
+            }
+            __syncthreads();
+            if (!s_pol) continue;
+            // bit values less the local threshold, sharpened (decode.c:340-377)
+            const int64_t tw = F.tw;
+            const int64_t minc = (wab - tw) / 2;
+            for (int64_t t = tid; t < tw * tw; t += blockDim.x) s_vals[t] = 0.0;
+            __syncthreads();
+            for (int64_t i = tid; i < F.nbits; i += blockDim.x) {
+                int64_t bx = F.bit_x[i], by = F.bit_y[i];
+                double tx = 2.0 * (((double)bx + 0.5) / wab - 0.5), ty = 2.0 * (((double)by + 0.5) / wab - 0.5);
+                double zz = s_H[6] * tx + s_H[7] * ty + s_H[8];
+                double px = (s_H[0] * tx + s_H[1] * ty + s_H[2]) / zz;
+                double py = (s_H[3] * tx + s_H[4] * ty + s_H[5]) / zz;
+                double val = bilinear_at(v, px, py);
+                if (val == -1.0) continue;
+                double thr = ((s_bc[0] * tx + s_bc[1] * ty + s_bc[2]) + (s_wc[0] * tx + s_wc[1] * ty + s_wc[2])) / 2.0;
+                s_vals[tw * (by - minc) + (bx - minc)] = val - thr;
+            }
+            __syncthreads();
+            for (int64_t t = tid; t < tw * tw; t += blockDim.x) {
+                int64_t y = t / tw, x = t - y * tw;
+                double acc = 0.0;
+                if (y > 0) acc = acc + -s_vals[(y - 1) * tw + x];
+                if (x > 0) acc = acc + -s_vals[y * tw + x - 1];
+                acc = acc + s_vals[y * tw + x] * 4.0;
+                if (x + 1 < tw) acc = acc + -s_vals[y * tw + x + 1];
+                if (y + 1 < tw) acc = acc + -s_vals[(y + 1) * tw + x];
+                s_sharp[t] = acc;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                float bs = 0.0f, ws = 0.0f, bc = 1.0f, wc = 1.0f;
+                uint64_t rcode = 0;
+                for (int64_t i = 0; i < F.nbits; i++) {
+                    rcode <<= 1;
+                    int64_t cell = (F.bit_y[i] - minc) * tw + (F.bit_x[i] - minc);
+                    double vv = s_vals[cell] + prm.decode_sharpening * s_sharp[cell];
+                    if (vv > 0.0) {
+                        ws = (float)((double)ws + vv);
+                        wc = __fadd_rn(wc, 1.0f);
+                        rcode |= 1;
+                    } else {
+                        bs = (float)((double)bs - vv);
+                        bc = __fadd_rn(bc, 1.0f);
+                    }
+                }
+                double x = (double)__fdiv_rn(ws, wc), y = (double)__fdiv_rn(bs, bc);
+                double m = x != x ? y : y != y ? x : x < y ? x : y;  // fmin
+                float margin = (float)m;
+                uint32_t lk = qd_lookup(F, rcode);
+                int64_t id = lk & 0xffff, ham = (lk >> 16) & 0xff, rot = lk >> 24;
+                if (margin >= 0.0f && ham < 255) {
+                    // H = qH * R(rot * pi/2) (fast/detector.c:83-107)
+                    double c = prm.rot_cs[rot][0], s = prm.rot_cs[rot][1];
+                    const double r[9] = {c, -s, 0.0, s, c, 0.0, 0.0, 0.0, 1.0};
+                    GpuDetection d;
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++) {
+                            double acc = 0.0;
+                            for (int k = 0; k < 3; k++) acc = acc + s_H[i * 3 + k] * r[k * 3 + j];
+                            d.H[i * 3 + j] = acc;
+                        }
+                    d.family = fi;
+                    d.id = (int32_t)id;
+                    d.hamming = (int32_t)ham;
+                    d.decision_margin = margin;
+                    project(d.H, 0.0, 0.0, &d.c[0], &d.c[1]);
+                    for (int i = 0; i < 4; i++) {
+                        double tx = i == 1 || i == 2 ? 1.0 : -1.0;
+                        double ty = i < 2 ? 1.0 : -1.0;
+                        project(d.H, tx, ty, &d.p[i][0], &d.p[i][1]);
+                    }
+                    dets[qi * prm.nfam + fi] = d;
+                    det_ok[qi * prm.nfam + fi] = 1;
+                }
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 10. Per frame: gather the detections in (quad, family) order, remove
+// overlapping detections of one tag (fast/decode.c:766-891), stable sort by
+// id (fast/detector.c:164-179). One thread per frame.
+
+struct GLine {
+    double p[2], u[2];
+};
+
+__device__ GLine gline_of(const double *p0, const double *p1) {
+    double u0 = p1[0] - p0[0], u1 = p1[1] - p0[1];
+    double mag = (double)__fsqrt_rn((float)(u0 * u0 + u1 * u1));
+    GLine l;
+    l.p[0] = p0[0];
+    l.p[1] = p0[1];
+    l.u[0] = u0 / mag;
+    l.u[1] = u1 / mag;
+    return l;
+}
+__device__ __forceinline__ double gline_coord(const GLine &l, const double *q) {
+    return (q[0] - l.p[0]) * l.u[0] + (q[1] - l.p[1]) * l.u[1];
+}
+__device__ bool segments_cross(const double *a0, const double *a1, const double *b0, const double *b1) {
+    GLine la = gline_of(a0, a1), lb = gline_of(b0, b1);
+    double m00 = la.u[0], m01 = -lb.u[0], m10 = la.u[1], m11 = -lb.u[1];
+    double det = m00 * m11 - m01 * m10;
+    if (fabs(det) < 0.00000001) return false;
+    double i00 = m11 / det, i01 = -m01 / det;
+    double b00 = lb.p[0] - la.p[0], b10 = lb.p[1] - la.p[1];
+    double x00 = i00 * b00 + i01 * b10;
+    double t[2] = {la.u[0] * x00 + la.p[0], la.u[1] * x00 + la.p[1]};
+    double a = gline_coord(la, la.p), b = gline_coord(la, a1), c = gline_coord(la, t);
+    if ((c < a && c < b) || (c > a && c > b)) return false;
+    a = gline_coord(lb, lb.p);
+    b = gline_coord(lb, b1);
+    c = gline_coord(lb, t);
+    if ((c < a && c < b) || (c > a && c > b)) return false;
+    return true;
+}
+__device__ bool poly_contains(const double (*poly)[2], const double *q) {
+    int last = 0, acc = 0;
+    for (int i = 0; i < 5; i++) {
+        const double *p = poly[i % 4];
+        int quad = p[0] < q[0] ? (p[1] < q[1] ? 2 : 1) : (p[1] < q[1] ? 3 : 0);
+        if (i > 0) {
+            int dq = quad - last;
+            if (dq == -3 || dq == 1)
+                acc++;
+            else if (dq == -1 || dq == 3)
+                acc--;
+            else if (dq == -2 || dq == 2) {
+                const double *p0 = poly[i - 1];
+                double nx = p[1] - q[1], ny = -p[0] + q[0];
+                double dot = nx * (p0[0] - q[0]) + ny * (p0[1] - q[1]);
+                acc += dot < 0.0 ? -2 : 2;
+            }
+        }
+        last = quad;
+    }
+    return acc >= 2 || acc <= -2;
+}
+__device__ bool quads_overlap(const double (*pa)[2], const double (*pb)[2]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            if (segments_cross(pa[i], pa[(i + 1) % 4], pb[j], pb[(j + 1) % 4])) return true;
+    double qb[2] = {(pb[0][0] + pb[1][0] + pb[2][0]) / 3.0, (pb[0][1] + pb[1][1] + pb[2][1]) / 3.0};
+    if (poly_contains(pa, qb)) return true;
+    double qa[2] = {(pa[0][0] + pa[1][0] + pa[2][0]) / 3.0, (pa[0][1] + pa[1][1] + pa[2][1]) / 3.0};
+    return poly_contains(pb, qa);
+}
+__device__ __forceinline__ int prefer(int pref, double a, double b) {
+    return pref ? pref : a < b ? -1 : b < a ? 1 : 0;
+}
+
+__global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
+                           const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nframes) return;
+    GpuDetection *d = out + out_off[f];
+    int64_t n = 0;
+    for (int64_t i = frame_qstart[f] * nfam; i < frame_qstart[f + 1] * nfam; i++)
+        if (det_ok[i]) d[n++] = dets[i];
+    int64_t i0 = 0;
+    while (i0 < n) {
+        bool gone = false;
+        int64_t i1 = i0 + 1;
+        while (i1 < n) {
+            if (d[i0].id != d[i1].id || d[i0].family != d[i1].family || !quads_overlap(d[i0].p, d[i1].p)) {
+                i1++;
+                continue;
+            }
+            int pref = prefer(0, d[i0].hamming, d[i1].hamming);
+            pref = prefer(pref, -(double)d[i0].decision_margin, -(double)d[i1].decision_margin);
+            for (int i = 0; i < 4; i++) {
+                pref = prefer(pref, d[i0].p[i][0], d[i1].p[i][0]);
+                pref = prefer(pref, d[i0].p[i][1], d[i1].p[i][1]);
+            }
+            int64_t drop = pref < 0 ? i1 : i0;
+            for (int64_t k = drop; k + 1 < n; k++) d[k] = d[k + 1];
+            n--;
+            if (drop == i0) {
+                gone = true;
+                break;
+            }
+        }
+        if (!gone) i0++;
+    }
+    for (int64_t i = 1; i < n; i++) {  // stable insertion sort by id
+        GpuDetection x = d[i];
+        int64_t j = i;
+        while (j > 0 && d[j - 1].id > x.id) {
+            d[j] = d[j - 1];
+            j--;
+        }
+        d[j] = x;
+    }
+    out_n[f] = n;
+}
+
+__global__ void k_gather_quads(const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
+                               GpuQuad *out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (ok[i]) out[scan[i]] = quads[i];
+}
+
+// ---------------------------------------------------------------------------
+// Launchers.
+
+static inline dim3 frame_grid(const Launch &L) { return dim3((unsigned)L.blocks_per_frame, (unsigned)L.nframes); }
+static inline unsigned flat_blocks(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)b;
+}
+
+void launch_decimate(const Launch &L, const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor) {
+    k_decimate<<<frame_grid(L), 256, 0, L.stream>>>(frames, img, qim, factor);
+}
+
+void launch_blur(const Launch &L, const FrameDesc *frames, uint8_t *qim, uint8_t *tmp_a, uint8_t *tmp_b,
+                 const BlurTaps &taps, bool sharpen) {
+    k_blur_pass<<<frame_grid(L), 256, 0, L.stream>>>(frames, qim, tmp_a, taps, 0);
+    k_blur_pass<<<frame_grid(L), 256, 0, L.stream>>>(frames, tmp_a, tmp_b, taps, 1);
+    k_blur_finish<<<frame_grid(L), 256, 0, L.stream>>>(frames, tmp_b, qim, sharpen ? 1 : 0);
+}
+
+void launch_threshold(const Launch &L, const FrameDesc *frames, const uint8_t *qim, uint8_t *tmax, uint8_t *tmin,
+                      uint8_t *thr, int32_t diff) {
+    k_tile_minmax<<<frame_grid(L), 256, 0, L.stream>>>(frames, qim, tmax, tmin);
+    k_threshold<<<frame_grid(L), 256, 0, L.stream>>>(frames, qim, tmax, tmin, thr, diff);
+}
+
+void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uint8_t *tmp) {
+    k_morph<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, tmp, 1);
+    k_morph<<<frame_grid(L), 256, 0, L.stream>>>(frames, tmp, thr, 0);
+}
+
+void launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
+                    uint32_t *lab, int32_t min_px) {
+    k_runs<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    k_union<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    k_flatten<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns);
+    k_labels<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+}
+
+void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                        uint64_t *row_npts) {
+    k_point_count<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_npts);
+}
+
+void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                       const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb) {
+    k_point_emit<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
+}
+
+void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head) {
+    k_cluster_heads<<<flat_blocks(n, 256), 256, 0, s>>>(key, n, head);
+}
+
+void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
+                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe) {
+    k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe);
+}
+
+void launch_fit_quads(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+                      const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
+                      int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
+    if (nclusters <= 0) return;
+    unsigned blocks = (unsigned)(nclusters < 148 * 64 ? nclusters : 148 * 64);
+    k_fit_quads<<<blocks, AT_FIT_THREADS, 0, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+                                                  quads, quad_ok, err);
+}
+
+void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
+                         GpuQuad *out) {
+    if (n <= 0) return;
+    k_gather_quads<<<flat_blocks(n, 256), 256, 0, s>>>(quads, ok, scan, n, out);
+}
+
+void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads, GpuDetection *dets,
+                   uint32_t *det_ok) {
+    if (nquads <= 0) return;
+    unsigned blocks = (unsigned)(nquads < 148 * 64 ? nquads : 148 * 64);
+    k_decode<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, fams, img, qim, quads, nquads, dets, det_ok);
+}
+
+void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
+                     const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n) {
+    k_finalize<<<(nframes + 63) / 64, 64, 0, s>>>(nframes, frame_qstart, nfam, dets, det_ok, out, out_off, out_n);
+}

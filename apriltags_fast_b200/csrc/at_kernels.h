@@ -1,0 +1,62 @@
+// Launchers of the detection kernels (defined in at_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "at_gpu.h"
+
+// Run table and union-find nodes, indexed by node id.
+struct RunArrays {
+    uint16_t *start, *end;
+    uint8_t *v;
+    uint32_t *parent;  // union-find parent (after k_flatten: the root)
+    uint32_t *px;      // at a root: its component's pixel count
+};
+
+// Per-point scratch of the quad fit, indexed by point position.
+struct FitScratch {
+    uint64_t *keys, *skey;
+    uint32_t *sval;
+    double *w, *fx, *fy;
+    double *mx, *my, *mxx, *mxy, *myy, *mw;
+    double *errs, *filt, *mxe;
+    int32_t *mxi;
+};
+
+struct BlurTaps {
+    int n;
+    uint8_t k[64];
+};
+
+// The grid of the per-frame kernels: x blocks per frame, one row of frames.
+struct Launch {
+    cudaStream_t stream;
+    int nframes;
+    int blocks_per_frame;
+};
+
+void launch_decimate(const Launch &L, const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor);
+void launch_blur(const Launch &L, const FrameDesc *frames, uint8_t *qim, uint8_t *tmp_a, uint8_t *tmp_b,
+                 const BlurTaps &taps, bool sharpen);
+void launch_threshold(const Launch &L, const FrameDesc *frames, const uint8_t *qim, uint8_t *tmax, uint8_t *tmin,
+                      uint8_t *thr, int32_t diff);
+void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uint8_t *tmp);
+void launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
+                    uint32_t *lab, int32_t min_px);
+void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                        uint64_t *row_npts);
+void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                       const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb);
+void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head);
+void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
+                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe);
+void launch_fit_quads(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+                      const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
+                      int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
+void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
+                         GpuQuad *out);
+void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads, GpuDetection *dets,
+                   uint32_t *det_ok);
+void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
+                     const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n);

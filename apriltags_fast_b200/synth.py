@@ -1,0 +1,205 @@
+"""Seeded synthetic AprilTag frames with the shapes of the benchmark configs.
+
+There is no public dataset for the benchmark; these frames stand in for it:
+a linear-gradient background with Gaussian noise, tags rendered from the
+family code tables (a 1-module white border, as apriltag_to_image draws
+them), placed by random homographies without overlap, optional filled
+rectangle/ellipse distractors and an illumination ramp, a Gaussian blur,
+rounded and clamped to u8. Tag codes are drawn without replacement, so
+every detection id in a frame is distinct.
+
+    img, truth = make_frame(CONFIGS["1080p"], seed=2)
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Config:
+    width: int
+    height: int
+    families: tuple = ("tag36h11",)
+    ntags: tuple = (4, 4)            # inclusive range
+    side: tuple = (60, 140)          # tag side in pixels
+    tilt_deg: float = 40.0
+    noise: float = 3.0
+    blur: tuple = (0.7, 0.7)         # per-tag blur sigma range (one value: global)
+    distractors: int = 0
+    ramp: tuple | None = None        # illumination ramp (lo, hi)
+    gradient: tuple = (60.0, 190.0)
+
+
+CONFIGS = {
+    # 640x480, 4 tags of 60-140 px, tilt <= 40 deg, noise 3, blur 0.7
+    "640x480": Config(640, 480),
+    # 1920x1080, 24 tags of 30-220 px, tilt <= 60, noise 4, blur 0.8, 200 distractors
+    "1080p": Config(1920, 1080, ntags=(24, 24), side=(30, 220), tilt_deg=60.0, noise=4.0, blur=(0.8, 0.8),
+                    distractors=200),
+    # 4032x3024, two families, 80 tags of 16-400 px, tilt <= 65, noise 6,
+    # per-tag blur 0.5-1.5, ramp 0.4-1.0, 1000 distractors
+    "4032x3024": Config(4032, 3024, families=("tagStandard52h13", "tag36h11"), ntags=(80, 80), side=(16, 400),
+                        tilt_deg=65.0, noise=6.0, blur=(0.5, 1.5), distractors=1000, ramp=(0.4, 1.0)),
+}
+
+
+def tag_pattern(code: int, nbits: int, bit_x, bit_y, wab: int, tw: int, reversed_border: bool) -> np.ndarray:
+    """The tag's module grid (tw x tw, 0 black / 255 white), drawn the way
+    the upstream library's apriltag_to_image draws it (apriltag.c:271-297)."""
+    im = np.zeros((tw, tw), np.uint8)
+    wbw = wab + (0 if reversed_border else 2)
+    wbs = (tw - wbw) // 2
+    for i in range(wbw - 1):
+        im[wbs, wbs + i] = 255
+        im[wbs + i, tw - 1 - wbs] = 255
+        im[tw - 1 - wbs, wbs + i + 1] = 255
+        im[wbs + 1 + i, wbs] = 255
+    bs = (tw - wab) // 2
+    for i in range(nbits):
+        if code >> (nbits - i - 1) & 1:
+            im[bit_y[i] + bs, bit_x[i] + bs] = 255
+    return im
+
+
+def _homography(src, dst):
+    A = []
+    for (x, y), (u, v) in zip(src, dst):
+        A.append([x, y, 1, 0, 0, 0, -u * x, -u * y, -u])
+        A.append([0, 0, 0, x, y, 1, -v * x, -v * y, -v])
+    _, _, vt = np.linalg.svd(np.asarray(A, float))
+    H = vt[-1].reshape(3, 3)
+    return H / H[2, 2]
+
+
+def _tag_corners(rng, cx, cy, side, tilt_deg):
+    """Corners of a square of `side` px centred at (cx, cy), rotated
+    uniformly and tilted out of plane by up to tilt_deg (pinhole view)."""
+    rot = rng.uniform(0, 2 * math.pi)
+    tilt = math.radians(rng.uniform(0, tilt_deg))
+    axis = rng.uniform(0, math.pi)
+    h = side / 2.0
+    sq = np.array([[-h, -h, 0], [h, -h, 0], [h, h, 0], [-h, h, 0]], float)
+    c, s = math.cos(rot), math.sin(rot)
+    Rz = np.array([[c, -s, 0], [s, c, 0], [0, 0, 1]])
+    ax = np.array([math.cos(axis), math.sin(axis), 0.0])
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    Rt = np.eye(3) + math.sin(tilt) * K + (1 - math.cos(tilt)) * K @ K
+    p = sq @ Rz.T @ Rt.T
+    f = 4.0 * side
+    z = f + p[:, 2]
+    return np.stack([cx + f * p[:, 0] / z, cy + f * p[:, 1] / z], 1)
+
+
+def _blur(img, sigma):
+    if sigma <= 0:
+        return img
+    r = max(1, int(math.ceil(3 * sigma)))
+    x = np.arange(-r, r + 1)
+    k = np.exp(-0.5 * (x / sigma) ** 2)
+    k /= k.sum()
+    pad = np.pad(img, ((0, 0), (r, r)), mode="edge")
+    out = sum(k[i] * pad[:, i:i + img.shape[1]] for i in range(2 * r + 1))
+    pad = np.pad(out, ((r, r), (0, 0)), mode="edge")
+    return sum(k[i] * pad[i:i + img.shape[0], :] for i in range(2 * r + 1))
+
+
+@dataclass
+class TagTruth:
+    family: str
+    id: int
+    corners: np.ndarray
+    side: float
+
+
+def make_frame(cfg: Config, seed: int, family_tables=None):
+    """One frame (u8, h x w) and the list of TagTruth of the tags drawn.
+
+    family_tables: name -> (codes, nbits, bit_x, bit_y, wab, tw, reversed);
+    defaults to the built-in families of the library."""
+    if family_tables is None:
+        family_tables = {n: builtin_table(n) for n in cfg.families}
+    rng = np.random.default_rng(seed)
+    W, H = cfg.width, cfg.height
+    yy, xx = np.mgrid[0:H, 0:W].astype(np.float32)
+    ang = rng.uniform(0, 2 * math.pi)
+    t = (xx * math.cos(ang) + yy * math.sin(ang))
+    t = (t - t.min()) / max(1e-6, float(t.max() - t.min()))
+    img = (cfg.gradient[0] + (cfg.gradient[1] - cfg.gradient[0]) * t).astype(np.float32)
+
+    # distractors: filled rectangles and ellipses, intensity U(0, 255)
+    for _ in range(cfg.distractors):
+        sz = rng.uniform(10, 150, size=2)
+        x0, y0 = rng.uniform(0, W), rng.uniform(0, H)
+        val = rng.uniform(0, 255)
+        x1, x2 = int(max(0, x0 - sz[0] / 2)), int(min(W, x0 + sz[0] / 2))
+        y1, y2 = int(max(0, y0 - sz[1] / 2)), int(min(H, y0 + sz[1] / 2))
+        if x2 <= x1 or y2 <= y1:
+            continue
+        if rng.uniform() < 0.5:
+            img[y1:y2, x1:x2] = val
+        else:
+            sy, sx = np.mgrid[y1:y2, x1:x2]
+            m = ((sx - x0) / (sz[0] / 2)) ** 2 + ((sy - y0) / (sz[1] / 2)) ** 2 <= 1.0
+            img[y1:y2, x1:x2][m] = val
+
+    ntags = int(rng.integers(cfg.ntags[0], cfg.ntags[1] + 1))
+    placed, truths = [], []
+    used = {n: set() for n in cfg.families}
+    tries = 0
+    while len(truths) < ntags and tries < 200 * max(1, ntags):
+        tries += 1
+        side = rng.uniform(*cfg.side)
+        r = side * 0.75 + 4
+        cx, cy = rng.uniform(r, W - r), rng.uniform(r, H - r)
+        if any((cx - px) ** 2 + (cy - py) ** 2 < (r + pr) ** 2 for px, py, pr in placed):
+            continue
+        fname = cfg.families[int(rng.integers(len(cfg.families)))]
+        codes, nbits, bx, by, wab, tw, rev = family_tables[fname]
+        if len(used[fname]) >= len(codes):
+            continue
+        while True:
+            tid = int(rng.integers(len(codes)))
+            if tid not in used[fname]:
+                break
+        used[fname].add(tid)
+        pat = tag_pattern(int(codes[tid]), nbits, bx, by, wab, tw, rev)
+        corners = _tag_corners(rng, cx, cy, side, cfg.tilt_deg)
+        # the tag's outer edge maps to the corners: module grid [0, tw]
+        Hm = _homography([(0, 0), (tw, 0), (tw, tw), (0, tw)], corners)
+        Hi = np.linalg.inv(Hm)
+        x1, y1 = np.floor(corners.min(0)).astype(int)
+        x2, y2 = np.ceil(corners.max(0)).astype(int) + 1
+        x1, y1, x2, y2 = max(x1, 0), max(y1, 0), min(x2, W), min(y2, H)
+        sy, sx = np.mgrid[y1:y2, x1:x2].astype(np.float64)
+        q = Hi @ np.stack([sx.ravel() + 0.5, sy.ravel() + 0.5, np.ones(sx.size)])
+        u, v = q[0] / q[2], q[1] / q[2]
+        inside = (u >= 0) & (u < tw) & (v >= 0) & (v < tw)
+        vals = pat[np.clip(v.astype(int), 0, tw - 1), np.clip(u.astype(int), 0, tw - 1)].astype(np.float32)
+        sub = img[y1:y2, x1:x2].ravel()
+        sub[inside] = vals[inside]
+        img[y1:y2, x1:x2] = sub.reshape(y2 - y1, x2 - x1)
+        placed.append((cx, cy, r))
+        truths.append(TagTruth(fname, tid, corners, side))
+
+    if cfg.ramp is not None:
+        ra = rng.uniform(0, 2 * math.pi)
+        t2 = (xx * math.cos(ra) + yy * math.sin(ra))
+        t2 = (t2 - t2.min()) / max(1e-6, float(t2.max() - t2.min()))
+        img = img * (cfg.ramp[0] + (cfg.ramp[1] - cfg.ramp[0]) * t2)
+    sig = float(rng.uniform(*cfg.blur))
+    img = _blur(img, sig)
+    img = img + rng.normal(0.0, cfg.noise, size=img.shape)
+    return np.clip(np.rint(img), 0, 255).astype(np.uint8), truths
+
+
+def builtin_table(name: str):
+    """(codes, nbits, bit_x, bit_y, wab, tw, reversed) of a built-in family."""
+    from . import family
+
+    f = family(name)
+    codes = np.ctypeslib.as_array(f.codes, shape=(f.ncodes,)).copy()
+    return (codes, f.nbits, list(f.bit_x[:f.nbits]), list(f.bit_y[:f.nbits]), f.width_at_border, f.total_width,
+            bool(f.reversed_border))

@@ -1,0 +1,192 @@
+/* apriltags-b200: the native C API of the GPU AprilTag detector.
+
+   A drop-in for the native API of bouk/apriltags-fast
+   (fast/apriltag_fast.h:99-141): the same function names, arguments and
+   struct layouts (at_detection is 168 bytes, at_detector 160 bytes, at_family
+   584 bytes; checked with offsetof in the tests), so code written against
+   that header links against libapriltag_b200.so unchanged:
+
+       at_detector *td = at_detector_create();
+       at_add_family(td, at_tag36h11(), 2);
+       at_detect(td, pixels, width, height, stride);
+       for (int64_t i = 0; i < td->ndetections; i++) use(td->detections[i]);
+       at_detector_destroy(td);
+
+   Every stage of at_detect runs as sm_100a CUDA kernels on the current
+   device; there is no CPU path. The detections are bit-identical to the
+   reference built with -ffp-contract=off; detections that share an id keep
+   the order of their quads, which here is the order of their boundary
+   clusters by component label (see at_detector_last_error below for the
+   error model). */
+#ifndef APRILTAG_FAST_H
+#define APRILTAG_FAST_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A tag family (fast/apriltag_fast.h:24-36). `codes` stays owned by the
+   caller (or is static for the built-in families). */
+typedef struct at_family {
+    char name[32];
+    const uint64_t *codes;
+    int64_t ncodes;
+    int32_t nbits;
+    int32_t h;
+    int32_t width_at_border;
+    int32_t total_width;
+    bool reversed_border;
+    int32_t bit_x[64]; /* bit positions in tag coordinates, MSB first */
+    int32_t bit_y[64];
+} at_family;
+
+/* Quad detection parameters (fast/apriltag_fast.h:40-48). */
+typedef struct at_quad_thresh_params {
+    int32_t min_cluster_pixels;   /* default 24 */
+    int32_t max_nmaxima;          /* default 10 */
+    float critical_rad;           /* unused, kept for the layout */
+    float cos_critical_rad;       /* default (float)cos(10 degrees) */
+    float max_line_fit_mse;       /* default 10 */
+    int32_t min_white_black_diff; /* default 5 */
+    bool deglitch;                /* default false */
+} at_quad_thresh_params;
+
+/* One detection (fast/apriltag_fast.h:52-64). `family` indexes the
+   detector's families in the order they were added. H maps tag coordinates
+   in [-1, 1] to pixels (row major); p holds the corners counter-clockwise
+   from tag coordinate (-1, -1). */
+typedef struct at_detection {
+    int32_t family;
+    int32_t id;
+    int32_t hamming;
+    float decision_margin;
+    double H[9];
+    double c[2];
+    double p[4][2];
+} at_detection;
+
+/* Seconds spent per stage in the last at_detect (fast/apriltag_fast.h:67-69),
+   measured with CUDA events around each stage's kernels. */
+typedef struct at_timing {
+    double decimate, blur, threshold, unionfind, clusters, fit_quads, decode, reconcile, total;
+} at_timing;
+
+struct at_internal;
+
+/* The detector (fast/apriltag_fast.h:73-96). nthreads is accepted and
+   ignored: the results do not depend on it. */
+typedef struct at_detector {
+    int32_t nthreads;
+    float quad_decimate;   /* 1.5, or an integer factor; default 2 */
+    float quad_sigma;      /* blur (>0) or sharpen (<0) of the quad image */
+    bool refine_edges;     /* default true */
+    double decode_sharpening; /* default 0.25 */
+    bool debug;            /* writes debug_preprocess.pnm / debug_threshold.pnm */
+    at_quad_thresh_params qtp;
+
+    at_detection *detections; /* valid until the next at_detect */
+    int64_t ndetections;
+    int64_t nquads;
+    at_timing timing;
+
+    struct at_internal *in;
+} at_detector;
+
+/* Replaces at_detector_create (fast/detector.c:4-31): default parameters,
+   no families. Aborts if no CUDA device can be used. */
+at_detector *at_detector_create(void);
+/* Replaces at_detector_destroy (fast/detector.c:35-43). */
+void at_detector_destroy(at_detector *td);
+/* Replaces at_add_family (fast/detector.c:45-54): false for
+   bits_corrected outside 0..3, a 17th family, ncodes >= 65536 or nbits
+   outside 1..64. The decode tables are built once and kept on the device. */
+bool at_add_family(at_detector *td, const at_family *fam, int bits_corrected);
+/* Replaces at_clear_families (fast/detector.c:56-60). */
+void at_clear_families(at_detector *td);
+/* Replaces at_family_name (fast/detector.c:62-64). */
+const char *at_family_name(const at_detector *td, const at_detection *d);
+/* Replaces at_detect (fast/detector.c:246-335). pixels is host memory
+   (pageable or pinned) or device memory; it is never written. */
+void at_detect(at_detector *td, const uint8_t *pixels, int64_t width, int64_t height, int64_t stride);
+/* Replaces at_shutdown (fast/detector.c:33): releases the detector's
+   device arenas; the next at_detect allocates them again. */
+void at_shutdown(at_detector *td);
+
+/* The built-in families (fast/families.c:44-78). NULL when the library
+   was built without the family tables. */
+const at_family *at_tag16h5(void);
+const at_family *at_tag25h9(void);
+const at_family *at_tag36h10(void);
+const at_family *at_tag36h11(void);
+const at_family *at_tagCircle21h7(void);
+const at_family *at_tagCircle49h12(void);
+const at_family *at_tagCustom48h12(void);
+const at_family *at_tagStandard41h12(void);
+const at_family *at_tagStandard52h13(void);
+/* Replaces at_family_by_name (fast/families.c:64-68). */
+const at_family *at_family_by_name(const char *name);
+
+/* PNM files (fast/image.c:204-266): same behaviour as the reference. */
+bool at_read_pnm(const char *path, int64_t *width, int64_t *height, uint8_t **pixels);
+bool at_read_pnm_into(const char *path, int64_t *width, int64_t *height, uint8_t **pixels, int64_t *cap);
+bool at_write_pgm(const char *path, const uint8_t *pixels, int64_t width, int64_t height);
+
+/* ---------------------------------------------------------------------
+   Additions of the GPU library (no counterpart in the reference). */
+
+/* The last error of the detector: 0 for none. A failed CUDA call or a
+   device-side check (a buffer bound, a bounded wait) makes at_detect return
+   no detections and sets this; the message is kept until the next call. */
+int at_detector_last_error(const at_detector *td, const char **message);
+
+/* One frame of a batch. */
+typedef struct at_frame {
+    const uint8_t *pixels; /* host or device memory */
+    int64_t width, height, stride;
+    uint32_t family_mask;  /* bit i: decode with family i (0: all) */
+} at_frame;
+
+/* The result of one frame of a batch: detections [first, first + count)
+   of td->detections, and that frame's quad count. */
+typedef struct at_frame_result {
+    int64_t first, count, nquads;
+} at_frame_result;
+
+/* Detect tags in n frames of any sizes in one pass over the GPU: each
+   stage runs once for all frames. results[i] is what at_detect would give
+   for frame i alone (bit-identical). td->detections holds all frames'
+   detections, frame by frame; td->ndetections their total. */
+void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *results);
+
+/* Diagnostics: copy an intermediate array of the last at_detect (or of
+   frame 0 of the last batch) to host memory `dst` of `cap` bytes. Returns
+   the array's size in bytes (copying min(size, cap)), or -1. `what`:
+     AT_DIAG_QUAD_IMAGE  u8 qw*qh, the decimated (blurred) image
+     AT_DIAG_THRESHOLD   u8 qw*qh, 0 / 127 / 255
+     AT_DIAG_LABELS      u32 qw*qh, each pixel's component label (its
+                         smallest union-find node id) or 0xffffffff
+     AT_DIAG_POINTS      u64 per boundary point in cluster order:
+                         x | y<<16 | gx<<32 | gy<<48
+     AT_DIAG_CLUSTERS    u32 per cluster, the index of its first point
+     AT_DIAG_QUADS       per fitted quad: 8 f32 corners (quad image
+                         coordinates) then i32 reversed_border, i32 frame
+     AT_DIAG_SIZES       i64 qw, qh, points, clusters, quads */
+enum {
+    AT_DIAG_QUAD_IMAGE = 0,
+    AT_DIAG_THRESHOLD = 1,
+    AT_DIAG_LABELS = 2,
+    AT_DIAG_POINTS = 3,
+    AT_DIAG_CLUSTERS = 4,
+    AT_DIAG_QUADS = 5,
+    AT_DIAG_SIZES = 6
+};
+int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -247,3 +247,56 @@ def ref_lib():
         L.at_family_by_name.restype = C.POINTER(Family)
         _ref = L
     return _ref
+
+
+class _QTP(C.Structure):
+    _fields_ = [("min_cluster_pixels", C.c_int32), ("max_nmaxima", C.c_int32), ("critical_rad", C.c_float),
+                ("cos_critical_rad", C.c_float), ("max_line_fit_mse", C.c_float),
+                ("min_white_black_diff", C.c_int32), ("deglitch", C.c_bool)]
+
+
+class _RefDetector(C.Structure):
+    """The reference's at_detector layout (fast/apriltag_fast.h:73-96)."""
+
+    _fields_ = [("nthreads", C.c_int32), ("quad_decimate", C.c_float), ("quad_sigma", C.c_float),
+                ("refine_edges", C.c_bool), ("decode_sharpening", C.c_double), ("debug", C.c_bool),
+                ("qtp", _QTP), ("detections", C.POINTER(Detection)), ("ndetections", C.c_int64),
+                ("nquads", C.c_int64), ("timing", C.c_double * 9), ("internal", C.c_void_p)]
+
+
+def ref_detect(img: np.ndarray, family_names, bits, params: Params | None = None, nthreads: int = 1):
+    """Run the reference itself (oracle/_ref) on an image: (detections, nquads).
+    Detections in the reference's output order."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref not built (make -C oracle ref)")
+    R.at_detector_create.restype = C.POINTER(_RefDetector)
+    R.at_detector_destroy.argtypes = [C.POINTER(_RefDetector)]
+    R.at_add_family.argtypes = [C.POINTER(_RefDetector), C.POINTER(Family), C.c_int]
+    R.at_add_family.restype = C.c_bool
+    R.at_detect.argtypes = [C.POINTER(_RefDetector), C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape
+    p = params or default_params()
+    td = R.at_detector_create()
+    try:
+        for n, b in zip(family_names, bits):
+            if not R.at_add_family(td, R.at_family_by_name(n.encode()), b):
+                raise ValueError("reference refused the family")
+        d = td.contents
+        d.nthreads = nthreads
+        d.quad_decimate = p.quad_decimate
+        d.quad_sigma = p.quad_sigma
+        d.refine_edges = bool(p.refine_edges)
+        d.decode_sharpening = p.decode_sharpening
+        d.qtp.min_cluster_pixels = p.min_cluster_pixels
+        d.qtp.max_nmaxima = p.max_nmaxima
+        d.qtp.cos_critical_rad = p.cos_critical_rad
+        d.qtp.max_line_fit_mse = p.max_line_fit_mse
+        d.qtp.min_white_black_diff = p.min_white_black_diff
+        d.qtp.deglitch = bool(p.deglitch)
+        R.at_detect(td, img.ctypes.data, w, h, w)
+        d = td.contents
+        return [det_tuple(d.detections[i]) for i in range(d.ndetections)], int(d.nquads)
+    finally:
+        R.at_detector_destroy(td)
