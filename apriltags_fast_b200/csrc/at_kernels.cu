@@ -330,6 +330,19 @@ __global__ void k_union(const FrameDesc *frames, const uint8_t *thr, RunArrays r
     }
 }
 
+// The root of x without writes. After the unions, k_flatten must not use
+// uf_find: a path-halving write that read its value before another thread
+// stored the root would put a non-root parent back.
+__device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
+    const volatile uint32_t *p = par;
+    uint32_t px = p[x];
+    while (px != x) {
+        x = px;
+        px = p[x];
+    }
+    return x;
+}
+
 // Every node points at its root; each root sums its component's pixels.
 __global__ void k_flatten(const FrameDesc *frames, RunArrays runs, const uint32_t *row_nruns) {
     const FrameDesc f = frames[blockIdx.y];
@@ -341,7 +354,7 @@ __global__ void k_flatten(const FrameDesc *frames, RunArrays runs, const uint32_
         const int64_t n = row_nruns[f.row0 + y];
         for (int64_t i = lane; i <= n; i += 32) {
             int64_t node = i < n ? base + i : f.node_off + (int64_t)f.qw * f.qh + y;
-            uint32_t r = uf_find(runs.parent, (uint32_t)node);
+            uint32_t r = uf_root(runs.parent, (uint32_t)node);
             runs.parent[node] = r;
             uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
             atomicAdd(runs.px + r, px);
@@ -374,7 +387,7 @@ __global__ void k_labels(const FrameDesc *frames, const RunArrays runs, const ui
         }
         uint32_t l = AT_NOK;
         if (node >= 0) {
-            uint32_t r = runs.parent[node];
+            uint32_t r = uf_root(runs.parent, (uint32_t)node);
             if ((int64_t)runs.px[r] >= min_px) l = r;
         }
         lab[f.q_off + i] = l;
