@@ -253,8 +253,8 @@ class Detector:
         stage-by-stage checks: quad_image, threshold, labels, points,
         clusters, quads or sizes."""
         code = DIAG[what]
-        sizes = np.zeros(5, np.int64)
-        self._L.at_detector_diag(self._td, DIAG["sizes"], sizes.ctypes.data, 40)
+        sizes = np.zeros(6, np.int64)
+        self._L.at_detector_diag(self._td, DIAG["sizes"], sizes.ctypes.data, 48)
         if what == "sizes":
             return sizes
         nbytes = self._L.at_detector_diag(self._td, code, None, 0)

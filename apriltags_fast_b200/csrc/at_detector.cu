@@ -109,6 +109,7 @@ struct at_internal {
     std::string msg;
     // sizes of the last run (frame 0), for at_detector_diag
     int64_t last_qw = 0, last_qh = 0, last_npts = 0, last_ncl = 0, last_nq = 0;
+    int64_t launches = 0;  // kernels of this library launched so far
 };
 
 // ---------------------------------------------------------------------------
@@ -375,16 +376,25 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     }
     uint8_t *qim = B[B_QIM].as<uint8_t>(), *thr = B[B_THR].as<uint8_t>();
     launch_decimate(L, dfr, B[B_IMG].as<uint8_t>(), qim, td->quad_decimate);
+    in->launches += 1;
     CK(cudaEventRecord(in->ev[1], st));
-    if (ntaps > 1) launch_blur(L, dfr, qim, B[B_TMPA].as<uint8_t>(), B[B_TMPB].as<uint8_t>(), taps, td->quad_sigma < 0);
+    if (ntaps > 1) {
+        launch_blur(L, dfr, qim, B[B_TMPA].as<uint8_t>(), B[B_TMPB].as<uint8_t>(), taps, td->quad_sigma < 0);
+        in->launches += 3;
+    }
     CK(cudaEventRecord(in->ev[2], st));
     launch_threshold(L, dfr, qim, B[B_TMAX].as<uint8_t>(), B[B_TMIN].as<uint8_t>(), thr, td->qtp.min_white_black_diff);
-    if (td->qtp.deglitch) launch_deglitch(L, dfr, thr, B[B_TMPA].as<uint8_t>());
+    in->launches += 2;
+    if (td->qtp.deglitch) {
+        launch_deglitch(L, dfr, thr, B[B_TMPA].as<uint8_t>());
+        in->launches += 2;
+    }
     CK(cudaEventRecord(in->ev[3], st));
     RunArrays runs{B[B_RSTART].as<uint16_t>(), B[B_REND].as<uint16_t>(), B[B_RV].as<uint8_t>(),
                    B[B_PARENT].as<uint32_t>(), B[B_PX].as<uint32_t>()};
     uint32_t *lab = B[B_LAB].as<uint32_t>();
     launch_segment(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), lab, td->qtp.min_cluster_pixels);
+    in->launches += 4;
     CK(cudaEventRecord(in->ev[4], st));
     CK(cudaGetLastError());
 
@@ -392,6 +402,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     uint64_t *row_npts = B[B_ROWPTS].as<uint64_t>(), *row_off = B[B_ROWOFF].as<uint64_t>();
     CK(cudaMemsetAsync(row_npts + rows, 0, 8, st));
     launch_point_count(L, dfr, thr, lab, row_npts);
+    in->launches += 1;
     if (!cub_call(in, [&](void *t, size_t &b) {
             return cub::DeviceScan::ExclusiveSum(t, b, row_npts, row_off, rows + 1, st);
         }))
@@ -410,6 +421,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_HEAD].ensure(npts * 4));
         CK(B[B_HSCAN].ensure(npts * 4));
         launch_point_emit(L, dfr, thr, lab, row_off, B[B_KEY].as<uint64_t>(), B[B_VAL].as<uint64_t>(), nb);
+        in->launches += 1;
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
                                                        B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
@@ -419,6 +431,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         const uint64_t *skey = B[B_KEY2].as<uint64_t>(), *spts = B[B_VAL2].as<uint64_t>();
         uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
         launch_cluster_heads(st, skey, npts, head);
+        in->launches += 1;
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
             }))
@@ -432,6 +445,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_CFRAME].ensure(ncl * 4));
         launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
                               B[B_CFRAME].as<int32_t>());
+        in->launches += 1;
         CK(cudaEventRecord(in->ev[5], st));
 
         // quads
@@ -452,6 +466,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
         launch_fit_quads(st, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
+        in->launches += 1;
         CK(cudaGetLastError());
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
@@ -464,6 +479,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         if (nq > 0) {
             CK(B[B_QUADSC].ensure(nq * sizeof(GpuQuad)));
             launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>());
+            in->launches += 1;
             hq.resize(nq);
             CK(cudaMemcpyAsync(hq.data(), B[B_QUADSC].p, nq * sizeof(GpuQuad), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -504,6 +520,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         launch_decode(st, dfr, prm, in->dfam.as<GpuFamily>(), B[B_IMG].as<uint8_t>(), qim, B[B_QUADSC].as<GpuQuad>(),
                       nq, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
         CK(cudaEventRecord(in->ev[7], st));
+        in->launches += 2;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
                         B[B_OUTN].as<int64_t>());
@@ -685,7 +702,7 @@ int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap
     const DBuf *B = in->buf;
     const void *src = nullptr;
     int64_t bytes = 0;
-    int64_t sizes[5] = {in->last_qw, in->last_qh, in->last_npts, in->last_ncl, in->last_nq};
+    int64_t sizes[6] = {in->last_qw, in->last_qh, in->last_npts, in->last_ncl, in->last_nq, in->launches};
     switch (what) {
     case AT_DIAG_QUAD_IMAGE: src = B[B_QIM].p, bytes = in->last_qw * in->last_qh; break;
     case AT_DIAG_THRESHOLD: src = B[B_THR].p, bytes = in->last_qw * in->last_qh; break;
@@ -694,8 +711,8 @@ int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap
     case AT_DIAG_CLUSTERS: src = B[B_CSTART].p, bytes = 4 * in->last_ncl; break;
     case AT_DIAG_QUADS: src = B[B_QUADSC].p, bytes = (int64_t)sizeof(GpuQuad) * in->last_nq; break;
     case AT_DIAG_SIZES:
-        memcpy(dst, sizes, (size_t)(cap < 40 ? cap : 40));
-        return 40;
+        memcpy(dst, sizes, (size_t)(cap < 48 ? cap : 48));
+        return 48;
     default: return -1;
     }
     int64_t n = bytes < cap ? bytes : cap;

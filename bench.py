@@ -1,0 +1,354 @@
+"""Benchmark of the GPU AprilTag detector on the 1080p synthetic workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl gpu|reference]
+
+Workload: 1920x1080 u8 frames, tag36h11 (bits_corrected 2), decimate 2,
+refine on; 24 tags of 30-220 px, tilt <= 60 deg, noise 4, blur 0.8, 200
+distractor shapes per frame (seeded synthetic frames: no public dataset
+exists for this benchmark). A pool of 64 distinct frames (132 MB, larger
+than the 126 MB L2) rotates through the steps, so no step reads inputs that
+a previous step left in L2.
+
+A step is one at_detect_batch over B frames. `value` is frames/s with the
+frames already in device memory; `e2e` is the same call on pinned host
+frames (the host-to-device copies and the copy of the detections back are
+inside the timed region). `single_frame` is the plain at_detect path, one
+frame per call, with its per-frame latency percentiles. One JSON line.
+
+With torchrun (N > 1) each rank runs its own detector on its own frames
+(frames are independent: no collective on the data path); `value` is all
+ranks' frames over the slowest rank's time.
+
+--impl reference times the reference's own CPU detector (compiled from its
+sources into oracle/_ref) with all host threads on the same frames.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p frames/s (batched GPU detector, bit-exact detections)"
+W, H = 1920, 1080
+POOL = 64
+
+
+def make_pool(rank: int, n: int = POOL):
+    from apriltags_fast_b200 import synth
+
+    cfg = synth.CONFIGS["1080p"]
+    base = [synth.make_frame(cfg, 1000 * rank + s)[0] for s in range((n + 1) // 2)]
+    pool = base + [np.ascontiguousarray(f[::-1, ::-1]) for f in base]  # 180 deg: still valid tags
+    return pool[:n]
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._p = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self._p:
+            time.sleep(0.25)
+            self._p.terminate()
+            self._p.wait()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_reference_fps(pool, nthreads: int, seconds: float):
+    """The reference (oracle/_ref) on the host: frames/s over a bounded
+    sample of the pool (at most `seconds` of work)."""
+    from oracle import oracle as O
+
+    if O.ref_lib() is None:
+        return None, 0
+    R = O.ref_lib()
+    import ctypes as C
+
+    R.at_detector_create.restype = C.POINTER(O._RefDetector)
+    R.at_add_family.argtypes = [C.POINTER(O._RefDetector), C.POINTER(O.Family), C.c_int]
+    R.at_detect.argtypes = [C.POINTER(O._RefDetector), C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
+    R.at_detector_destroy.argtypes = [C.POINTER(O._RefDetector)]
+    td = R.at_detector_create()
+    R.at_add_family(td, R.at_family_by_name(b"tag36h11"), 2)
+    td.contents.nthreads = nthreads
+    R.at_detect(td, pool[0].ctypes.data, W, H, W)  # warm-up (starts the workers)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        f = pool[n % len(pool)]
+        R.at_detect(td, f.ctypes.data, W, H, W)
+        n += 1
+    dt = time.perf_counter() - t0
+    R.at_detector_destroy(td)
+    return n / dt, n
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pool = make_pool(0, 16)
+    cores = os.cpu_count() or 1
+    from oracle import oracle as O
+
+    if O.ref_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
+        return
+    # each step: B frames through the reference's at_detect, all threads
+    import ctypes as C
+
+    R = O.ref_lib()
+    R.at_detector_create.restype = C.POINTER(O._RefDetector)
+    R.at_add_family.argtypes = [C.POINTER(O._RefDetector), C.POINTER(O.Family), C.c_int]
+    R.at_detect.argtypes = [C.POINTER(O._RefDetector), C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
+    td = R.at_detector_create()
+    R.at_add_family(td, R.at_family_by_name(b"tag36h11"), 2)
+    td.contents.nthreads = cores
+    B = args.batch
+    k = 0
+    for _ in range(args.warmup):
+        for _ in range(B):
+            R.at_detect(td, pool[k % len(pool)].ctypes.data, W, H, W)
+            k += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for _ in range(B):
+            R.at_detect(td, pool[k % len(pool)].ctypes.data, W, H, W)
+            k += 1
+    dt = time.perf_counter() - t0
+    fps = args.steps * B / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "1080p tag36h11 decimate 2, 24 tags + 200 distractors", "batch": B,
+                   "frame": [W, H], "threads": cores},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} steps x {B} frames of 16 distinct 1080p frames"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import apriltags_fast_b200 as AT
+
+    pool = make_pool(rank)
+    dev = [torch.from_numpy(f).cuda() for f in pool]
+    pinned = [torch.from_numpy(f).pin_memory() for f in pool]
+    det = AT.Detector(["tag36h11"], 2)
+    B = args.batch
+
+    def batch_at(step, src):
+        i0 = (step * B) % len(src)
+        return [src[(i0 + j) % len(src)] for j in range(B)]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- batched, frames resident in HBM ---
+    for s in range(args.warmup):
+        det.detect_batch(batch_at(s, dev))
+    stage = {k: 0.0 for k in det.timing}
+    launches0 = int(det.diag("sizes")[5]) if len(det.diag("sizes")) > 5 else 0
+    ndet = 0
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record()
+        for s in range(args.steps):
+            out = det.detect_batch(batch_at(args.warmup + s, dev))
+            ndet += sum(len(o) for o in out)
+            for k, v in det.timing.items():
+                stage[k] += v
+        ev1.record()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = int(det.diag("sizes")[5]) - launches0 if len(det.diag("sizes")) > 5 else None
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * args.steps * B / (t_max / 1e3)
+
+    # --- e2e: the same call on pinned host frames ---
+    for s in range(args.warmup):
+        det.detect_batch(batch_at(s, pinned))
+    barrier()
+    ndet_e2e = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(args.steps):
+        out = det.detect_batch(batch_at(args.warmup + s, pinned))
+        ndet_e2e += sum(len(o) for o in out)
+    e1.record()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * args.steps * B / (ms_e2e / 1e3)
+
+    # --- the plain single-frame path (at_detect), per-frame latency ---
+    lat = []
+    nsf = max(args.steps * 4, 64)
+    for i in range(5):
+        det.detect(pinned[i % len(pinned)].numpy())
+    torch.cuda.synchronize()
+    for i in range(nsf):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        det.detect(pinned[i % len(pinned)].numpy())
+        b.record()
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+    lat = np.array(lat)
+
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # the dominant stage by device time, and its roofline (HBM bound)
+    steps = args.steps
+    stage_ms = {k: v / steps * 1e3 for k, v in stage.items() if k != "total"}
+    dom = max(stage_ms, key=stage_ms.get)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    sizes = det.diag("sizes")
+    npts = int(sizes[2])  # last batch's frame 0; per-frame points, typical
+    qpx = (W // 2) * (H // 2)
+    # algorithmic bytes per launch (per batch of B frames), per stage:
+    alg = {
+        "decimate": B * (W * H + qpx),                 # read the frame, write the quad image
+        "threshold": B * 2 * qpx,                      # read the quad image, write the threshold image
+        "unionfind": B * (qpx + 13 * qpx // 4),        # threshold image + runs and nodes (13 B a node)
+        "clusters": B * npts * (8 + 8 + 2 * 16),       # points written, then sorted (key + value)
+        "fit_quads": B * npts * 8,                     # each boundary point read once
+        "decode": B * 24 * 4 * 64 * 25 * 8,            # refine samples along the quads' edges
+        "reconcile": B * 24 * 168,
+        "blur": 0,
+    }
+    dur = stage_ms[dom] / 1e3
+    achieved = alg.get(dom, 0) / dur / 1e9 if dur > 0 else 0.0
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "frames/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": "1080p tag36h11 decimate 2, 24 tags + 200 distractors, bits 2", "batch": B,
+                   "frame": [W, H], "pool_frames": len(pool), "l2": "inputs larger than L2 (64 frames, 132 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "detections_per_frame": ndet / (steps * B),
+        "single_frame": {"fps": 1e3 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
+                         "p99_ms": float(np.percentile(lat, 99)), "p999_ms": float(np.percentile(lat, 99.9)),
+                         "frames": int(nsf), "input": "pinned host"},
+        "stage_ms_per_step": stage_ms,
+        "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": B * W * H,
+                "d2h_bytes_per_step": int(ndet_e2e / steps * 168 + 8 * B)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+        "frame_roofline": {"bytes_per_frame": W * H, "achieved_gbs": value * W * H / 1e9,
+                           "frac": value * W * H / 1e9 / peak},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        fps_all, n_all = cpu_reference_fps(pool[:16], cores, 10.0)
+        fps_1, n_1 = cpu_reference_fps(pool[:16], 1, 6.0)
+        if fps_all is not None:
+            line["cpu_baseline"] = {"value": fps_all, "unit": "frames/s", "cores": cores, "kind": "reference",
+                                    "sample": f"{n_all} frames (16 distinct 1080p) at {cores} threads, ~10 s",
+                                    "value_1thread": fps_1, "sample_1thread": f"{n_1} frames, ~6 s"}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -173,7 +173,8 @@ void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_fram
      AT_DIAG_CLUSTERS    u32 per cluster, the index of its first point
      AT_DIAG_QUADS       per fitted quad: 8 f32 corners (quad image
                          coordinates) then i32 reversed_border, i32 frame
-     AT_DIAG_SIZES       i64 qw, qh, points, clusters, quads */
+     AT_DIAG_SIZES       i64 qw, qh, points, clusters, quads, and the number
+                         of this library's kernels launched so far */
 enum {
     AT_DIAG_QUAD_IMAGE = 0,
     AT_DIAG_THRESHOLD = 1,
