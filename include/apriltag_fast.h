@@ -186,6 +186,25 @@ enum {
 };
 int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap);
 
+/* The threshold stage without any device allocation (it has no counterpart
+   in the reference). For callers that cannot call cudaMalloc: a frame loop
+   whose latency must not include the device-wide synchronisation that
+   cudaMalloc/cudaFree imply, or a process whose device memory is all owned
+   by one pool or framework that hands it only buffers. `image` (width x
+   height u8, rows width bytes apart) and `out` (same size) are device
+   memory of the caller; `stream` is a cudaStream_t (NULL: the default
+   stream). The result equals the threshold image of at_detect for a quad
+   image `image` (0 / 127 / 255, min_white_black_diff as qtp).
+   The only scratch is a fixed 2 MiB array of the library that each GPU
+   holds from the first call until the process exits: images above 1 Mi
+   4x4 tiles (e.g. 4096 x 4096) are refused, as are images below one tile.
+   The first call on a device finds that array's device address (once per
+   device): make that first call before any stream capture. Every call
+   shares the array: calls that overlap on the GPU race. Returns 0, 1 for
+   a refused size, 2 for a CUDA error (message on stderr). */
+int at_threshold_noalloc(const uint8_t *image, int64_t width, int64_t height, int32_t min_white_black_diff,
+                         uint8_t *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
