@@ -83,7 +83,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -99,8 +99,9 @@ struct at_internal {
     bool fam_dirty = true;
 
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev[12];
+    cudaEvent_t fork = nullptr, join = nullptr;  // ordering only, no timing
     DBuf buf[B_NBUF];
     HBuf h_frames, h_small, h_out;
     std::vector<at_detection> dets;
@@ -464,9 +465,9 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                        B[B_SERRS].as<double>(),   B[B_SFILT].as<double>(),  B[B_SMXE].as<double>(),
                        B[B_SMXI].as<int32_t>()};
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
-        launch_fit_quads(st, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
+        launch_fit_quads(st, in->side, in->fork, in->join, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
-        in->launches += 1;
+        in->launches += 2;
         CK(cudaGetLastError());
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
@@ -506,6 +507,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_DETS].ensure(nd * sizeof(GpuDetection)));
         CK(B[B_DETOK].ensure(nd * 4));
         CK(B[B_OUT].ensure(nd * sizeof(GpuDetection)));
+        CK(B[B_DIDX].ensure(nd * 4));
+        CK(B[B_DRM].ensure(nd));
         CK(B[B_QSTART].ensure((n + 1) * 8));
         CK(B[B_OUTOFF].ensure((n + 1) * 8));
         CK(B[B_OUTN].ensure((n + 1) * 8));
@@ -522,7 +525,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(cudaEventRecord(in->ev[7], st));
         in->launches += 2;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
-                        B[B_DETOK].as<uint32_t>(), B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
+                        B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
+                        B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
                         B[B_OUTN].as<int64_t>());
         CK(cudaGetLastError());
         CK(in->h_out.ensure(nd * sizeof(GpuDetection)));
@@ -611,6 +615,9 @@ at_detector *at_detector_create(void) {
         abort();
     }
     for (int k = 0; k < 12; k++) cudaEventCreate(&in->ev[k]);
+    cudaStreamCreateWithFlags(&in->side, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&in->fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&in->join, cudaEventDisableTiming);
     return td;
 }
 
@@ -636,6 +643,9 @@ void at_detector_destroy(at_detector *td) {
         for (void *p : in->fam_mem[i]) cudaFree(p);
     in->dfam.release();
     for (int k = 0; k < 12; k++) cudaEventDestroy(in->ev[k]);
+    cudaEventDestroy(in->fork);
+    cudaEventDestroy(in->join);
+    cudaStreamDestroy(in->side);
     cudaStreamDestroy(in->stream);
     delete in;
     free(td);

@@ -739,21 +739,36 @@ __device__ double kth_largest(double *v, int64_t n, int64_t k) {
     return v[k];
 }
 
-#define FIT_SORT_CAP 2048
+// Two size classes of clusters, one kernel template: 128 threads for
+// clusters of at most FIT_SMALL points (everything staged in shared
+// memory), 512 threads for the larger ones (dynamic shared memory; sorts
+// beyond FIT_LARGE_SORT points fall back to global scratch).
+#define FIT_SMALL 1024
+#define FIT_LARGE_SORT 8192
+#define FIT_CHUNK_SMALL 1024
+#define FIT_CHUNK_LARGE 2048
 
-__global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *frames, GpuParams prm,
-                                                                 const uint8_t *qim, const uint64_t *pts,
-                                                                 const uint32_t *cstart, const int32_t *cframe,
-                                                                 int64_t nclusters, int64_t npoints, FitScratch scr,
-                                                                 GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
-    __shared__ uint64_t s_key[FIT_SORT_CAP];
-    __shared__ uint32_t s_val[FIT_SORT_CAP];
+// dynamic shared memory of one block of the fit kernel
+__host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk) {
+    return (size_t)sort_cap * 12 + (size_t)chunk * 24;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
+                                                   const uint64_t *pts, const uint32_t *cstart,
+                                                   const int32_t *cframe, int64_t nclusters, int64_t npoints,
+                                                   FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err,
+                                                   int64_t class_lo, int64_t class_hi, int sort_cap, int chunk) {
+    extern __shared__ __align__(16) unsigned char fit_smem[];
+    uint64_t *s_key = reinterpret_cast<uint64_t *>(fit_smem);
+    double *s_w = reinterpret_cast<double *>(fit_smem + (size_t)sort_cap * 8);
+    double *s_fx = s_w + chunk, *s_fy = s_fx + chunk;
+    uint32_t *s_val = reinterpret_cast<uint32_t *>(fit_smem + (size_t)sort_cap * 8 + (size_t)chunk * 24);
     __shared__ float s_lane[8];
-    __shared__ int s_rev;
-    __shared__ uint32_t s_bb[4][AT_FIT_THREADS / 32];
+    __shared__ int s_rev, s_ok;
+    __shared__ uint32_t s_bb[4][NT / 32];
     __shared__ uint32_t s_scan[32];
     __shared__ int64_t s_nm;
-    __shared__ int s_ok;
     __shared__ double s_perr[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pmse[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA],
         s_pnx[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pny[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA];
     const int tid = threadIdx.x;
@@ -761,6 +776,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
     for (int64_t c = blockIdx.x; c < nclusters; c += gridDim.x) {
         const int64_t s0 = cstart[c];
         const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
+        if (sz < class_lo || sz > class_hi) continue;  // the other class's kernel
         const FrameDesc f = frames[cframe[c]];
         if (tid == 0) quad_ok[c] = 0;
         if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
@@ -771,7 +787,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         const uint64_t *P = pts + s0;
         // bounding box (fast/quads.c:515-528)
         uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
-        for (int64_t i = tid; i < sz; i += blockDim.x) {
+        for (int64_t i = tid; i < sz; i += NT) {
             uint32_t x = (uint32_t)(P[i] & 0xffff), y = (uint32_t)(P[i] >> 16 & 0xffff);
             xmin = min(xmin, x);
             xmax = max(xmax, x);
@@ -792,7 +808,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
             s_bb[3][tid >> 5] = ymax;
         }
         __syncthreads();
-        for (int w = 0; w < AT_FIT_THREADS / 32; w++) {
+        for (int w = 0; w < NT / 32; w++) {
             xmin = min(xmin, s_bb[0][w]);
             xmax = max(xmax, s_bb[1][w]);
             ymin = min(ymin, s_bb[2][w]);
@@ -805,7 +821,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         // angle keys, and the dot product of offsets and gradients: 8 lanes
         // over the whole groups of 8, then the rest (fast/quads.c:467-512)
         uint64_t *keys = scr.keys + s0;
-        for (int64_t i = tid; i < sz; i += blockDim.x) {
+        for (int64_t i = tid; i < sz; i += NT) {
             float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
             keys[i] = angle_key(dx, dy, (uint32_t)i);
         }
@@ -846,10 +862,10 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         // block head and its place in the leaf; then one sort by (head,
         // place), packed into 64 bits as head's slope bits, 0xffff - head's
         // index, and the place.
-        const bool in_smem = sz <= FIT_SORT_CAP;
+        const bool in_smem = sz <= sort_cap;
         uint64_t *sk = in_smem ? s_key : scr.skey + s0;
         uint32_t *sv = in_smem ? s_val : scr.sval + s0;
-        for (int64_t p = tid; p < sz; p += blockDim.x) {
+        for (int64_t p = tid; p < sz; p += NT) {
             uint32_t lf = leaf_of(sz, p);
             int64_t lo = lf >> 8, len = lf & 255;
             if (p != lo) continue;
@@ -868,44 +884,50 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         block_sort_pairs(sk, sv, sz);
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
-        // w = sqrt(gx^2 + gy^2) + 1 on the quad image, 1 at its border
-        double *wb = scr.w + s0, *fxb = scr.fx + s0, *fyb = scr.fy + s0;
+        // w = sqrt(gx^2 + gy^2) + 1 on the quad image (1 at its border),
+        // fx = x/2 + 1/2. Each chunk of points is staged in shared memory,
+        // then lane c of warp 0 (c < 6) runs prefix sum c in point order:
+        // the term of sum c is (w * a) * b with a, b in {fx, fy, 1} (a
+        // product with 1.0 is exact), so no lane branches.
         const uint8_t *im = qim + f.q_off;
-        for (int64_t k = tid; k < sz; k += blockDim.x) {
-            uint32_t src = sv[k];
-            int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
-            int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
-            int32_t g2 = 0;
-            if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
-                int64_t cc = (int64_t)iy * f.qw + ix;
-                int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
-                int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
-                g2 = gx * gx + gy * gy;
-            }
-            wb[k] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
-            fxb[k] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
-            fyb[k] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
-        }
-        __syncthreads();
         double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
-        if (tid < 6) {
-            double s = 0.0;
-            double *out = M[tid];
-            for (int64_t k = 0; k < sz; k++) {
-                double w = wb[k], fx = fxb[k], fy = fyb[k], v;
-                switch (tid) {
-                case 0: v = __dmul_rn(w, fx); break;
-                case 1: v = __dmul_rn(w, fy); break;
-                case 2: v = __dmul_rn(__dmul_rn(w, fx), fx); break;
-                case 3: v = __dmul_rn(__dmul_rn(w, fx), fy); break;
-                case 4: v = __dmul_rn(__dmul_rn(w, fy), fy); break;
-                default: v = w; break;
+        double run = 0.0;
+        const int ln = tid & 31;
+        double *mout = M[ln < 6 ? ln : 5];
+        for (int64_t k0 = 0; k0 < sz; k0 += chunk) {
+            const int64_t kn = dmin((int64_t)chunk, sz - k0);
+            for (int64_t t = tid; t < kn; t += NT) {
+                uint32_t src = sv[k0 + t];
+                int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
+                int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
+                int32_t g2 = 0;
+                if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
+                    int64_t cc = (int64_t)iy * f.qw + ix;
+                    int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
+                    int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
+                    g2 = gx * gx + gy * gy;
                 }
-                s = __dadd_rn(s, v);
-                out[k] = s;
+                s_w[t] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
+                s_fx[t] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
+                s_fy[t] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
             }
+            __syncthreads();
+            if (tid < 6) {
+                const int ca = tid == 1 || tid == 4 ? 1 : tid == 5 ? 2 : 0;  // 0 fx, 1 fy, 2 one
+                const int cb = tid == 2 ? 0 : tid == 3 || tid == 4 ? 1 : 2;
+                const double *A = ca == 0 ? s_fx : s_fy, *Bv = cb == 0 ? s_fx : s_fy;
+                double *o = mout + k0;
+#pragma unroll 4
+                for (int64_t t = 0; t < kn; t++) {
+                    double w = s_w[t];
+                    double a = ca == 2 ? 1.0 : A[t];
+                    double b = cb == 2 ? 1.0 : Bv[t];
+                    run = __dadd_rn(run, __dmul_rn(__dmul_rn(w, a), b));
+                    o[t] = run;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
         const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
 
         // corner search (fast/quads.c:788-959)
@@ -913,7 +935,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         if (ksz < 2) continue;
         const double nn = (double)(2 * ksz + 1);
         double *errs = scr.errs + s0, *filt = scr.filt + s0;
-        for (int64_t i = tid; i < sz; i += blockDim.x) {
+        for (int64_t i = tid; i < sz; i += NT) {
             int64_t i0 = i - ksz, i1 = i + ksz;
             MSum s;
             if (i0 < 0)
@@ -925,7 +947,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
             errs[i] = window_error(s, nn);
         }
         __syncthreads();
-        for (int64_t i = tid; i < sz; i += blockDim.x) {
+        for (int64_t i = tid; i < sz; i += NT) {
             double acc;
             if (i >= 3 && i < sz - 3) {
                 acc = errs[i - 3] * prm.qsm[0];
@@ -946,7 +968,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         int32_t *mxi = scr.mxi + s0;
         double *mxe = scr.mxe + s0;
         int64_t nm_run = 0;
-        for (int64_t i0 = 0; i0 < sz; i0 += blockDim.x) {
+        for (int64_t i0 = 0; i0 < sz; i0 += NT) {
             int64_t i = i0 + tid;
             uint32_t is_max = 0;
             double e = 0.0;
@@ -981,7 +1003,7 @@ __global__ void __launch_bounds__(AT_FIT_THREADS) k_fit_quads(const FrameDesc *f
         }
         // line fits of pairs of maxima: (a, b), a < b, and the closing pair
         // (b, a) wrapping around for b >= a + 3
-        for (int64_t t = tid; t < nm * nm; t += blockDim.x) {
+        for (int64_t t = tid; t < nm * nm; t += NT) {
             int64_t p = t / nm, q = t - p * nm;
             bool used = p < q || p >= q + 3;
             if (!used) continue;
@@ -1657,49 +1679,84 @@ __device__ __forceinline__ int prefer(int pref, double a, double b) {
     return pref ? pref : a < b ? -1 : b < a ? 1 : 0;
 }
 
+// One block per frame. Overlap removal only ever drops a detection in favour
+// of another with the same (family, id), and its outcome for one such
+// group depends only on that group's detections in quad order; so the
+// groups are resolved independently (one thread each, the rare groups of
+// two or more), and the survivors are placed by their stable rank by id.
 __global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
-                           const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
+                           const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
+                           const int64_t *out_off, int64_t *out_n) {
+    __shared__ uint32_t sh[32];
+    const int f = blockIdx.x;
     if (f >= nframes) return;
-    GpuDetection *d = out + out_off[f];
+    const int64_t a = frame_qstart[f] * nfam, b = frame_qstart[f + 1] * nfam;
+    uint32_t *ix = idx + a;
+    uint8_t *rm = removed + a;
+    // the detections of the frame in (quad, family) order
     int64_t n = 0;
-    for (int64_t i = frame_qstart[f] * nfam; i < frame_qstart[f + 1] * nfam; i++)
-        if (det_ok[i]) d[n++] = dets[i];
-    int64_t i0 = 0;
-    while (i0 < n) {
-        bool gone = false;
-        int64_t i1 = i0 + 1;
-        while (i1 < n) {
-            if (d[i0].id != d[i1].id || d[i0].family != d[i1].family || !quads_overlap(d[i0].p, d[i1].p)) {
-                i1++;
+    for (int64_t s0 = a; s0 < b; s0 += blockDim.x) {
+        int64_t s = s0 + threadIdx.x;
+        uint32_t ok = s < b ? det_ok[s] : 0u;
+        uint32_t total;
+        uint32_t off = block_excl_scan(ok, &total, sh);
+        if (ok) ix[n + off] = (uint32_t)s;
+        n += total;
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) rm[i] = 0;
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const GpuDetection &di = dets[ix[i]];
+        bool first = true, more = false;
+        for (int64_t j = 0; j < n && first; j++)
+            if (j != i && dets[ix[j]].id == di.id && dets[ix[j]].family == di.family) {
+                if (j < i) first = false;
+                else more = true;
+            }
+        if (!first || !more) continue;
+        // the reference's loop (fast/decode.c:860-891) over this group only
+        int64_t i0 = i;
+        while (i0 < n) {
+            if (rm[i0] || dets[ix[i0]].id != di.id || dets[ix[i0]].family != di.family) {
+                i0++;
                 continue;
             }
-            int pref = prefer(0, d[i0].hamming, d[i1].hamming);
-            pref = prefer(pref, -(double)d[i0].decision_margin, -(double)d[i1].decision_margin);
-            for (int i = 0; i < 4; i++) {
-                pref = prefer(pref, d[i0].p[i][0], d[i1].p[i][0]);
-                pref = prefer(pref, d[i0].p[i][1], d[i1].p[i][1]);
-            }
-            int64_t drop = pref < 0 ? i1 : i0;
-            for (int64_t k = drop; k + 1 < n; k++) d[k] = d[k + 1];
-            n--;
-            if (drop == i0) {
-                gone = true;
+            for (int64_t i1 = i0 + 1; i1 < n; i1++) {
+                const GpuDetection &d0 = dets[ix[i0]], &d1 = dets[ix[i1]];
+                if (rm[i1] || d1.id != di.id || d1.family != di.family || !quads_overlap(d0.p, d1.p)) continue;
+                int pref = prefer(0, d0.hamming, d1.hamming);
+                pref = prefer(pref, -(double)d0.decision_margin, -(double)d1.decision_margin);
+                for (int k = 0; k < 4; k++) {
+                    pref = prefer(pref, d0.p[k][0], d1.p[k][0]);
+                    pref = prefer(pref, d0.p[k][1], d1.p[k][1]);
+                }
+                if (pref < 0) {
+                    rm[i1] = 1;
+                    continue;
+                }
+                rm[i0] = 1;
                 break;
             }
+            i0++;
         }
-        if (!gone) i0++;
     }
-    for (int64_t i = 1; i < n; i++) {  // stable insertion sort by id
-        GpuDetection x = d[i];
-        int64_t j = i;
-        while (j > 0 && d[j - 1].id > x.id) {
-            d[j] = d[j - 1];
-            j--;
-        }
-        d[j] = x;
+    __syncthreads();
+    // stable sort by id (fast/detector.c:164-179): rank among survivors
+    GpuDetection *o = out + out_off[f];
+    uint32_t kept = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        if (rm[i]) continue;
+        kept++;
+        int32_t id = dets[ix[i]].id;
+        int64_t r = 0;
+        for (int64_t j = 0; j < n; j++)
+            if (!rm[j] && (dets[ix[j]].id < id || (dets[ix[j]].id == id && j < i))) r++;
+        o[r] = dets[ix[i]];
     }
-    out_n[f] = n;
+    uint32_t total;
+    block_excl_scan(kept, &total, sh);
+    if (threadIdx.x == 0) out_n[f] = total;
 }
 
 __global__ void k_gather_quads(const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
@@ -1768,13 +1825,25 @@ void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *
     k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe);
 }
 
-void launch_fit_quads(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
-                      const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
-                      int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
+void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const FrameDesc *frames,
+                      const GpuParams &prm, const uint8_t *qim, const uint64_t *pts, const uint32_t *cstart,
+                      const int32_t *cframe, int64_t nclusters, int64_t npoints, const FitScratch &scr, GpuQuad *quads,
+                      uint32_t *quad_ok, uint32_t *err) {
     if (nclusters <= 0) return;
+    const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL), large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE);
+    cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
+    cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
+    // the few large clusters on a side stream, beside the many small ones
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    k_fit_quads<512><<<(unsigned)(nclusters < 148 * 2 ? nclusters : 148 * 2), 512, large, side>>>(
+        frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, quads, quad_ok, err, FIT_SMALL + 1,
+        INT64_MAX, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
+    cudaEventRecord(join, side);
     unsigned blocks = (unsigned)(nclusters < 148 * 64 ? nclusters : 148 * 64);
-    k_fit_quads<<<blocks, AT_FIT_THREADS, 0, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
-                                                  quads, quad_ok, err);
+    k_fit_quads<128><<<blocks, 128, small, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+                                                quads, quad_ok, err, 0, FIT_SMALL, FIT_SMALL, FIT_CHUNK_SMALL);
+    cudaStreamWaitEvent(s, join, 0);
 }
 
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
@@ -1792,6 +1861,7 @@ void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm
 }
 
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
-                     const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n) {
-    k_finalize<<<(nframes + 63) / 64, 64, 0, s>>>(nframes, frame_qstart, nfam, dets, det_ok, out, out_off, out_n);
+                     const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
+                     const int64_t *out_off, int64_t *out_n) {
+    k_finalize<<<nframes, 256, 0, s>>>(nframes, frame_qstart, nfam, dets, det_ok, idx, removed, out, out_off, out_n);
 }

@@ -50,13 +50,15 @@ void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *
 void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head);
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
                            int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe);
-void launch_fit_quads(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
-                      const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
-                      int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
+void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const FrameDesc *frames,
+                      const GpuParams &prm, const uint8_t *qim, const uint64_t *pts, const uint32_t *cstart,
+                      const int32_t *cframe, int64_t nclusters, int64_t npoints, const FitScratch &scr, GpuQuad *quads,
+                      uint32_t *quad_ok, uint32_t *err);
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
                          GpuQuad *out);
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
                    const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads, GpuDetection *dets,
                    uint32_t *det_ok);
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
-                     const uint32_t *det_ok, GpuDetection *out, const int64_t *out_off, int64_t *out_n);
+                     const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
+                     const int64_t *out_off, int64_t *out_n);
