@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libapriltag_b200.so")
+LIB_PATH = os.environ.get("APRILTAG_B200_LIB") or os.path.join(_HERE, "libapriltag_b200.so")
 
 
 class Family(C.Structure):

@@ -25,6 +25,33 @@ __device__ __forceinline__ int64_t c_int(double x) {
     return -2147483648LL;
 }
 
+// Block-wide exclusive scan of one value per thread (blockDim <= 1024).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total, uint32_t *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __syncthreads();
+    if (lane == 31) sh[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += t;
+        }
+        if (lane < nw) sh[lane] = s;
+    }
+    __syncthreads();
+    uint32_t off = wid > 0 ? sh[wid - 1] : 0;
+    *total = sh[nw - 1];
+    return off + incl - v;
+}
+
 #define FRAME_LOOP_BEGIN(n_items)                                                               \
     const FrameDesc fd = frames[blockIdx.y];                                                   \
     for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < (n_items);          \
@@ -198,63 +225,8 @@ __global__ void k_morph(const FrameDesc *frames, const uint8_t *in, uint8_t *out
 }
 
 // ---------------------------------------------------------------------------
-// 4. Runs (fast/threshold.c:210-283). One warp per row: the run starts of
-// 32 columns at a time by ballot; runs of 127 are not kept. Each run gets
-// union-find node node_off + y*qw + i, initialised as its own root.
-
-__global__ void k_runs(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns) {
-    const FrameDesc f = frames[blockIdx.y];
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    for (int64_t y = warp; y < f.qh; y += nwarps) {
-        const uint8_t *t = thr + f.q_off + y * f.qw;
-        const int64_t base = f.node_off + y * f.qw;
-        const int64_t xmax = f.qw - 2;
-        int64_t count = 0, open = -1;
-        for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
-            int64_t x = x0 + lane;
-            bool valid = x <= xmax;
-            uint8_t v = valid ? t[x] : 0;
-            bool start = valid && (x == 0 || t[x - 1] != v);
-            uint32_t S = __ballot_sync(0xffffffffu, start);
-            uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
-            if (start) {
-                uint32_t below = S & lt;
-                int64_t prev_slot;
-                if (below) {
-                    int pl = 31 - __clz(below);
-                    prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
-                } else {
-                    prev_slot = open;
-                }
-                if (prev_slot >= 0) runs.end[base + prev_slot] = (uint16_t)(x - 1);
-                if (v != 127) {
-                    int64_t s = base + count + __popc(N & lt);
-                    runs.start[s] = (uint16_t)x;
-                    runs.v[s] = v;
-                    runs.parent[s] = (uint32_t)s;
-                    runs.px[s] = 0;
-                }
-            }
-            if (S) {
-                int ls = 31 - __clz(S);
-                open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
-            }
-            count += __popc(N);
-        }
-        if (lane == 0) {
-            if (open >= 0) runs.end[base + open] = (uint16_t)xmax;
-            row_nruns[f.row0 + y] = (uint32_t)count;
-            int64_t vn = f.node_off + (int64_t)f.qw * f.qh + y;
-            runs.parent[vn] = (uint32_t)vn;
-            runs.px[vn] = 0;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
+// 4-5. Runs and connected components over runs.
+//
 // 5. Connected components over runs (fast/unionfind.c:89-196): the same
 // pairs of runs join as in the reference; lock-free union that links the
 // larger root under the smaller, so every component's root is its smallest
@@ -265,8 +237,9 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *par, uint32_t x) {
     uint32_t px = p[x];
     while (px != x) {
         uint32_t ppx = p[px];
-        if (ppx != px) p[x] = ppx;  // path halving: only ever an ancestor
-        x = px;
+        if (ppx == px) return px;
+        p[x] = ppx;  // path halving: only ever an ancestor
+        x = ppx;
         px = p[x];
     }
     return x;
@@ -293,46 +266,280 @@ __device__ __forceinline__ bool runs_touch(int64_t a0, int64_t a1, int64_t b0, i
     return dmax(dmax(a0, b0 - 1), 1) <= dmin(a1, b1 - 1);
 }
 
-__global__ void k_union(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, const uint32_t *row_nruns) {
-    const FrameDesc f = frames[blockIdx.y];
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t y = 1 + warp; y < f.qh; y += nwarps) {
-        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
-        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
-        for (int64_t i = lane; i < ncur; i += 32) {
-            int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
-            uint8_t v = runs.v[cur + i];
-            // the first run above with end + 1 >= a0 (unionfind.c:124)
-            int64_t lo = 0, hi = nprev;
-            while (lo < hi) {
-                int64_t mid = (lo + hi) >> 1;
-                if ((int64_t)runs.end[prev + mid] + 1 < a0)
-                    lo = mid + 1;
-                else
-                    hi = mid;
-            }
-            for (int64_t k = lo; k < nprev && (int64_t)runs.start[prev + k] <= a1 + 1; k++) {
-                if (runs.v[prev + k] != v) continue;
-                if (runs_touch(a0, a1, runs.start[prev + k], runs.end[prev + k], v))
-                    uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + k));
-            }
+// Runs and the unions inside a band of R rows, all in shared memory: the
+// band's runs (slot r*qw + i for run i of band row r), their union-find
+// (link the larger root under the smaller, so a root is its piece's
+// smallest slot, which is also the piece's smallest global id), and each
+// root's pixel sum. Each run's global parent becomes its band-local root;
+// the band-local roots (and the last-column nodes, one-pixel roots) go to
+// a list, the only nodes the merges across bands touch.
+#define BAND_MAX_ROWS 16
+
+__device__ __forceinline__ uint32_t sm_find(uint32_t *par, uint32_t x) {
+    volatile uint32_t *p = par;
+    uint32_t px = p[x];
+    while (px != x) {
+        uint32_t ppx = p[px];
+        if (ppx != px) p[x] = ppx;
+        x = px;
+        px = p[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void sm_unite(uint32_t *par, uint32_t a, uint32_t b) {
+    for (;;) {
+        a = sm_find(par, a);
+        b = sm_find(par, b);
+        if (a == b) return;
+        if (a < b) {
+            uint32_t t = a;
+            a = b;
+            b = t;
         }
-        if (lane == 0 && ncur > 0) {
-            // a white run ending at w-2 joins pixel (w-1, y-1) when that is
-            // white and (w-2, y-1) is not (unionfind.c:89-97)
-            int64_t last = cur + ncur - 1;
-            const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
-            if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
-                uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
-        }
+        if (atomicCAS(par + a, a, b) == a) return;
     }
 }
 
-// The root of x without writes. After the unions, k_flatten must not use
-// uf_find: a path-halving write that read its value before another thread
-// stored the root would put a non-root parent back.
+// The runs of row y of slots [base, base + n) that touch run (a0, a1, v),
+// in order, by binary search for the first with end + 1 >= a0.
+#define FOR_TOUCHING(SE, V, base, n, a0, a1, v, k, BODY)                                 \
+    {                                                                                     \
+        int64_t lo_ = 0, hi_ = (n);                                                       \
+        while (lo_ < hi_) {                                                               \
+            int64_t mid_ = (lo_ + hi_) >> 1;                                              \
+            if ((int64_t)((SE)[(base) + mid_] >> 16) + 1 < (a0))                          \
+                lo_ = mid_ + 1;                                                           \
+            else                                                                          \
+                hi_ = mid_;                                                               \
+        }                                                                                 \
+        for (int64_t k = lo_; k < (n) && (int64_t)((SE)[(base) + k] & 0xffff) <= (a1) + 1; k++) { \
+            if ((V)[(base) + k] != (v)) continue;                                         \
+            if (runs_touch((a0), (a1), (SE)[(base) + k] & 0xffff, (SE)[(base) + k] >> 16, (v))) BODY \
+        }                                                                                 \
+    }
+
+__global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
+                                               uint32_t *row_nruns, int R, int64_t slot_w, uint32_t *broots,
+                                               uint32_t *nbroots) {
+    extern __shared__ __align__(16) unsigned char band_smem[];
+    const int64_t cap = (int64_t)R * slot_w;
+    uint32_t *s_par = reinterpret_cast<uint32_t *>(band_smem);
+    uint32_t *s_se = s_par + cap;   // start | end << 16
+    uint32_t *s_px = s_se + cap;    // pixel sum at a root
+    uint8_t *s_v = reinterpret_cast<uint8_t *>(s_px + cap);
+    __shared__ uint32_t s_cnt[BAND_MAX_ROWS];
+    __shared__ uint32_t sh[32];
+    __shared__ uint32_t s_base;
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t y0 = (int64_t)blockIdx.x * R;
+    if (y0 >= f.qh) return;
+    const int64_t y1 = dmin(y0 + R, (int64_t)f.qh);
+    const int nrows = (int)(y1 - y0);
+    const int qw = f.qw;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    // 1. the runs of each row (fast/threshold.c:210-266): one warp per row,
+    // the run starts of 32 columns at a time by ballot; runs of 127 dropped
+    for (int r = warp; r < nrows; r += nwarps) {
+        const int64_t y = y0 + r;
+        const uint8_t *t = thr + f.q_off + y * qw;
+        const int64_t sb = (int64_t)r * qw;
+        const int64_t xmax = qw - 2;
+        int64_t count = 0, open = -1;
+        for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
+            int64_t x = x0 + lane;
+            bool valid = x <= xmax;
+            uint8_t v = valid ? t[x] : 0;
+            bool start = valid && (x == 0 || t[x - 1] != v);
+            uint32_t S = __ballot_sync(0xffffffffu, start);
+            uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
+            // the starts first: a run's start and end share one word
+            if (start && v != 127) {
+                int64_t sl = sb + count + __popc(N & lt);
+                s_se[sl] = (uint32_t)x;
+                s_v[sl] = v;
+            }
+            __syncwarp();
+            if (start) {
+                uint32_t below = S & lt;
+                int64_t prev_slot;
+                if (below) {
+                    int pl = 31 - __clz(below);
+                    prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
+                } else {
+                    prev_slot = open;
+                }
+                if (prev_slot >= 0) s_se[sb + prev_slot] |= (uint32_t)(x - 1) << 16;
+            }
+            __syncwarp();
+            if (S) {
+                int ls = 31 - __clz(S);
+                open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
+            }
+            count += __popc(N);
+        }
+        if (lane == 0) {
+            if (open >= 0) s_se[sb + open] |= (uint32_t)xmax << 16;
+            s_cnt[r] = (uint32_t)count;
+            row_nruns[f.row0 + y] = (uint32_t)count;
+        }
+    }
+    __syncthreads();
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
+            int64_t sl = (int64_t)r * qw + i;
+            s_par[sl] = (uint32_t)sl;
+            s_px[sl] = 0;
+        }
+    __syncthreads();
+    // 2. the links between consecutive rows of the band (unionfind.c:112-146)
+    for (int r = 1; r < nrows; r++) {
+        const int64_t cb = (int64_t)r * qw, pb = cb - qw, np = s_cnt[r - 1];
+        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
+            uint32_t se = s_se[cb + i];
+            int64_t a0 = se & 0xffff, a1 = se >> 16;
+            uint8_t v = s_v[cb + i];
+            FOR_TOUCHING(s_se, s_v, pb, np, a0, a1, v, k, { sm_unite(s_par, (uint32_t)(cb + i), (uint32_t)(pb + k)); })
+        }
+    }
+    __syncthreads();
+    // 3. flatten the band's forest by pointer jumping (parallel, in place:
+    // a parent only ever moves up its tree), then each root's pixel sum
+    for (;;) {
+        int changed = 0;
+        for (int r = 0; r < nrows; r++)
+            for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
+                int64_t sl = (int64_t)r * qw + i;
+                uint32_t p = s_par[sl], pp = s_par[p];
+                if (pp != p) {
+                    s_par[sl] = pp;
+                    changed = 1;
+                }
+            }
+        if (!__syncthreads_or(changed)) break;
+    }
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i0 = 0; i0 < s_cnt[r]; i0 += blockDim.x) {
+            const int64_t i = i0 + threadIdx.x;
+            const bool valid = i < s_cnt[r];
+            const uint32_t live = __ballot_sync(0xffffffffu, valid);
+            if (!valid) continue;
+            int64_t sl = (int64_t)r * qw + i;
+            uint32_t se = s_se[sl];
+            uint32_t add = (se >> 16) - (se & 0xffff) + 1;
+            uint32_t root = s_par[sl];
+            // one shared-memory atomic per distinct root of the warp
+            uint32_t peers = __match_any_sync(live, root);
+            uint32_t sum = 0;
+            for (uint32_t m = peers; m; m &= m - 1) sum += __shfl_sync(peers, add, __ffs(m) - 1);
+            if (lane == __ffs(peers) - 1) atomicAdd(s_px + root, sum);
+        }
+    __syncthreads();
+    uint32_t nroot_thread = 0;
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
+            int64_t sl = (int64_t)r * qw + i;
+            uint32_t root = s_par[sl];
+            int64_t node = f.node_off + (y0 + r) * qw + i;
+            int64_t rr = root / qw;
+            runs.start[node] = (uint16_t)(s_se[sl] & 0xffff);
+            runs.end[node] = (uint16_t)(s_se[sl] >> 16);
+            runs.v[node] = s_v[sl];
+            runs.parent[node] = (uint32_t)(f.node_off + (y0 + rr) * qw + (root - rr * qw));
+            if (root == (uint32_t)sl) {
+                runs.px[node] = s_px[sl];
+                nroot_thread++;
+            }
+        }
+    // the last-column nodes of the band's rows: one-pixel roots
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+        int64_t vn = f.node_off + (int64_t)qw * f.qh + y0 + r;
+        runs.parent[vn] = (uint32_t)vn;
+        runs.px[vn] = 1;
+        nroot_thread++;
+    }
+    // append the band's roots to the list: one atomic per block
+    uint32_t total;
+    uint32_t off = block_excl_scan(nroot_thread, &total, sh);
+    if (threadIdx.x == 0) s_base = atomicAdd(nbroots, total);
+    __syncthreads();
+    uint32_t at = s_base + off;
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
+            int64_t sl = (int64_t)r * qw + i;
+            if (s_par[sl] == (uint32_t)sl) broots[at++] = (uint32_t)(f.node_off + (y0 + r) * qw + i);
+        }
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x)
+        broots[at++] = (uint32_t)(f.node_off + (int64_t)qw * f.qh + y0 + r);
+}
+
+// One level of the merge across bands, in global memory: the band
+// boundaries b (row b*R against the row above) with b a multiple of
+// base^level but not of base^(level+1); at level 0 also every row's
+// last-column link (unionfind.c:89-97). The groups merged at one level are
+// compressed (their roots point at their root), so finds stay short.
+#define MERGE_ROW_CAP 4096
+__global__ void k_merge_level(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, const uint32_t *row_nruns,
+                              int R, int64_t step, int first_level) {
+    __shared__ uint32_t s_se[MERGE_ROW_CAP];
+    __shared__ uint8_t s_v[MERGE_ROW_CAP];
+    const FrameDesc f = frames[blockIdx.y];
+    const int64_t nb = (f.qh + R - 1) / R;
+    // block k takes the k-th boundary of this level: b = step * (k + k / 7 + 1)
+    // skips the multiples of 8 * step
+    for (int64_t k = blockIdx.x; ; k += gridDim.x) {
+        const int64_t b = step * (k + k / 7 + 1);
+        if (b >= nb) break;
+        const int64_t y = b * R;
+        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
+        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
+        // the row above in shared memory (its runs are searched by every run)
+        const bool staged = nprev <= MERGE_ROW_CAP;
+        __syncthreads();
+        if (staged)
+            for (int64_t t = threadIdx.x; t < nprev; t += blockDim.x) {
+                s_se[t] = (uint32_t)runs.start[prev + t] | (uint32_t)runs.end[prev + t] << 16;
+                s_v[t] = runs.v[prev + t];
+            }
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
+            int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
+            uint8_t v = runs.v[cur + i];
+            if (staged) {
+                FOR_TOUCHING(s_se, s_v, 0, nprev, a0, a1, v, kk,
+                             { uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk)); })
+            } else {
+                int64_t lo = 0, hi = nprev;
+                while (lo < hi) {
+                    int64_t mid = (lo + hi) >> 1;
+                    if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                for (int64_t kk = lo; kk < nprev && (int64_t)runs.start[prev + kk] <= a1 + 1; kk++) {
+                    if (runs.v[prev + kk] != v) continue;
+                    if (runs_touch(a0, a1, runs.start[prev + kk], runs.end[prev + kk], v))
+                        uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk));
+                }
+            }
+        }
+    }
+    if (!first_level) return;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t y = 1 + tid; y < f.qh; y += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ncur = row_nruns[f.row0 + y];
+        if (ncur == 0) continue;
+        int64_t last = f.node_off + y * f.qw + ncur - 1;
+        const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
+        if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
+            uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
+    }
+}
+
+// The root of x without writes (after the unions: a path-halving write that
+// read its value before another thread stored a root would undo it).
 __device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
     const volatile uint32_t *p = par;
     uint32_t px = p[x];
@@ -343,22 +550,22 @@ __device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
     return x;
 }
 
-// Every node points at its root; each root sums its component's pixels.
-__global__ void k_flatten(const FrameDesc *frames, RunArrays runs, const uint32_t *row_nruns) {
-    const FrameDesc f = frames[blockIdx.y];
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t y = warp; y < f.qh; y += nwarps) {
-        const int64_t base = f.node_off + y * f.qw;
-        const int64_t n = row_nruns[f.row0 + y];
-        for (int64_t i = lane; i <= n; i += 32) {
-            int64_t node = i < n ? base + i : f.node_off + (int64_t)f.qw * f.qh + y;
-            uint32_t r = uf_root(runs.parent, (uint32_t)node);
-            runs.parent[node] = r;
-            uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
-            atomicAdd(runs.px + r, px);
-        }
+// Point each listed root at the root of its tree.
+__global__ void k_compress(uint32_t *parent, const uint32_t *broots, const uint32_t *nbroots) {
+    const int64_t n = *nbroots;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x = broots[i];
+        parent[x] = uf_root(parent, x);
+    }
+}
+
+// Each band root that is not a final root adds its band's pixels to it.
+__global__ void k_roots_px(const uint32_t *parent, uint32_t *px, const uint32_t *broots, const uint32_t *nbroots) {
+    const int64_t n = *nbroots;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x = broots[i];
+        uint32_t r = uf_root(parent, x);
+        if (r != x) atomicAdd(px + r, px[x]);
     }
 }
 
@@ -415,32 +622,6 @@ __device__ __forceinline__ uint32_t point_mask(const uint8_t *a, const uint8_t *
     return c10 | c01 << 1 | (cm1 & (left11 ^ 1u)) << 2 | c11 << 3;
 }
 
-// Block-wide exclusive scan of one value per thread (blockDim <= 1024).
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total, uint32_t *sh) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    uint32_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    __syncthreads();
-    if (lane == 31) sh[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t s = lane < nw ? sh[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += t;
-        }
-        if (lane < nw) sh[lane] = s;
-    }
-    __syncthreads();
-    uint32_t off = wid > 0 ? sh[wid - 1] : 0;
-    *total = sh[nw - 1];
-    return off + incl - v;
-}
 
 __global__ void k_point_count(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, uint64_t *row_npts) {
     __shared__ uint32_t sh[32];
@@ -602,30 +783,37 @@ __device__ __forceinline__ void leaf_network(uint64_t *k, int n) {
 // Sort (key, val) pairs ascending by key, in place, n items (any n): a
 // bitonic network with every comparator ascending; partners past n act as
 // +infinity and are skipped.
-__device__ void block_sort_pairs(uint64_t *key, uint32_t *val, int64_t n) {
-    int64_t P = 1;
-    while (P < n) P <<= 1;
-    for (int64_t k = 2; k <= P; k <<= 1) {
-        for (int64_t j = k >> 1; j > 0; j >>= 1) {
-            for (int64_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+__device__ void block_sort_pairs(uint64_t *key, uint32_t *val, int64_t n64) {
+    const int n = (int)n64;
+    int P = 1, lp = 0;
+    while (P < n) {
+        P <<= 1;
+        lp++;
+    }
+    for (int lk = 1; lk <= lp; lk++) {
+        const int k = 1 << lk;
+        for (int lj = lk - 1; lj >= 0; lj--) {
+            const int j = 1 << lj;
+            for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
                 // comparator t of this step: i < p
-                int64_t i, p;
-                if (j == (k >> 1)) {
-                    int64_t blk = t / j, off = t % j;
-                    i = blk * k + off;
-                    p = blk * k + k - 1 - off;
+                const int blk = t >> lj, off = t & (j - 1);
+                int i, p;
+                if (lj == lk - 1) {
+                    i = (blk << lk) + off;
+                    p = (blk << lk) + k - 1 - off;
                 } else {
-                    int64_t blk = t / j, off = t % j;
-                    i = blk * 2 * j + off;
+                    i = (blk << (lj + 1)) + off;
                     p = i + j;
                 }
-                if (p < n && key[p] < key[i]) {
-                    uint64_t tk = key[i];
-                    key[i] = key[p];
-                    key[p] = tk;
-                    uint32_t tv = val[i];
-                    val[i] = val[p];
-                    val[p] = tv;
+                if (p < n) {
+                    const uint64_t ki = key[i], kp = key[p];
+                    if (kp < ki) {
+                        key[i] = kp;
+                        key[p] = ki;
+                        const uint32_t tv = val[i];
+                        val[i] = val[p];
+                        val[p] = tv;
+                    }
                 }
             }
             __syncthreads();
@@ -712,32 +900,6 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
     *mse = eig_small;
 }
 
-// The k-th largest (0-based) of v[0..n) by quickselect; v is reordered.
-__device__ double kth_largest(double *v, int64_t n, int64_t k) {
-    int64_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        double pivot = v[(lo + hi) / 2];
-        int64_t i = lo, j = hi;
-        while (i <= j) {
-            while (v[i] > pivot) i++;
-            while (v[j] < pivot) j--;
-            if (i <= j) {
-                double t = v[i];
-                v[i] = v[j];
-                v[j] = t;
-                i++;
-                j--;
-            }
-        }
-        if (k <= j)
-            hi = j;
-        else if (k >= i)
-            lo = i;
-        else
-            break;
-    }
-    return v[k];
-}
 
 // Two size classes of clusters, one kernel template: 128 threads for
 // clusters of at most FIT_SMALL points (everything staged in shared
@@ -752,6 +914,18 @@ __device__ double kth_largest(double *v, int64_t n, int64_t k) {
 __host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk) {
     return (size_t)sort_cap * 12 + (size_t)chunk * 24;
 }
+
+// Optional phase timers of the fit kernel (a -DAT_FIT_PROF build only).
+#ifdef AT_FIT_PROF
+__device__ long long g_fitprof[16384][12];
+#define FIT_PROF(k)                                              \
+    if (tid == 0 && c < 16384) g_fitprof[c][k] = clock64();
+extern "C" int at_fit_prof_copy(void *dst, int n) {
+    return (int)cudaMemcpyFromSymbol(dst, g_fitprof, (size_t)n * 12 * 8);
+}
+#else
+#define FIT_PROF(k)
+#endif
 
 template <int NT>
 __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
@@ -768,7 +942,6 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
     __shared__ int s_rev, s_ok;
     __shared__ uint32_t s_bb[4][NT / 32];
     __shared__ uint32_t s_scan[32];
-    __shared__ int64_t s_nm;
     __shared__ double s_perr[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pmse[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA],
         s_pnx[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pny[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA];
     const int tid = threadIdx.x;
@@ -784,6 +957,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             if (tid == 0) atomicOr(err, AT_ERR_CLUSTER_TOO_BIG);
             continue;
         }
+        FIT_PROF(1)
         const uint64_t *P = pts + s0;
         // bounding box (fast/quads.c:515-528)
         uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
@@ -818,6 +992,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
         const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
 
+        FIT_PROF(2)
         // angle keys, and the dot product of offsets and gradients: 8 lanes
         // over the whole groups of 8, then the rest (fast/quads.c:467-512)
         uint64_t *keys = scr.keys + s0;
@@ -826,14 +1001,36 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             keys[i] = angle_key(dx, dy, (uint32_t)i);
         }
         const int64_t nv = sz - sz % 8;
-        if (tid < 8) {
+        {
+            // the terms dx*gx + dy*gy by all threads into shared memory (the
+            // moment staging area, free here), then lane l < 8 sums terms
+            // l, l+8, ... in order
+            float *s_term = reinterpret_cast<float *>(s_w);
+            const int64_t tcap = 6 * (int64_t)chunk;  // a multiple of 8
             float acc = 0.0f;
-            for (int64_t i = tid; i < nv; i += 8) {
-                float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
-                float gx = (float)(int16_t)(P[i] >> 32 & 0xffff), gy = (float)(int16_t)(P[i] >> 48);
-                acc = __fadd_rn(acc, __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy)));
+            for (int64_t c0 = 0; c0 < nv; c0 += tcap) {
+                const int64_t cn = dmin(tcap, nv - c0);
+                for (int64_t i = tid; i < cn; i += NT) {
+                    uint64_t pt = P[c0 + i];
+                    float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
+                    float gx = (float)(int16_t)(pt >> 32 & 0xffff), gy = (float)(int16_t)(pt >> 48);
+                    s_term[i] = __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy));
+                }
+                __syncthreads();
+                if (tid < 8) {
+                    int64_t i = tid;
+                    for (; i + 56 < cn; i += 64) {
+                        float v[8];
+#pragma unroll
+                        for (int u = 0; u < 8; u++) v[u] = s_term[i + 8 * u];
+#pragma unroll
+                        for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, v[u]);
+                    }
+                    for (; i < cn; i += 8) acc = __fadd_rn(acc, s_term[i]);
+                }
+                __syncthreads();
             }
-            s_lane[tid] = acc;
+            if (tid < 8) s_lane[tid] = acc;
         }
         __syncthreads();
         if (tid == 0) {
@@ -862,6 +1059,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         // block head and its place in the leaf; then one sort by (head,
         // place), packed into 64 bits as head's slope bits, 0xffff - head's
         // index, and the place.
+        FIT_PROF(3)
         const bool in_smem = sz <= sort_cap;
         uint64_t *sk = in_smem ? s_key : scr.skey + s0;
         uint32_t *sv = in_smem ? s_val : scr.sval + s0;
@@ -881,7 +1079,9 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             }
         }
         __syncthreads();
+        FIT_PROF(4)
         block_sort_pairs(sk, sv, sz);
+        FIT_PROF(5)
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
         // w = sqrt(gx^2 + gy^2) + 1 on the quad image (1 at its border),
@@ -917,18 +1117,34 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
                 const int cb = tid == 2 ? 0 : tid == 3 || tid == 4 ? 1 : 2;
                 const double *A = ca == 0 ? s_fx : s_fy, *Bv = cb == 0 ? s_fx : s_fy;
                 double *o = mout + k0;
-#pragma unroll 4
-                for (int64_t t = 0; t < kn; t++) {
-                    double w = s_w[t];
+                // 8 terms at a time: their loads and products first, then the
+                // 8 dependent additions (the terms do not depend on the sum)
+                int64_t t = 0;
+                for (; t + 8 <= kn; t += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        double a = ca == 2 ? 1.0 : A[t + u];
+                        double b = cb == 2 ? 1.0 : Bv[t + u];
+                        v[u] = __dmul_rn(__dmul_rn(s_w[t + u], a), b);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        run = __dadd_rn(run, v[u]);
+                        o[t + u] = run;
+                    }
+                }
+                for (; t < kn; t++) {
                     double a = ca == 2 ? 1.0 : A[t];
                     double b = cb == 2 ? 1.0 : Bv[t];
-                    run = __dadd_rn(run, __dmul_rn(__dmul_rn(w, a), b));
+                    run = __dadd_rn(run, __dmul_rn(__dmul_rn(s_w[t], a), b));
                     o[t] = run;
                 }
             }
             __syncthreads();
         }
         const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
+        FIT_PROF(6)
 
         // corner search (fast/quads.c:788-959)
         const int64_t ksz = dmin(20, sz / 12);
@@ -964,6 +1180,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             filt[i] = acc;
         }
         __syncthreads();
+        FIT_PROF(7)
         // local maxima with wrap-around, compacted in index order
         int32_t *mxi = scr.mxi + s0;
         double *mxe = scr.mxe + s0;
@@ -989,18 +1206,36 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         int64_t nm = nm_run;
         if (nm < 4) continue;
         if (nm > prm.max_nmaxima) {
-            if (tid == 0) {
-                double *sel = filt;  // free now: a copy of the maxima's errors
-                for (int64_t i = 0; i < nm; i++) sel[i] = mxe[i];
-                double thresh = kth_largest(sel, nm, prm.max_nmaxima);
-                int64_t o = 0;
-                for (int64_t i = 0; i < nm; i++)
-                    if (mxe[i] > thresh) mxi[o++] = mxi[i];
-                s_nm = o;
+            // The reference keeps the maxima whose error is above the
+            // (max_nmaxima+1)-th largest (its quickselect, quads.c:827-862).
+            // e_i exceeds that order statistic exactly when at most
+            // max_nmaxima errors are >= e_i: a parallel count, then an
+            // order-keeping compaction.
+            const int64_t k = prm.max_nmaxima;
+            double *e = in_smem && nm <= sort_cap ? reinterpret_cast<double *>(s_key) : filt;
+            for (int64_t i = tid; i < nm; i += NT) e[i] = mxe[i];
+            __syncthreads();
+            int64_t kept_run = 0;
+            for (int64_t i0 = 0; i0 < nm; i0 += NT) {
+                int64_t i = i0 + tid;
+                uint32_t keep = 0;
+                if (i < nm) {
+                    double ei = e[i];
+                    int64_t ge = 0;
+                    for (int64_t j = 0; j < nm && ge <= k; j++) ge += e[j] >= ei;
+                    keep = ge <= k;
+                }
+                uint32_t total;
+                uint32_t off = block_excl_scan(keep, &total, s_scan);
+                int32_t mi = i < nm ? mxi[i] : 0;
+                __syncthreads();
+                if (keep) mxi[kept_run + off] = mi;
+                kept_run += total;
             }
             __syncthreads();
-            nm = s_nm;
+            nm = kept_run;
         }
+        FIT_PROF(8)
         // line fits of pairs of maxima: (a, b), a < b, and the closing pair
         // (b, a) wrapping around for b >= a + 3
         for (int64_t t = tid; t < nm * nm; t += NT) {
@@ -1018,6 +1253,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             s_pny[t] = lp[3];
         }
         __syncthreads();
+        FIT_PROF(9)
         if (tid == 0) {
             const double inf = __longlong_as_double(0x7ff0000000000000ll);
             double best = inf;
@@ -1105,6 +1341,10 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
                 quads[c] = q;
                 quad_ok[c] = 1;
             }
+            FIT_PROF(10)
+#ifdef AT_FIT_PROF
+            if (c < 16384) g_fitprof[c][0] = sz;
+#endif
         }
         __syncthreads();
     }
@@ -1798,12 +2038,38 @@ void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uin
     k_morph<<<frame_grid(L), 256, 0, L.stream>>>(frames, tmp, thr, 0);
 }
 
-void launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
-                    uint32_t *lab, int32_t min_px) {
-    k_runs<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
-    k_union<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
-    k_flatten<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns);
+int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
+                    uint32_t *lab, int32_t min_px, int64_t max_qw, int64_t max_qh, uint32_t *broots,
+                    uint32_t *nbroots) {
+    // rows per band: as many as keep the band's runs (13 B a slot, qw slots
+    // a row) within about 110 KiB of shared memory
+    int R = (int)((110 * 1024) / (13 * (max_qw > 0 ? max_qw : 1)));
+    R = R < 2 ? 2 : R > BAND_MAX_ROWS ? BAND_MAX_ROWS : R;
+    size_t smem = (size_t)R * (size_t)max_qw * 13;
+    cudaFuncSetAttribute(k_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaMemsetAsync(nbroots, 0, 4, L.stream);
+    const int64_t nbands = (max_qh + R - 1) / R;
+    dim3 bg((unsigned)nbands, (unsigned)L.nframes);
+    k_band<<<bg, 512, smem, L.stream>>>(frames, thr, runs, row_nruns, R, max_qw, broots, nbroots);
+    // merge bands in groups of 8: level l joins the groups of 8^l bands
+    int64_t step = 1;
+    int level = 0, launched = 3;
+    const unsigned flat = 148 * 4;
+    do {
+        // boundaries of this level: multiples of step, not of 8 * step
+        int64_t nbl = (nbands - 1) / step - (nbands - 1) / (8 * step);
+        unsigned gx = (unsigned)(nbl > 0 ? (nbl < 148 * 8 ? nbl : 148 * 8) : 1);
+        if (level == 0 && gx < 8) gx = 8;
+        k_merge_level<<<dim3(gx, (unsigned)L.nframes), 256, 0, L.stream>>>(frames, thr, runs, row_nruns, R, step,
+                                                                           level == 0);
+        k_compress<<<flat, 256, 0, L.stream>>>(runs.parent, broots, nbroots);
+        step *= 8;
+        level++;
+        launched += 2;
+    } while (step < nbands);
+    k_roots_px<<<flat, 256, 0, L.stream>>>(runs.parent, runs.px, broots, nbroots);
     k_labels<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+    return launched;
 }
 
 void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
