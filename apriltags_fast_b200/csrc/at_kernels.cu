@@ -245,12 +245,21 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *par, uint32_t x) {
     return x;
 }
 
+// Roots are linked in the order of a bijective hash of their ids: one fixed
+// total order, so concurrent links can never form a cycle, and a random one,
+// so trees stay shallow (linking by id would chain the pieces of a row).
+// The label of a component, its smallest node id, is tracked apart.
+__device__ __forceinline__ uint32_t uf_rank(uint32_t x) {
+    uint32_t h = x * 0x9e3779b1u;
+    return h ^ (h >> 16);
+}
+
 __device__ __forceinline__ void uf_unite(uint32_t *par, uint32_t a, uint32_t b) {
     for (;;) {
         a = uf_find(par, a);
         b = uf_find(par, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_rank(a) < uf_rank(b)) {
             uint32_t t = a;
             a = b;
             b = t;
@@ -292,7 +301,7 @@ __device__ __forceinline__ void sm_unite(uint32_t *par, uint32_t a, uint32_t b) 
         a = sm_find(par, a);
         b = sm_find(par, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_rank(a) < uf_rank(b)) {
             uint32_t t = a;
             a = b;
             b = t;
@@ -319,6 +328,17 @@ __device__ __forceinline__ void sm_unite(uint32_t *par, uint32_t a, uint32_t b) 
         }                                                                                 \
     }
 
+#ifdef AT_BAND_PROF
+__device__ long long g_bandprof[4096][10];
+#define BAND_PROF(k)                                                              \
+    if (threadIdx.x == 0 && blockIdx.x < 4096) g_bandprof[blockIdx.x][k] = clock64();
+extern "C" int at_band_prof_copy(void *dst, int n) {
+    return (int)cudaMemcpyFromSymbol(dst, g_bandprof, (size_t)n * 10 * 8);
+}
+#else
+#define BAND_PROF(k)
+#endif
+
 __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                                                uint32_t *row_nruns, int R, int64_t slot_w, uint32_t *broots,
                                                uint32_t *nbroots) {
@@ -327,7 +347,8 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
     uint32_t *s_par = reinterpret_cast<uint32_t *>(band_smem);
     uint32_t *s_se = s_par + cap;   // start | end << 16
     uint32_t *s_px = s_se + cap;    // pixel sum at a root
-    uint8_t *s_v = reinterpret_cast<uint8_t *>(s_px + cap);
+    uint32_t *s_mn = s_px + cap;    // smallest slot of a piece, at its root
+    uint8_t *s_v = reinterpret_cast<uint8_t *>(s_mn + cap);
     __shared__ uint32_t s_cnt[BAND_MAX_ROWS];
     __shared__ uint32_t sh[32];
     __shared__ uint32_t s_base;
@@ -339,6 +360,7 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
     const int qw = f.qw;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
+    BAND_PROF(0)
     // 1. the runs of each row (fast/threshold.c:210-266): one warp per row,
     // the run starts of 32 columns at a time by ballot; runs of 127 dropped
     for (int r = warp; r < nrows; r += nwarps) {
@@ -393,6 +415,7 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
             s_px[sl] = 0;
         }
     __syncthreads();
+    BAND_PROF(1)
     // 2. the links between consecutive rows of the band (unionfind.c:112-146)
     for (int r = 1; r < nrows; r++) {
         const int64_t cb = (int64_t)r * qw, pb = cb - qw, np = s_cnt[r - 1];
@@ -404,6 +427,7 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
         }
     }
     __syncthreads();
+    BAND_PROF(2)
     // 3. flatten the band's forest by pointer jumping (parallel, in place:
     // a parent only ever moves up its tree), then each root's pixel sum
     for (;;) {
@@ -419,6 +443,8 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
             }
         if (!__syncthreads_or(changed)) break;
     }
+    BAND_PROF(3)
+    // each piece's pixel sum, kept at its root
     for (int r = 0; r < nrows; r++)
         for (int64_t i0 = 0; i0 < s_cnt[r]; i0 += blockDim.x) {
             const int64_t i = i0 + threadIdx.x;
@@ -436,19 +462,43 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
             if (lane == __ffs(peers) - 1) atomicAdd(s_px + root, sum);
         }
     __syncthreads();
+    BAND_PROF(4)
+    // the smallest slot of each piece: the lowest slot whose root is the
+    // piece's root. The slots are in increasing order along rows and
+    // rows, so the first slot (in slot order) with a root is its minimum:
+    // mark it with an atomicMin on the root's entry of s_mn.
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) s_mn[(int64_t)r * qw + i] = 0xffffffffu;
+    __syncthreads();
+    for (int r = 0; r < nrows; r++)
+        for (int64_t i0 = 0; i0 < s_cnt[r]; i0 += blockDim.x) {
+            const int64_t i = i0 + threadIdx.x;
+            const bool valid = i < s_cnt[r];
+            const uint32_t live = __ballot_sync(0xffffffffu, valid);
+            if (!valid) continue;
+            uint32_t sl = (uint32_t)((int64_t)r * qw + i);
+            uint32_t root = s_par[sl];
+            uint32_t peers = __match_any_sync(live, root);
+            if (lane == __ffs(peers) - 1) atomicMin(s_mn + root, sl);  // lowest lane: smallest slot
+        }
+    __syncthreads();
+    BAND_PROF(5)
+    // each run's global parent: its piece's smallest node (the band root)
     uint32_t nroot_thread = 0;
     for (int r = 0; r < nrows; r++)
         for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
             int64_t sl = (int64_t)r * qw + i;
             uint32_t root = s_par[sl];
+            uint32_t mn = s_mn[root];
             int64_t node = f.node_off + (y0 + r) * qw + i;
-            int64_t rr = root / qw;
+            int64_t mr = mn / qw;
             runs.start[node] = (uint16_t)(s_se[sl] & 0xffff);
             runs.end[node] = (uint16_t)(s_se[sl] >> 16);
             runs.v[node] = s_v[sl];
-            runs.parent[node] = (uint32_t)(f.node_off + (y0 + rr) * qw + (root - rr * qw));
-            if (root == (uint32_t)sl) {
-                runs.px[node] = s_px[sl];
+            runs.parent[node] = (uint32_t)(f.node_off + (y0 + mr) * qw + (mn - mr * qw));
+            if (mn == (uint32_t)sl) {
+                runs.px[node] = s_px[root];
+                runs.minid[node] = (uint32_t)node;
                 nroot_thread++;
             }
         }
@@ -457,8 +507,10 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
         int64_t vn = f.node_off + (int64_t)qw * f.qh + y0 + r;
         runs.parent[vn] = (uint32_t)vn;
         runs.px[vn] = 1;
+        runs.minid[vn] = (uint32_t)vn;
         nroot_thread++;
     }
+    BAND_PROF(6)
     // append the band's roots to the list: one atomic per block
     uint32_t total;
     uint32_t off = block_excl_scan(nroot_thread, &total, sh);
@@ -468,10 +520,11 @@ __global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uin
     for (int r = 0; r < nrows; r++)
         for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
             int64_t sl = (int64_t)r * qw + i;
-            if (s_par[sl] == (uint32_t)sl) broots[at++] = (uint32_t)(f.node_off + (y0 + r) * qw + i);
+            if (s_mn[s_par[sl]] == (uint32_t)sl) broots[at++] = (uint32_t)(f.node_off + (y0 + r) * qw + i);
         }
     for (int r = threadIdx.x; r < nrows; r += blockDim.x)
         broots[at++] = (uint32_t)(f.node_off + (int64_t)qw * f.qh + y0 + r);
+    BAND_PROF(7)
 }
 
 // One level of the merge across bands, in global memory: the band
@@ -538,6 +591,120 @@ __global__ void k_merge_level(const FrameDesc *frames, const uint8_t *thr, RunAr
     }
 }
 
+// The flat form of the same union-find: one block per row, one thread per
+// run, links in global memory (hash-ordered, so trees stay shallow), then
+// one pass that sums each component's pixels and smallest node at its root.
+#define ROW_STAGE 4096
+
+__global__ void __launch_bounds__(256) k_row_runs(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
+                                                  uint32_t *row_nruns) {
+    __shared__ __align__(16) uint8_t s_row[ROW_STAGE + 16];
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int64_t y = blockIdx.x; y < f.qh; y += gridDim.x) {
+        const uint8_t *t = thr + f.q_off + y * f.qw;
+        const int64_t base = f.node_off + y * f.qw;
+        const int64_t xmax = f.qw - 2;
+        const bool staged = f.qw <= ROW_STAGE;
+        __syncthreads();
+        if (staged)
+            for (int64_t x = threadIdx.x; x < f.qw; x += blockDim.x) s_row[x] = t[x];
+        __syncthreads();
+        const uint8_t *row = staged ? s_row : t;
+        if (warp == 0) {
+            int64_t count = 0, open = -1;
+            for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
+                int64_t x = x0 + lane;
+                bool valid = x <= xmax;
+                uint8_t v = valid ? row[x] : 0;
+                bool start = valid && (x == 0 || row[x - 1] != v);
+                uint32_t S = __ballot_sync(0xffffffffu, start);
+                uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
+                if (start) {
+                    uint32_t below = S & lt;
+                    int64_t prev_slot;
+                    if (below) {
+                        int pl = 31 - __clz(below);
+                        prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
+                    } else {
+                        prev_slot = open;
+                    }
+                    if (prev_slot >= 0) runs.end[base + prev_slot] = (uint16_t)(x - 1);
+                    if (v != 127) {
+                        int64_t sl = base + count + __popc(N & lt);
+                        runs.start[sl] = (uint16_t)x;
+                        runs.v[sl] = v;
+                        runs.parent[sl] = (uint32_t)sl;
+                        runs.px[sl] = 0;
+                        runs.minid[sl] = 0xffffffffu;
+                    }
+                }
+                if (S) {
+                    int ls = 31 - __clz(S);
+                    open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
+                }
+                count += __popc(N);
+            }
+            if (lane == 0) {
+                if (open >= 0) runs.end[base + open] = (uint16_t)xmax;
+                row_nruns[f.row0 + y] = (uint32_t)count;
+                int64_t vn = f.node_off + (int64_t)f.qw * f.qh + y;
+                runs.parent[vn] = (uint32_t)vn;
+                runs.px[vn] = 0;
+                runs.minid[vn] = 0xffffffffu;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_row_union(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
+                                                   const uint32_t *row_nruns) {
+    __shared__ uint32_t s_se[ROW_STAGE];
+    __shared__ uint8_t s_v[ROW_STAGE];
+    const FrameDesc f = frames[blockIdx.y];
+    for (int64_t y = 1 + blockIdx.x; y < f.qh; y += gridDim.x) {
+        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
+        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
+        const bool staged = nprev <= ROW_STAGE;
+        __syncthreads();
+        if (staged)
+            for (int64_t t = threadIdx.x; t < nprev; t += blockDim.x) {
+                s_se[t] = (uint32_t)runs.start[prev + t] | (uint32_t)runs.end[prev + t] << 16;
+                s_v[t] = runs.v[prev + t];
+            }
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
+            int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
+            uint8_t v = runs.v[cur + i];
+            if (staged) {
+                FOR_TOUCHING(s_se, s_v, 0, nprev, a0, a1, v, kk,
+                             { uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk)); })
+            } else {
+                int64_t lo = 0, hi = nprev;
+                while (lo < hi) {
+                    int64_t mid = (lo + hi) >> 1;
+                    if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                for (int64_t kk = lo; kk < nprev && (int64_t)runs.start[prev + kk] <= a1 + 1; kk++) {
+                    if (runs.v[prev + kk] != v) continue;
+                    if (runs_touch(a0, a1, runs.start[prev + kk], runs.end[prev + kk], v))
+                        uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk));
+                }
+            }
+        }
+        if (threadIdx.x == 0 && ncur > 0) {
+            int64_t last = cur + ncur - 1;
+            const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
+            if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
+                uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
+        }
+    }
+}
+
 // The root of x without writes (after the unions: a path-halving write that
 // read its value before another thread stored a root would undo it).
 __device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
@@ -559,13 +726,50 @@ __global__ void k_compress(uint32_t *parent, const uint32_t *broots, const uint3
     }
 }
 
-// Each band root that is not a final root adds its band's pixels to it.
-__global__ void k_roots_px(const uint32_t *parent, uint32_t *px, const uint32_t *broots, const uint32_t *nbroots) {
+// Each band root that is not a final root adds its band's pixels to it, and
+// offers its id as the component's smallest (the label).
+__global__ void k_roots_px(const uint32_t *parent, uint32_t *px, uint32_t *minid, const uint32_t *broots,
+                           const uint32_t *nbroots) {
     const int64_t n = *nbroots;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         uint32_t x = broots[i];
         uint32_t r = uf_root(parent, x);
-        if (r != x) atomicAdd(px + r, px[x]);
+        if (r != x) {
+            atomicAdd(px + r, px[x]);
+            atomicMin(minid + r, x);
+        }
+    }
+}
+
+// Each node adds its pixels and offers its id to its root (one atomic per
+// distinct root of a warp).
+__global__ void __launch_bounds__(256) k_row_sums(const FrameDesc *frames, RunArrays runs, const uint32_t *row_nruns) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    for (int64_t y = blockIdx.x; y < f.qh; y += gridDim.x) {
+        const int64_t base = f.node_off + y * f.qw;
+        const int64_t n = row_nruns[f.row0 + y];
+        for (int64_t i0 = 0; i0 <= n; i0 += blockDim.x) {
+            const int64_t i = i0 + threadIdx.x;
+            const bool valid = i <= n;
+            const uint32_t live = __ballot_sync(0xffffffffu, valid);
+            if (!valid) continue;
+            const int64_t node = i < n ? base + i : f.node_off + (int64_t)f.qw * f.qh + y;
+            const uint32_t r = uf_root(runs.parent, (uint32_t)node);
+            const uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
+            const uint32_t peers = __match_any_sync(live, r);
+            uint32_t sum = 0, mn = 0xffffffffu;
+            for (uint32_t m = peers; m; m &= m - 1) {
+                int src = __ffs(m) - 1;
+                sum += __shfl_sync(peers, px, src);
+                uint32_t o = __shfl_sync(peers, (uint32_t)node, src);
+                mn = o < mn ? o : mn;
+            }
+            if (lane == __ffs(peers) - 1) {
+                atomicAdd(runs.px + r, sum);
+                atomicMin(runs.minid + r, mn);
+            }
+        }
     }
 }
 
@@ -595,7 +799,7 @@ __global__ void k_labels(const FrameDesc *frames, const RunArrays runs, const ui
         uint32_t l = AT_NOK;
         if (node >= 0) {
             uint32_t r = uf_root(runs.parent, (uint32_t)node);
-            if ((int64_t)runs.px[r] >= min_px) l = r;
+            if ((int64_t)runs.px[r] >= min_px) l = runs.minid[r];
         }
         lab[f.q_off + i] = l;
     }
@@ -2039,37 +2243,17 @@ void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uin
 }
 
 int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
-                    uint32_t *lab, int32_t min_px, int64_t max_qw, int64_t max_qh, uint32_t *broots,
-                    uint32_t *nbroots) {
-    // rows per band: as many as keep the band's runs (13 B a slot, qw slots
-    // a row) within about 110 KiB of shared memory
-    int R = (int)((110 * 1024) / (13 * (max_qw > 0 ? max_qw : 1)));
-    R = R < 2 ? 2 : R > BAND_MAX_ROWS ? BAND_MAX_ROWS : R;
-    size_t smem = (size_t)R * (size_t)max_qw * 13;
-    cudaFuncSetAttribute(k_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaMemsetAsync(nbroots, 0, 4, L.stream);
-    const int64_t nbands = (max_qh + R - 1) / R;
-    dim3 bg((unsigned)nbands, (unsigned)L.nframes);
-    k_band<<<bg, 512, smem, L.stream>>>(frames, thr, runs, row_nruns, R, max_qw, broots, nbroots);
-    // merge bands in groups of 8: level l joins the groups of 8^l bands
-    int64_t step = 1;
-    int level = 0, launched = 3;
-    const unsigned flat = 148 * 4;
-    do {
-        // boundaries of this level: multiples of step, not of 8 * step
-        int64_t nbl = (nbands - 1) / step - (nbands - 1) / (8 * step);
-        unsigned gx = (unsigned)(nbl > 0 ? (nbl < 148 * 8 ? nbl : 148 * 8) : 1);
-        if (level == 0 && gx < 8) gx = 8;
-        k_merge_level<<<dim3(gx, (unsigned)L.nframes), 256, 0, L.stream>>>(frames, thr, runs, row_nruns, R, step,
-                                                                           level == 0);
-        k_compress<<<flat, 256, 0, L.stream>>>(runs.parent, broots, nbroots);
-        step *= 8;
-        level++;
-        launched += 2;
-    } while (step < nbands);
-    k_roots_px<<<flat, 256, 0, L.stream>>>(runs.parent, runs.px, broots, nbroots);
+                   uint32_t *lab, int32_t min_px, int64_t max_qw, int64_t max_qh, uint32_t *broots,
+                   uint32_t *nbroots) {
+    (void)max_qw;
+    (void)broots;
+    (void)nbroots;
+    dim3 rg((unsigned)(max_qh < 148 * 16 ? max_qh : 148 * 16), (unsigned)L.nframes);
+    k_row_runs<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
     k_labels<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
-    return launched;
+    return 4;
 }
 
 void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,

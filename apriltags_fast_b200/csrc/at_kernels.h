@@ -9,8 +9,9 @@
 struct RunArrays {
     uint16_t *start, *end;
     uint8_t *v;
-    uint32_t *parent;  // union-find parent (after k_flatten: the root)
+    uint32_t *parent;  // union-find parent
     uint32_t *px;      // at a root: its component's pixel count
+    uint32_t *minid;   // at a root: its component's smallest node id (the label)
 };
 
 // Per-point scratch of the quad fit, indexed by point position.
