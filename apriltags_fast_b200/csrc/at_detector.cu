@@ -83,7 +83,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_BROOTS, B_NBROOTS, B_MINID,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -395,16 +395,10 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     RunArrays runs{B[B_RSTART].as<uint16_t>(), B[B_REND].as<uint16_t>(), B[B_RV].as<uint8_t>(),
                    B[B_PARENT].as<uint32_t>(), B[B_PX].as<uint32_t>(), B[B_MINID].as<uint32_t>()};
     uint32_t *lab = B[B_LAB].as<uint32_t>();
-    int64_t max_qw = 0, max_qh = 0;
-    for (auto &f : fd) {
-        max_qw = f.qw > max_qw ? f.qw : max_qw;
-        max_qh = f.qh > max_qh ? f.qh : max_qh;
-    }
-    CK(B[B_BROOTS].ensure(nodes * 4));
-    CK(B[B_MINID].ensure(nodes * 4));
-    CK(B[B_NBROOTS].ensure(4));
+    int64_t max_qh = 0;
+    for (auto &f : fd) max_qh = f.qh > max_qh ? f.qh : max_qh;
     in->launches += launch_segment(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), lab, td->qtp.min_cluster_pixels,
-                                   max_qw, max_qh, B[B_BROOTS].as<uint32_t>(), B[B_NBROOTS].as<uint32_t>());
+                                   max_qh);
     CK(cudaEventRecord(in->ev[4], st));
     CK(cudaGetLastError());
 

@@ -275,41 +275,6 @@ __device__ __forceinline__ bool runs_touch(int64_t a0, int64_t a1, int64_t b0, i
     return dmax(dmax(a0, b0 - 1), 1) <= dmin(a1, b1 - 1);
 }
 
-// Runs and the unions inside a band of R rows, all in shared memory: the
-// band's runs (slot r*qw + i for run i of band row r), their union-find
-// (link the larger root under the smaller, so a root is its piece's
-// smallest slot, which is also the piece's smallest global id), and each
-// root's pixel sum. Each run's global parent becomes its band-local root;
-// the band-local roots (and the last-column nodes, one-pixel roots) go to
-// a list, the only nodes the merges across bands touch.
-#define BAND_MAX_ROWS 16
-
-__device__ __forceinline__ uint32_t sm_find(uint32_t *par, uint32_t x) {
-    volatile uint32_t *p = par;
-    uint32_t px = p[x];
-    while (px != x) {
-        uint32_t ppx = p[px];
-        if (ppx != px) p[x] = ppx;
-        x = px;
-        px = p[x];
-    }
-    return x;
-}
-
-__device__ __forceinline__ void sm_unite(uint32_t *par, uint32_t a, uint32_t b) {
-    for (;;) {
-        a = sm_find(par, a);
-        b = sm_find(par, b);
-        if (a == b) return;
-        if (uf_rank(a) < uf_rank(b)) {
-            uint32_t t = a;
-            a = b;
-            b = t;
-        }
-        if (atomicCAS(par + a, a, b) == a) return;
-    }
-}
-
 // The runs of row y of slots [base, base + n) that touch run (a0, a1, v),
 // in order, by binary search for the first with end + 1 >= a0.
 #define FOR_TOUCHING(SE, V, base, n, a0, a1, v, k, BODY)                                 \
@@ -327,269 +292,6 @@ __device__ __forceinline__ void sm_unite(uint32_t *par, uint32_t a, uint32_t b) 
             if (runs_touch((a0), (a1), (SE)[(base) + k] & 0xffff, (SE)[(base) + k] >> 16, (v))) BODY \
         }                                                                                 \
     }
-
-#ifdef AT_BAND_PROF
-__device__ long long g_bandprof[4096][10];
-#define BAND_PROF(k)                                                              \
-    if (threadIdx.x == 0 && blockIdx.x < 4096) g_bandprof[blockIdx.x][k] = clock64();
-extern "C" int at_band_prof_copy(void *dst, int n) {
-    return (int)cudaMemcpyFromSymbol(dst, g_bandprof, (size_t)n * 10 * 8);
-}
-#else
-#define BAND_PROF(k)
-#endif
-
-__global__ void __launch_bounds__(512) k_band(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
-                                               uint32_t *row_nruns, int R, int64_t slot_w, uint32_t *broots,
-                                               uint32_t *nbroots) {
-    extern __shared__ __align__(16) unsigned char band_smem[];
-    const int64_t cap = (int64_t)R * slot_w;
-    uint32_t *s_par = reinterpret_cast<uint32_t *>(band_smem);
-    uint32_t *s_se = s_par + cap;   // start | end << 16
-    uint32_t *s_px = s_se + cap;    // pixel sum at a root
-    uint32_t *s_mn = s_px + cap;    // smallest slot of a piece, at its root
-    uint8_t *s_v = reinterpret_cast<uint8_t *>(s_mn + cap);
-    __shared__ uint32_t s_cnt[BAND_MAX_ROWS];
-    __shared__ uint32_t sh[32];
-    __shared__ uint32_t s_base;
-    const FrameDesc f = frames[blockIdx.y];
-    const int64_t y0 = (int64_t)blockIdx.x * R;
-    if (y0 >= f.qh) return;
-    const int64_t y1 = dmin(y0 + R, (int64_t)f.qh);
-    const int nrows = (int)(y1 - y0);
-    const int qw = f.qw;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    BAND_PROF(0)
-    // 1. the runs of each row (fast/threshold.c:210-266): one warp per row,
-    // the run starts of 32 columns at a time by ballot; runs of 127 dropped
-    for (int r = warp; r < nrows; r += nwarps) {
-        const int64_t y = y0 + r;
-        const uint8_t *t = thr + f.q_off + y * qw;
-        const int64_t sb = (int64_t)r * qw;
-        const int64_t xmax = qw - 2;
-        int64_t count = 0, open = -1;
-        for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
-            int64_t x = x0 + lane;
-            bool valid = x <= xmax;
-            uint8_t v = valid ? t[x] : 0;
-            bool start = valid && (x == 0 || t[x - 1] != v);
-            uint32_t S = __ballot_sync(0xffffffffu, start);
-            uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
-            // the starts first: a run's start and end share one word
-            if (start && v != 127) {
-                int64_t sl = sb + count + __popc(N & lt);
-                s_se[sl] = (uint32_t)x;
-                s_v[sl] = v;
-            }
-            __syncwarp();
-            if (start) {
-                uint32_t below = S & lt;
-                int64_t prev_slot;
-                if (below) {
-                    int pl = 31 - __clz(below);
-                    prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
-                } else {
-                    prev_slot = open;
-                }
-                if (prev_slot >= 0) s_se[sb + prev_slot] |= (uint32_t)(x - 1) << 16;
-            }
-            __syncwarp();
-            if (S) {
-                int ls = 31 - __clz(S);
-                open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
-            }
-            count += __popc(N);
-        }
-        if (lane == 0) {
-            if (open >= 0) s_se[sb + open] |= (uint32_t)xmax << 16;
-            s_cnt[r] = (uint32_t)count;
-            row_nruns[f.row0 + y] = (uint32_t)count;
-        }
-    }
-    __syncthreads();
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
-            int64_t sl = (int64_t)r * qw + i;
-            s_par[sl] = (uint32_t)sl;
-            s_px[sl] = 0;
-        }
-    __syncthreads();
-    BAND_PROF(1)
-    // 2. the links between consecutive rows of the band (unionfind.c:112-146)
-    for (int r = 1; r < nrows; r++) {
-        const int64_t cb = (int64_t)r * qw, pb = cb - qw, np = s_cnt[r - 1];
-        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
-            uint32_t se = s_se[cb + i];
-            int64_t a0 = se & 0xffff, a1 = se >> 16;
-            uint8_t v = s_v[cb + i];
-            FOR_TOUCHING(s_se, s_v, pb, np, a0, a1, v, k, { sm_unite(s_par, (uint32_t)(cb + i), (uint32_t)(pb + k)); })
-        }
-    }
-    __syncthreads();
-    BAND_PROF(2)
-    // 3. flatten the band's forest by pointer jumping (parallel, in place:
-    // a parent only ever moves up its tree), then each root's pixel sum
-    for (;;) {
-        int changed = 0;
-        for (int r = 0; r < nrows; r++)
-            for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
-                int64_t sl = (int64_t)r * qw + i;
-                uint32_t p = s_par[sl], pp = s_par[p];
-                if (pp != p) {
-                    s_par[sl] = pp;
-                    changed = 1;
-                }
-            }
-        if (!__syncthreads_or(changed)) break;
-    }
-    BAND_PROF(3)
-    // each piece's pixel sum, kept at its root
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i0 = 0; i0 < s_cnt[r]; i0 += blockDim.x) {
-            const int64_t i = i0 + threadIdx.x;
-            const bool valid = i < s_cnt[r];
-            const uint32_t live = __ballot_sync(0xffffffffu, valid);
-            if (!valid) continue;
-            int64_t sl = (int64_t)r * qw + i;
-            uint32_t se = s_se[sl];
-            uint32_t add = (se >> 16) - (se & 0xffff) + 1;
-            uint32_t root = s_par[sl];
-            // one shared-memory atomic per distinct root of the warp
-            uint32_t peers = __match_any_sync(live, root);
-            uint32_t sum = 0;
-            for (uint32_t m = peers; m; m &= m - 1) sum += __shfl_sync(peers, add, __ffs(m) - 1);
-            if (lane == __ffs(peers) - 1) atomicAdd(s_px + root, sum);
-        }
-    __syncthreads();
-    BAND_PROF(4)
-    // the smallest slot of each piece: the lowest slot whose root is the
-    // piece's root. The slots are in increasing order along rows and
-    // rows, so the first slot (in slot order) with a root is its minimum:
-    // mark it with an atomicMin on the root's entry of s_mn.
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) s_mn[(int64_t)r * qw + i] = 0xffffffffu;
-    __syncthreads();
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i0 = 0; i0 < s_cnt[r]; i0 += blockDim.x) {
-            const int64_t i = i0 + threadIdx.x;
-            const bool valid = i < s_cnt[r];
-            const uint32_t live = __ballot_sync(0xffffffffu, valid);
-            if (!valid) continue;
-            uint32_t sl = (uint32_t)((int64_t)r * qw + i);
-            uint32_t root = s_par[sl];
-            uint32_t peers = __match_any_sync(live, root);
-            if (lane == __ffs(peers) - 1) atomicMin(s_mn + root, sl);  // lowest lane: smallest slot
-        }
-    __syncthreads();
-    BAND_PROF(5)
-    // each run's global parent: its piece's smallest node (the band root)
-    uint32_t nroot_thread = 0;
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
-            int64_t sl = (int64_t)r * qw + i;
-            uint32_t root = s_par[sl];
-            uint32_t mn = s_mn[root];
-            int64_t node = f.node_off + (y0 + r) * qw + i;
-            int64_t mr = mn / qw;
-            runs.start[node] = (uint16_t)(s_se[sl] & 0xffff);
-            runs.end[node] = (uint16_t)(s_se[sl] >> 16);
-            runs.v[node] = s_v[sl];
-            runs.parent[node] = (uint32_t)(f.node_off + (y0 + mr) * qw + (mn - mr * qw));
-            if (mn == (uint32_t)sl) {
-                runs.px[node] = s_px[root];
-                runs.minid[node] = (uint32_t)node;
-                nroot_thread++;
-            }
-        }
-    // the last-column nodes of the band's rows: one-pixel roots
-    for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
-        int64_t vn = f.node_off + (int64_t)qw * f.qh + y0 + r;
-        runs.parent[vn] = (uint32_t)vn;
-        runs.px[vn] = 1;
-        runs.minid[vn] = (uint32_t)vn;
-        nroot_thread++;
-    }
-    BAND_PROF(6)
-    // append the band's roots to the list: one atomic per block
-    uint32_t total;
-    uint32_t off = block_excl_scan(nroot_thread, &total, sh);
-    if (threadIdx.x == 0) s_base = atomicAdd(nbroots, total);
-    __syncthreads();
-    uint32_t at = s_base + off;
-    for (int r = 0; r < nrows; r++)
-        for (int64_t i = threadIdx.x; i < s_cnt[r]; i += blockDim.x) {
-            int64_t sl = (int64_t)r * qw + i;
-            if (s_mn[s_par[sl]] == (uint32_t)sl) broots[at++] = (uint32_t)(f.node_off + (y0 + r) * qw + i);
-        }
-    for (int r = threadIdx.x; r < nrows; r += blockDim.x)
-        broots[at++] = (uint32_t)(f.node_off + (int64_t)qw * f.qh + y0 + r);
-    BAND_PROF(7)
-}
-
-// One level of the merge across bands, in global memory: the band
-// boundaries b (row b*R against the row above) with b a multiple of
-// base^level but not of base^(level+1); at level 0 also every row's
-// last-column link (unionfind.c:89-97). The groups merged at one level are
-// compressed (their roots point at their root), so finds stay short.
-#define MERGE_ROW_CAP 4096
-__global__ void k_merge_level(const FrameDesc *frames, const uint8_t *thr, RunArrays runs, const uint32_t *row_nruns,
-                              int R, int64_t step, int first_level) {
-    __shared__ uint32_t s_se[MERGE_ROW_CAP];
-    __shared__ uint8_t s_v[MERGE_ROW_CAP];
-    const FrameDesc f = frames[blockIdx.y];
-    const int64_t nb = (f.qh + R - 1) / R;
-    // block k takes the k-th boundary of this level: b = step * (k + k / 7 + 1)
-    // skips the multiples of 8 * step
-    for (int64_t k = blockIdx.x; ; k += gridDim.x) {
-        const int64_t b = step * (k + k / 7 + 1);
-        if (b >= nb) break;
-        const int64_t y = b * R;
-        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
-        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
-        // the row above in shared memory (its runs are searched by every run)
-        const bool staged = nprev <= MERGE_ROW_CAP;
-        __syncthreads();
-        if (staged)
-            for (int64_t t = threadIdx.x; t < nprev; t += blockDim.x) {
-                s_se[t] = (uint32_t)runs.start[prev + t] | (uint32_t)runs.end[prev + t] << 16;
-                s_v[t] = runs.v[prev + t];
-            }
-        __syncthreads();
-        for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
-            int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
-            uint8_t v = runs.v[cur + i];
-            if (staged) {
-                FOR_TOUCHING(s_se, s_v, 0, nprev, a0, a1, v, kk,
-                             { uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk)); })
-            } else {
-                int64_t lo = 0, hi = nprev;
-                while (lo < hi) {
-                    int64_t mid = (lo + hi) >> 1;
-                    if ((int64_t)runs.end[prev + mid] + 1 < a0)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                for (int64_t kk = lo; kk < nprev && (int64_t)runs.start[prev + kk] <= a1 + 1; kk++) {
-                    if (runs.v[prev + kk] != v) continue;
-                    if (runs_touch(a0, a1, runs.start[prev + kk], runs.end[prev + kk], v))
-                        uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + kk));
-                }
-            }
-        }
-    }
-    if (!first_level) return;
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (int64_t y = 1 + tid; y < f.qh; y += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t ncur = row_nruns[f.row0 + y];
-        if (ncur == 0) continue;
-        int64_t last = f.node_off + y * f.qw + ncur - 1;
-        const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
-        if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
-            uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
-    }
-}
 
 // The flat form of the same union-find: one block per row, one thread per
 // run, links in global memory (hash-ordered, so trees stay shallow), then
@@ -715,30 +417,6 @@ __device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
         px = p[x];
     }
     return x;
-}
-
-// Point each listed root at the root of its tree.
-__global__ void k_compress(uint32_t *parent, const uint32_t *broots, const uint32_t *nbroots) {
-    const int64_t n = *nbroots;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t x = broots[i];
-        parent[x] = uf_root(parent, x);
-    }
-}
-
-// Each band root that is not a final root adds its band's pixels to it, and
-// offers its id as the component's smallest (the label).
-__global__ void k_roots_px(const uint32_t *parent, uint32_t *px, uint32_t *minid, const uint32_t *broots,
-                           const uint32_t *nbroots) {
-    const int64_t n = *nbroots;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t x = broots[i];
-        uint32_t r = uf_root(parent, x);
-        if (r != x) {
-            atomicAdd(px + r, px[x]);
-            atomicMin(minid + r, x);
-        }
-    }
 }
 
 // Each node adds its pixels and offers its id to its root (one atomic per
@@ -984,44 +662,59 @@ __device__ __forceinline__ void leaf_network(uint64_t *k, int n) {
 #undef CX
 }
 
-// Sort (key, val) pairs ascending by key, in place, n items (any n): a
-// bitonic network with every comparator ascending; partners past n act as
-// +infinity and are skipped.
-__device__ void block_sort_pairs(uint64_t *key, uint32_t *val, int64_t n64) {
-    const int n = (int)n64;
-    int P = 1, lp = 0;
-    while (P < n) {
-        P <<= 1;
-        lp++;
-    }
-    for (int lk = 1; lk <= lp; lk++) {
-        const int k = 1 << lk;
-        for (int lj = lk - 1; lj >= 0; lj--) {
-            const int j = 1 << lj;
-            for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
-                // comparator t of this step: i < p
-                const int blk = t >> lj, off = t & (j - 1);
-                int i, p;
-                if (lj == lk - 1) {
-                    i = (blk << lk) + off;
-                    p = (blk << lk) + k - 1 - off;
+
+// Sort (key, val) pairs ascending by key (keys distinct): a merge sort of
+// log2(n) levels; at each level every thread writes a contiguous chunk of
+// the output, starting at the merge-path split of its first element (a
+// binary search). kb/vb are scratch of n entries; the result is in ka/va.
+__device__ void block_merge_sort(uint64_t *ka, uint32_t *va, uint64_t *kb, uint32_t *vb, int n) {
+    uint64_t *sk = ka, *dk = kb;
+    uint32_t *sv = va, *dv = vb;
+    const int ipt = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    for (int w = 1; w < n; w <<= 1) {
+        const int o0 = (int)threadIdx.x * ipt, o1 = min(n, o0 + ipt);
+        int o = o0;
+        while (o < o1) {
+            const int lo = (o / (2 * w)) * (2 * w);
+            const int la = min(w, n - lo), lb = max(0, min(w, n - lo - la));
+            const uint64_t *A = sk + lo, *B = sk + lo + la;
+            const int k = o - lo, seg_end = min(o1, lo + la + lb);
+            int l = max(0, k - lb), h = min(k, la);
+            while (l < h) {
+                const int m = (l + h) >> 1;
+                if (A[m] < B[k - m - 1])
+                    l = m + 1;
+                else
+                    h = m;
+            }
+            int i = l, j = k - l;
+            for (; o < seg_end; o++) {
+                const bool take_a = j >= lb || (i < la && A[i] < B[j]);
+                if (take_a) {
+                    dk[o] = A[i];
+                    dv[o] = sv[lo + i];
+                    i++;
                 } else {
-                    i = (blk << (lj + 1)) + off;
-                    p = i + j;
-                }
-                if (p < n) {
-                    const uint64_t ki = key[i], kp = key[p];
-                    if (kp < ki) {
-                        key[i] = kp;
-                        key[p] = ki;
-                        const uint32_t tv = val[i];
-                        val[i] = val[p];
-                        val[p] = tv;
-                    }
+                    dk[o] = B[j];
+                    dv[o] = sv[lo + la + j];
+                    j++;
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
+        uint64_t *tk = sk;
+        sk = dk;
+        dk = tk;
+        uint32_t *tv = sv;
+        sv = dv;
+        dv = tv;
+    }
+    if (sk != ka) {
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            ka[t] = sk[t];
+            va[t] = sv[t];
+        }
+        __syncthreads();
     }
 }
 
@@ -1112,7 +805,7 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
 #define FIT_SMALL 1024
 #define FIT_LARGE_SORT 8192
 #define FIT_CHUNK_SMALL 1024
-#define FIT_CHUNK_LARGE 2048
+#define FIT_CHUNK_LARGE 4096
 
 // dynamic shared memory of one block of the fit kernel
 __host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk) {
@@ -1148,6 +841,8 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
     __shared__ uint32_t s_scan[32];
     __shared__ double s_perr[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pmse[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA],
         s_pnx[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pny[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA];
+    __shared__ double s_be[NT / 32], s_lines[4][4], s_lmse[4], s_best;
+    __shared__ int64_t s_bo[NT / 32];
     const int tid = threadIdx.x;
 
     for (int64_t c = blockIdx.x; c < nclusters; c += gridDim.x) {
@@ -1284,7 +979,13 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         }
         __syncthreads();
         FIT_PROF(4)
-        block_sort_pairs(sk, sv, sz);
+        {
+            // the merge's second buffer: the moment staging area (free now)
+            // in shared memory, or two scratch arrays beside them
+            uint64_t *kb = in_smem ? reinterpret_cast<uint64_t *>(s_w) : reinterpret_cast<uint64_t *>(scr.w + s0);
+            uint32_t *vb = in_smem ? reinterpret_cast<uint32_t *>(kb + sort_cap) : reinterpret_cast<uint32_t *>(scr.fx + s0);
+            block_merge_sort(sk, sv, kb, vb, (int)sz);
+        }
         FIT_PROF(5)
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
@@ -1458,44 +1159,82 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         }
         __syncthreads();
         FIT_PROF(9)
-        if (tid == 0) {
+        // the 4 maxima with the smallest total error (quads.c:931-958): the
+        // reference keeps the first strictly smaller error in (m0, m1, m2, m3)
+        // order, i.e. the smallest error and, among equal ones, the first in
+        // that order. Each thread scans some (m0, m1, m2) triples; then a
+        // block-wide minimum of (error, order).
+        {
             const double inf = __longlong_as_double(0x7ff0000000000000ll);
-            double best = inf;
-            int64_t bi[4] = {0, 0, 0, 0};
-            for (int64_t m0 = 0; m0 < nm - 3; m0++)
-                for (int64_t m1 = m0 + 1; m1 < nm - 2; m1++) {
-                    int64_t p01 = m0 * nm + m1;
-                    if (s_pmse[p01] > prm.max_mse) continue;
-                    for (int64_t m2 = m1 + 1; m2 < nm - 1; m2++) {
-                        int64_t p12 = m1 * nm + m2;
-                        if (s_pmse[p12] > prm.max_mse) continue;
-                        double dot = s_pnx[p01] * s_pnx[p12] + s_pny[p01] * s_pny[p12];
-                        if (fabs(dot) > prm.max_dot) continue;
-                        double e012 = s_perr[p01] + s_perr[p12];
-                        for (int64_t m3 = m2 + 1; m3 < nm; m3++) {
-                            int64_t p23 = m2 * nm + m3, p30 = m3 * nm + m0;
-                            double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
-                            double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
-                            double e = e012 + e23 + e30;
-                            if (e < best) {
-                                best = e;
-                                bi[0] = mxi[m0];
-                                bi[1] = mxi[m1];
-                                bi[2] = mxi[m2];
-                                bi[3] = mxi[m3];
-                            }
-                        }
+            double be = inf;
+            int64_t bo = INT64_MAX;
+            for (int64_t t = tid; t < nm * nm * nm; t += NT) {
+                const int64_t m0 = t / (nm * nm), m1 = (t / nm) % nm, m2 = t % nm;
+                if (!(m0 < m1 && m1 < m2 && m2 < nm - 1)) continue;
+                const int64_t p01 = m0 * nm + m1, p12 = m1 * nm + m2;
+                if (s_pmse[p01] > prm.max_mse || s_pmse[p12] > prm.max_mse) continue;
+                const double dot = s_pnx[p01] * s_pnx[p12] + s_pny[p01] * s_pny[p12];
+                if (fabs(dot) > prm.max_dot) continue;
+                const double e012 = s_perr[p01] + s_perr[p12];
+                for (int64_t m3 = m2 + 1; m3 < nm; m3++) {
+                    const int64_t p23 = m2 * nm + m3, p30 = m3 * nm + m0;
+                    const double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
+                    const double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
+                    const double e = e012 + e23 + e30;
+                    if (e < be) {  // within a thread: ascending order already
+                        be = e;
+                        bo = t * nm + m3;
                     }
                 }
+            }
+            // block minimum of (be, bo)
+            for (int o = 16; o > 0; o >>= 1) {
+                double e2 = __shfl_xor_sync(0xffffffffu, be, o);
+                int64_t o2 = __shfl_xor_sync(0xffffffffu, bo, o);
+                if (e2 < be || (e2 == be && o2 < bo)) {
+                    be = e2;
+                    bo = o2;
+                }
+            }
+            if ((tid & 31) == 0) {
+                s_be[tid >> 5] = be;
+                s_bo[tid >> 5] = bo;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < NT / 32; w++)
+                    if (s_be[w] < be || (s_be[w] == be && s_bo[w] < bo)) {
+                        be = s_be[w];
+                        bo = s_bo[w];
+                    }
+                s_be[0] = be;
+                s_bo[0] = bo;
+            }
+            __syncthreads();
+            be = s_be[0];
+            bo = s_bo[0];
+            // the 4 line fits (quads.c:1069-1075), one per thread
+            if (be != inf && tid < 4) {
+                const int64_t t = bo / nm, m3 = bo % nm;
+                const int64_t mi[4] = {t / (nm * nm), (t / nm) % nm, t % nm, m3};
+                double mse;
+                line_of(seg_moments(mo, sz, mxi[mi[tid]], mxi[mi[(tid + 1) & 3]]), s_lines[tid], &mse);
+                s_lmse[tid] = mse;
+            }
+            __syncthreads();
+            if (tid == 0) s_best = be;
+        }
+        if (tid == 0) {
+            const double inf = __longlong_as_double(0x7ff0000000000000ll);
+            const double best = s_best;
             bool ok = best != inf && best / (double)sz < prm.max_mse;
             GpuQuad q;
             q.reversed_border = rev;
             q.frame = cframe[c];
             double lines[4][4];
             for (int i = 0; ok && i < 4; i++) {
-                double mse;
-                line_of(seg_moments(mo, sz, bi[i], bi[(i + 1) & 3]), lines[i], &mse);
-                if (mse > prm.max_mse) ok = false;
+                for (int k = 0; k < 4; k++) lines[i][k] = s_lines[i][k];
+                if (s_lmse[i] > prm.max_mse) ok = false;
             }
             for (int i = 0; ok && i < 4; i++) {
                 int j = (i + 1) & 3;
@@ -1777,14 +1516,18 @@ __device__ uint32_t qd_lookup(const GpuFamily &F, uint64_t rcode) {
     return 65535u | 255u << 16;
 }
 
+#define REF_CHUNK 128
+
 __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *frames, GpuParams prm,
                                                               const GpuFamily *fams, const uint8_t *img,
                                                               const uint8_t *qim, const GpuQuad *quads,
                                                               int64_t nquads, GpuDetection *dets, uint32_t *det_ok) {
     __shared__ float s_p[4][2];
     __shared__ double s_lines[4][4];
-    __shared__ double s_bx[AT_DEC_THREADS], s_by[AT_DEC_THREADS];
-    __shared__ int s_bok[AT_DEC_THREADS];
+    __shared__ double s_bx[4][REF_CHUNK], s_by[4][REF_CHUNK];
+    __shared__ int s_bok[4][REF_CHUNK];
+    __shared__ double s_enx[4], s_eny[4];
+    __shared__ int64_t s_ens[4];
     __shared__ double s_H[9];
     __shared__ int s_hok;
     __shared__ double s_gx[8 * AT_MAX_TW], s_gy[8 * AT_MAX_TW], s_gv[8 * AT_MAX_TW];
@@ -1809,12 +1552,14 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
         for (int fi = tid; fi < prm.nfam; fi += blockDim.x) det_ok[qi * prm.nfam + fi] = 0;
         __syncthreads();
         if (prm.refine_edges) {
-            // fast/decode.c:657-761
+            // fast/decode.c:657-761. The 4 edges are independent until the
+            // corners are moved: their sample points are refined together,
+            // and thread e < 4 sums edge e's samples in order.
             const int64_t range = (int64_t)__fadd_rn(prm.quad_decimate, 1.0f);
             const int64_t nsteps = 2 * 4 * range + 1;
             const int64_t vsteps = nsteps - nsteps % 4;
-            for (int edge = 0; edge < 4; edge++) {
-                int a = edge, b = (edge + 1) & 3;
+            if (tid < 4) {
+                int a = tid, b = (tid + 1) & 3;
                 double nx = (double)__fsub_rn(s_p[b][1], s_p[a][1]);
                 double ny = (double)__fadd_rn(-s_p[b][0], s_p[a][0]);
                 double mag = sqrt(nx * nx + ny * ny);
@@ -1824,48 +1569,57 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                     nx = -nx;
                     ny = -ny;
                 }
-                int64_t nsamples = dmax(16, c_int(mag / 8.0));
-                double mx = 0.0, my = 0.0, mxx = 0.0, mxy = 0.0, myy = 0.0, cnt = 0.0;
-                for (int64_t s0 = 0; s0 < nsamples; s0 += blockDim.x) {
-                    int64_t si = s0 + tid;
-                    if (si < nsamples) {
-                        double alpha = (1.0 + (double)si) / (double)(nsamples + 1);
-                        double x0 = alpha * (double)s_p[a][0] + (1.0 - alpha) * (double)s_p[b][0];
-                        double y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
-                        double n0;
-                        bool ok = refine_sample(v, x0, y0, nx, ny, range, vsteps, nsteps, &n0);
-                        s_bok[tid] = ok;
-                        if (ok) {
-                            s_bx[tid] = x0 + n0 * nx;
-                            s_by[tid] = y0 + n0 * ny;
-                        }
-                    }
-                    __syncthreads();
-                    if (tid == 0) {
-                        int64_t m = dmin((int64_t)blockDim.x, nsamples - s0);
-                        for (int64_t t = 0; t < m; t++) {
-                            if (!s_bok[t]) continue;
-                            double bx = s_bx[t], by = s_by[t];
-                            mx = mx + bx;
-                            my = my + by;
-                            mxx = mxx + bx * bx;
-                            mxy = mxy + bx * by;
-                            myy = myy + by * by;
-                            cnt = cnt + 1.0;
-                        }
-                    }
-                    __syncthreads();
-                }
-                if (tid == 0) {
-                    double ex = mx / cnt, ey = my / cnt;
-                    double cxx = mxx / cnt - ex * ex, cxy = mxy / cnt - ex * ey, cyy = myy / cnt - ey * ey;
-                    double theta = 0.5 * (double)cr_atan2f((float)(-2.0 * cxy), (float)(cyy - cxx));
-                    s_lines[edge][0] = ex;
-                    s_lines[edge][1] = ey;
-                    s_lines[edge][2] = (double)cr_cosf((float)theta);
-                    s_lines[edge][3] = (double)cr_sinf((float)theta);
-                }
+                s_enx[tid] = nx;
+                s_eny[tid] = ny;
+                s_ens[tid] = dmax(16, c_int(mag / 8.0));
             }
+            __syncthreads();
+            const int64_t maxns = dmax(dmax(s_ens[0], s_ens[1]), dmax(s_ens[2], s_ens[3]));
+            double mx = 0.0, my = 0.0, mxx = 0.0, mxy = 0.0, myy = 0.0, cnt = 0.0;
+            for (int64_t s0 = 0; s0 < maxns; s0 += REF_CHUNK) {
+                for (int w = tid; w < 4 * REF_CHUNK; w += blockDim.x) {
+                    const int e = w / REF_CHUNK, t = w - e * REF_CHUNK;
+                    const int64_t si = s0 + t, ns = s_ens[e];
+                    if (si >= ns) continue;
+                    const int a = e, b = (e + 1) & 3;
+                    const double nx = s_enx[e], ny = s_eny[e];
+                    double alpha = (1.0 + (double)si) / (double)(ns + 1);
+                    double x0 = alpha * (double)s_p[a][0] + (1.0 - alpha) * (double)s_p[b][0];
+                    double y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
+                    double n0;
+                    bool ok = refine_sample(v, x0, y0, nx, ny, range, vsteps, nsteps, &n0);
+                    s_bok[e][t] = ok;
+                    if (ok) {
+                        s_bx[e][t] = x0 + n0 * nx;
+                        s_by[e][t] = y0 + n0 * ny;
+                    }
+                }
+                __syncthreads();
+                if (tid < 4) {
+                    const int64_t m = dmin((int64_t)REF_CHUNK, s_ens[tid] - s0);
+                    for (int64_t t = 0; t < m; t++) {
+                        if (!s_bok[tid][t]) continue;
+                        double bx = s_bx[tid][t], by = s_by[tid][t];
+                        mx = mx + bx;
+                        my = my + by;
+                        mxx = mxx + bx * bx;
+                        mxy = mxy + bx * by;
+                        myy = myy + by * by;
+                        cnt = cnt + 1.0;
+                    }
+                }
+                __syncthreads();
+            }
+            if (tid < 4) {
+                double ex = mx / cnt, ey = my / cnt;
+                double cxx = mxx / cnt - ex * ex, cxy = mxy / cnt - ex * ey, cyy = myy / cnt - ey * ey;
+                double theta = 0.5 * (double)cr_atan2f((float)(-2.0 * cxy), (float)(cyy - cxx));
+                s_lines[tid][0] = ex;
+                s_lines[tid][1] = ey;
+                s_lines[tid][2] = (double)cr_cosf((float)theta);
+                s_lines[tid][3] = (double)cr_sinf((float)theta);
+            }
+            __syncthreads();
             if (tid == 0) {
                 for (int i = 0; i < 4; i++) {
                     int j = (i + 1) & 3;
@@ -2243,11 +1997,7 @@ void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uin
 }
 
 int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
-                   uint32_t *lab, int32_t min_px, int64_t max_qw, int64_t max_qh, uint32_t *broots,
-                   uint32_t *nbroots) {
-    (void)max_qw;
-    (void)broots;
-    (void)nbroots;
+                   uint32_t *lab, int32_t min_px, int64_t max_qh) {
     dim3 rg((unsigned)(max_qh < 148 * 16 ? max_qh : 148 * 16), (unsigned)L.nframes);
     k_row_runs<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
     k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);

@@ -43,8 +43,7 @@ void launch_threshold(const Launch &L, const FrameDesc *frames, const uint8_t *q
                       uint8_t *thr, int32_t diff);
 void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uint8_t *tmp);
 int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
-                    uint32_t *lab, int32_t min_px, int64_t max_qw, int64_t max_qh, uint32_t *broots,
-                    uint32_t *nbroots);
+                   uint32_t *lab, int32_t min_px, int64_t max_qh);
 void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                         uint64_t *row_npts);
 void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
