@@ -102,6 +102,11 @@ class FrameResult(C.Structure):
 
 DIAG = {"quad_image": 0, "threshold": 1, "labels": 2, "points": 3, "clusters": 4, "quads": 5, "sizes": 6}
 QUAD_DTYPE = np.dtype([("p", np.float32, (4, 2)), ("reversed_border", np.int32), ("frame", np.int32)])
+# at_detection as a numpy record (168 bytes)
+DETECTION_DTYPE = np.dtype([("family", np.int32), ("id", np.int32), ("hamming", np.int32),
+                            ("decision_margin", np.float32), ("H", np.float64, (9,)), ("c", np.float64, (2,)),
+                            ("p", np.float64, (4, 2))])
+assert DETECTION_DTYPE.itemsize == 168
 
 FAMILY_NAMES = ("tag16h5", "tag25h9", "tag36h10", "tag36h11", "tagCircle21h7", "tagCircle49h12",
                 "tagCustom48h12", "tagStandard41h12", "tagStandard52h13")
@@ -215,7 +220,10 @@ class Detector:
         td = self._td.contents
         return [_detection(td.detections[i]) for i in range(td.ndetections)]
 
-    def detect_batch(self, images, family_masks=None) -> list[list[Detection]]:
+    def detect_batch(self, images, family_masks=None, as_arrays: bool = False):
+        """at_detect_batch over images of any sizes. Returns per frame a list
+        of Detection, or with as_arrays a numpy record array (DETECTION_DTYPE,
+        a copy of the library's at_detection array) per frame."""
         n = len(images)
         frames = (Frame * max(n, 1))()
         keep = []
@@ -227,11 +235,16 @@ class Detector:
         self._L.at_detect_batch(self._td, frames, n, res)
         self._check()
         td = self._td.contents
-        out = []
-        for i in range(n):
-            out.append([_detection(td.detections[res[i].first + k]) for k in range(res[i].count)])
         self.last_batch_nquads = [int(res[i].nquads) for i in range(n)]
-        return out
+        if as_arrays:
+            total = int(td.ndetections)
+            if total:
+                buf = C.cast(td.detections, C.POINTER(C.c_uint8 * (168 * total))).contents
+                allv = np.frombuffer(buf, DETECTION_DTYPE, total).copy()
+            else:
+                allv = np.zeros(0, DETECTION_DTYPE)
+            return [allv[res[i].first:res[i].first + res[i].count] for i in range(n)]
+        return [[_detection(td.detections[res[i].first + k]) for k in range(res[i].count)] for i in range(n)]
 
     def _check(self):
         msg = C.c_char_p()

@@ -99,9 +99,9 @@ struct at_internal {
     bool fam_dirty = true;
 
     int device = 0;
-    cudaStream_t stream = nullptr, side = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr, side2 = nullptr;
     cudaEvent_t ev[12];
-    cudaEvent_t fork = nullptr, join = nullptr;  // ordering only, no timing
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;  // ordering only, no timing
     DBuf buf[B_NBUF];
     HBuf h_frames, h_small, h_out;
     std::vector<at_detection> dets;
@@ -468,7 +468,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                        B[B_SERRS].as<double>(),   B[B_SFILT].as<double>(),  B[B_SMXE].as<double>(),
                        B[B_SMXI].as<int32_t>()};
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
-        launch_fit_quads(st, in->side, in->fork, in->join, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
+        launch_fit_quads(st, in->side, in->side2, in->fork, in->join, in->join2, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
         in->launches += 2;
         CK(cudaGetLastError());
@@ -619,8 +619,10 @@ at_detector *at_detector_create(void) {
     }
     for (int k = 0; k < 12; k++) cudaEventCreate(&in->ev[k]);
     cudaStreamCreateWithFlags(&in->side, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&in->side2, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&in->fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&in->join, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&in->join2, cudaEventDisableTiming);
     return td;
 }
 
@@ -648,7 +650,9 @@ void at_detector_destroy(at_detector *td) {
     for (int k = 0; k < 12; k++) cudaEventDestroy(in->ev[k]);
     cudaEventDestroy(in->fork);
     cudaEventDestroy(in->join);
+    cudaEventDestroy(in->join2);
     cudaStreamDestroy(in->side);
+    cudaStreamDestroy(in->side2);
     cudaStreamDestroy(in->stream);
     delete in;
     free(td);

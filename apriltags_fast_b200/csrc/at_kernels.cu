@@ -1294,6 +1294,424 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
 }
 
 // ---------------------------------------------------------------------------
+// Clusters of at most FIT_WARP points: one warp each, FIT_WPB per block, no
+// block barriers. The same steps as k_fit_quads, with warp primitives.
+#define FIT_WARP 256
+#define FIT_WPB 4
+
+// per warp: sort keys and values (region A), the sort's second buffer reused
+// for the moment staging (region B), and the pair fits (4 * mm * mm)
+__host__ __device__ constexpr size_t fit_warp_smem(int mm) {
+    return (size_t)FIT_WARP * 36 + (size_t)4 * mm * mm * 8;
+}
+
+// merge sort of one warp (see block_merge_sort)
+__device__ void warp_merge_sort(uint64_t *ka, uint32_t *va, uint64_t *kb, uint32_t *vb, int n, int lane) {
+    uint64_t *sk = ka, *dk = kb;
+    uint32_t *sv = va, *dv = vb;
+    const int ipt = (n + 31) / 32;
+    for (int w = 1; w < n; w <<= 1) {
+        const int o1 = min(n, lane * ipt + ipt);
+        int o = lane * ipt;
+        while (o < o1) {
+            const int lo = (o / (2 * w)) * (2 * w);
+            const int la = min(w, n - lo), lb = max(0, min(w, n - lo - la));
+            const uint64_t *A = sk + lo, *B = sk + lo + la;
+            const int k = o - lo, seg_end = min(o1, lo + la + lb);
+            int l = max(0, k - lb), h = min(k, la);
+            while (l < h) {
+                const int m = (l + h) >> 1;
+                if (A[m] < B[k - m - 1])
+                    l = m + 1;
+                else
+                    h = m;
+            }
+            int i = l, j = k - l;
+            for (; o < seg_end; o++) {
+                const bool take_a = j >= lb || (i < la && A[i] < B[j]);
+                if (take_a) {
+                    dk[o] = A[i];
+                    dv[o] = sv[lo + i];
+                    i++;
+                } else {
+                    dk[o] = B[j];
+                    dv[o] = sv[lo + la + j];
+                    j++;
+                }
+            }
+        }
+        __syncwarp();
+        uint64_t *tk = sk;
+        sk = dk;
+        dk = tk;
+        uint32_t *tv = sv;
+        sv = dv;
+        dv = tv;
+    }
+    if (sk != ka) {
+        for (int t = lane; t < n; t += 32) {
+            ka[t] = sk[t];
+            va[t] = sv[t];
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
+                                                          const uint64_t *pts, const uint32_t *cstart,
+                                                          const int32_t *cframe, int64_t nclusters, int64_t npoints,
+                                                          FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, int mm) {
+    extern __shared__ __align__(16) unsigned char fw_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    unsigned char *base = fw_smem + fit_warp_smem(mm) * wid;
+    uint64_t *ka = reinterpret_cast<uint64_t *>(base);
+    uint32_t *va = reinterpret_cast<uint32_t *>(ka + FIT_WARP);
+    unsigned char *rb = base + FIT_WARP * 12;
+    uint64_t *kb = reinterpret_cast<uint64_t *>(rb);
+    uint32_t *vb = reinterpret_cast<uint32_t *>(kb + FIT_WARP);
+    double *s_w = reinterpret_cast<double *>(rb), *s_fx = s_w + FIT_WARP, *s_fy = s_fx + FIT_WARP;
+    float *s_term = reinterpret_cast<float *>(rb);
+    double *s_perr = reinterpret_cast<double *>(base + FIT_WARP * 36);
+    double *s_pmse = s_perr + mm * mm, *s_pnx = s_pmse + mm * mm, *s_pny = s_pnx + mm * mm;
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+
+    for (int64_t c = (int64_t)blockIdx.x * FIT_WPB + wid; c < nclusters; c += (int64_t)gridDim.x * FIT_WPB) {
+        const int64_t s0 = cstart[c];
+        const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
+        if (sz > FIT_WARP) continue;  // the block kernels' clusters
+        const FrameDesc f = frames[cframe[c]];
+        if (lane == 0) quad_ok[c] = 0;
+        if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
+        const int n = (int)sz;
+        const uint64_t *P = pts + s0;
+        // bounding box (fast/quads.c:515-528)
+        uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
+        for (int i = lane; i < n; i += 32) {
+            uint32_t x = (uint32_t)(P[i] & 0xffff), y = (uint32_t)(P[i] >> 16 & 0xffff);
+            xmin = min(xmin, x);
+            xmax = max(xmax, x);
+            ymin = min(ymin, y);
+            ymax = max(ymax, y);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(FULL, xmin, o));
+            xmax = max(xmax, __shfl_xor_sync(FULL, xmax, o));
+            ymin = min(ymin, __shfl_xor_sync(FULL, ymin, o));
+            ymax = max(ymax, __shfl_xor_sync(FULL, ymax, o));
+        }
+        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < prm.tag_width) continue;
+        const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
+        const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
+
+        // the dot product of offsets and gradients: lane l < 8 sums terms
+        // l, l+8, ... of the whole groups of 8; then the rest in order
+        const int nv = n - n % 8;
+        for (int i = lane; i < nv; i += 32) {
+            uint64_t pt = P[i];
+            float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
+            float gx = (float)(int16_t)(pt >> 32 & 0xffff), gy = (float)(int16_t)(pt >> 48);
+            s_term[i] = __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy));
+        }
+        __syncwarp();
+        float acc = 0.0f;
+        if (lane < 8)
+            for (int i = lane; i < nv; i += 8) acc = __fadd_rn(acc, s_term[i]);
+        float l[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) l[k] = __shfl_sync(FULL, acc, k);
+        int okrev = 0;
+        if (lane == 0) {
+            float dot = __fadd_rn(__fadd_rn(__fadd_rn(l[0], l[4]), __fadd_rn(l[2], l[6])),
+                                  __fadd_rn(__fadd_rn(l[1], l[5]), __fadd_rn(l[3], l[7])));
+            for (int i = nv; i < n; i++) {
+                float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
+                float gx = (float)(int16_t)(P[i] >> 32 & 0xffff), gy = (float)(int16_t)(P[i] >> 48);
+                dot = __fadd_rn(dot, __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy)));
+            }
+            int rev = dot < 0.0f;
+            int ok = 1;
+            if (!prm.reversed_border && rev) ok = 0;
+            if (!prm.normal_border && !rev) ok = 0;
+            okrev = ok | rev << 1;
+        }
+        okrev = __shfl_sync(FULL, okrev, 0);
+        if (!(okrev & 1)) continue;
+        const int rev = okrev >> 1;
+        __syncwarp();
+
+        // the angle sort: per leaf, its network order, block heads and
+        // places; then a sort by (head, place) (see k_fit_quads)
+        for (int p = lane; p < n; p += 32) {
+            uint32_t lf = leaf_of(n, p);
+            int lo = (int)(lf >> 8), len = (int)(lf & 255);
+            if (p != lo) continue;
+            uint64_t k5[5];
+            for (int t = 0; t < len; t++) {
+                uint64_t pt = P[lo + t];
+                float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
+                k5[t] = angle_key(dx, dy, (uint32_t)(lo + t));
+            }
+            leaf_network(k5, len);
+            uint64_t head = 0;
+            for (int t = 0; t < len; t++) {
+                if (t == 0 || k5[t] > head) head = k5[t];
+                uint32_t hidx = ~(uint32_t)head;
+                ka[lo + t] = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 3 | (uint64_t)t;
+                va[lo + t] = ~(uint32_t)k5[t];
+            }
+        }
+        __syncwarp();
+        warp_merge_sort(ka, va, kb, vb, n, lane);
+
+        // cumulative weighted moments in angle order (fast/quads.c:968-1035)
+        const uint8_t *im = qim + f.q_off;
+        for (int k = lane; k < n; k += 32) {
+            uint32_t src = va[k];
+            int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
+            int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
+            int32_t g2 = 0;
+            if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
+                int64_t cc = (int64_t)iy * f.qw + ix;
+                int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
+                int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
+                g2 = gx * gx + gy * gy;
+            }
+            s_w[k] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
+            s_fx[k] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
+            s_fy[k] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+        }
+        __syncwarp();
+        double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
+        if (lane < 6) {
+            const int ca = lane == 1 || lane == 4 ? 1 : lane == 5 ? 2 : 0;  // 0 fx, 1 fy, 2 one
+            const int cb = lane == 2 ? 0 : lane == 3 || lane == 4 ? 1 : 2;
+            const double *A = ca == 0 ? s_fx : s_fy, *Bv = cb == 0 ? s_fx : s_fy;
+            double *o = M[lane];
+            double run = 0.0;
+            int t = 0;
+            for (; t + 8 <= n; t += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    double a = ca == 2 ? 1.0 : A[t + u];
+                    double b = cb == 2 ? 1.0 : Bv[t + u];
+                    v[u] = __dmul_rn(__dmul_rn(s_w[t + u], a), b);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    run = __dadd_rn(run, v[u]);
+                    o[t + u] = run;
+                }
+            }
+            for (; t < n; t++) {
+                double a = ca == 2 ? 1.0 : A[t];
+                double b = cb == 2 ? 1.0 : Bv[t];
+                run = __dadd_rn(run, __dmul_rn(__dmul_rn(s_w[t], a), b));
+                o[t] = run;
+            }
+        }
+        __syncwarp();
+        const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
+
+        // corner search (fast/quads.c:788-959)
+        const int64_t ksz = dmin(20, sz / 12);
+        if (ksz < 2) continue;
+        const double nn = (double)(2 * ksz + 1);
+        double *errs = scr.errs + s0, *filt = scr.filt + s0;
+        for (int i = lane; i < n; i += 32) {
+            int64_t i0 = i - ksz, i1 = i + ksz;
+            MSum s;
+            if (i0 < 0)
+                s = seg_moments(mo, sz, i0 + sz, i1);
+            else if (i1 < sz)
+                s = seg_moments(mo, sz, i0, i1);
+            else
+                s = seg_moments(mo, sz, i0, i1 - sz);
+            errs[i] = window_error(s, nn);
+        }
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            double a;
+            if (i >= 3 && i < n - 3) {
+                a = errs[i - 3] * prm.qsm[0];
+                for (int t = 1; t < 7; t++) a = a + errs[i - 3 + t] * prm.qsm[t];
+            } else {
+                a = 0.0;
+                for (int t = 0; t < 7; t++) {
+                    int j = i - 3 + t;
+                    if (j < 0) j += n;
+                    if (j >= n) j -= n;
+                    a = a + errs[j] * prm.qsm[t];
+                }
+            }
+            filt[i] = a;
+        }
+        __syncwarp();
+        int32_t *mxi = scr.mxi + s0;
+        double *mxe = scr.mxe + s0;
+        int nm = 0;
+        for (int i0 = 0; i0 < n; i0 += 32) {
+            const int i = i0 + lane;
+            bool is_max = false;
+            double e = 0.0;
+            if (i < n) {
+                e = filt[i];
+                double lft = filt[i == 0 ? n - 1 : i - 1], rgt = filt[i + 1 == n ? 0 : i + 1];
+                is_max = e > lft && e > rgt;
+            }
+            const uint32_t bal = __ballot_sync(FULL, is_max);
+            if (is_max) {
+                const int at = nm + __popc(bal & ((1u << lane) - 1u));
+                mxi[at] = i;
+                mxe[at] = e;
+            }
+            nm += __popc(bal);
+        }
+        __syncwarp();
+        if (nm < 4) continue;
+        if (nm > prm.max_nmaxima) {
+            // keep e_i when at most max_nmaxima errors are >= e_i (quads.c:827-862)
+            const int k = prm.max_nmaxima;
+            int kept = 0;
+            for (int i0 = 0; i0 < nm; i0 += 32) {
+                const int i = i0 + lane;
+                bool keep = false;
+                int32_t mi = 0;
+                if (i < nm) {
+                    const double ei = mxe[i];
+                    int ge = 0;
+                    for (int j = 0; j < nm && ge <= k; j++) ge += mxe[j] >= ei;
+                    keep = ge <= k;
+                    mi = mxi[i];
+                }
+                const uint32_t bal = __ballot_sync(FULL, keep);
+                __syncwarp();
+                if (keep) mxi[kept + __popc(bal & ((1u << lane) - 1u))] = mi;
+                kept += __popc(bal);
+            }
+            __syncwarp();
+            nm = kept;
+        }
+        // line fits of pairs of maxima
+        for (int t = lane; t < nm * nm; t += 32) {
+            const int p = t / nm, q = t - p * nm;
+            if (!(p < q || p >= q + 3)) continue;
+            const int64_t i0 = mxi[p], i1 = mxi[q];
+            MSum s = seg_moments(mo, sz, i0, i1);
+            double cnt = (double)(i0 <= i1 ? i1 - i0 + 1 : sz - i0 + i1 + 1);
+            double lp[4], mse;
+            line_of(s, lp, &mse);
+            s_perr[t] = cnt * mse;
+            s_pmse[t] = mse;
+            s_pnx[t] = lp[2];
+            s_pny[t] = lp[3];
+        }
+        __syncwarp();
+        // the first smallest total error in (m0, m1, m2, m3) order
+        double be = inf;
+        int64_t bo = INT64_MAX;
+        for (int t = lane; t < nm * nm * nm; t += 32) {
+            const int m0 = t / (nm * nm), m1 = (t / nm) % nm, m2 = t % nm;
+            if (!(m0 < m1 && m1 < m2 && m2 < nm - 1)) continue;
+            const int p01 = m0 * nm + m1, p12 = m1 * nm + m2;
+            if (s_pmse[p01] > prm.max_mse || s_pmse[p12] > prm.max_mse) continue;
+            const double dot = s_pnx[p01] * s_pnx[p12] + s_pny[p01] * s_pny[p12];
+            if (fabs(dot) > prm.max_dot) continue;
+            const double e012 = s_perr[p01] + s_perr[p12];
+            for (int m3 = m2 + 1; m3 < nm; m3++) {
+                const int p23 = m2 * nm + m3, p30 = m3 * nm + m0;
+                const double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
+                const double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
+                const double e = e012 + e23 + e30;
+                if (e < be) {
+                    be = e;
+                    bo = (int64_t)t * nm + m3;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double e2 = __shfl_xor_sync(FULL, be, o);
+            int64_t o2 = __shfl_xor_sync(FULL, bo, o);
+            if (e2 < be || (e2 == be && o2 < bo)) {
+                be = e2;
+                bo = o2;
+            }
+        }
+        if (!(be != inf && be / (double)sz < prm.max_mse)) continue;
+        // the 4 line fits, lanes 0-3 (quads.c:1069-1075)
+        double ln[4] = {0.0, 0.0, 0.0, 0.0}, lmse = 0.0;
+        if (lane < 4) {
+            const int64_t t = bo / nm, m3 = bo % nm;
+            const int64_t mi[4] = {t / (nm * nm), (t / nm) % nm, t % nm, m3};
+            line_of(seg_moments(mo, sz, mxi[mi[lane]], mxi[mi[(lane + 1) & 3]]), ln, &lmse);
+        }
+        double lines[4][4], lm[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            lm[i] = __shfl_sync(FULL, lmse, i);
+#pragma unroll
+            for (int k = 0; k < 4; k++) lines[i][k] = __shfl_sync(FULL, ln[k], i);
+        }
+        if (lane == 0) {
+            bool ok = true;
+            for (int i = 0; i < 4; i++)
+                if (lm[i] > prm.max_mse) ok = false;
+            GpuQuad q;
+            q.reversed_border = rev;
+            q.frame = cframe[c];
+            for (int i = 0; ok && i < 4; i++) {
+                int j = (i + 1) & 3;
+                double a00 = lines[i][3], a01 = -lines[j][3], a10 = -lines[i][2], a11 = lines[j][2];
+                double b0 = -lines[i][0] + lines[j][0], b1 = -lines[i][1] + lines[j][1];
+                double det = a00 * a11 - a10 * a01;
+                if (fabs(det) < 0.001) {
+                    ok = false;
+                    break;
+                }
+                double w00 = a11 / det, w01 = -a01 / det;
+                double l0 = w00 * b0 + w01 * b1;
+                q.p[i][0] = (float)(lines[i][0] + l0 * a00);
+                q.p[i][1] = (float)(lines[i][1] + l0 * a10);
+            }
+            if (ok) {
+                const int tri[2][4] = {{0, 1, 2, 0}, {2, 3, 0, 2}};
+                double area = 0.0;
+                for (int t = 0; t < 2; t++) {
+                    double len[3];
+                    for (int i = 0; i < 3; i++) {
+                        int ia = tri[t][i], ib = tri[t][i + 1];
+                        double ddx = (double)__fsub_rn(q.p[ib][0], q.p[ia][0]);
+                        double ddy = (double)__fsub_rn(q.p[ib][1], q.p[ia][1]);
+                        len[i] = sqrt(ddx * ddx + ddy * ddy);
+                    }
+                    double pp = (len[0] + len[1] + len[2]) / 2.0;
+                    area = area + sqrt(pp * (pp - len[0]) * (pp - len[1]) * (pp - len[2]));
+                }
+                if (area < 0.95 * (double)prm.tag_width * (double)prm.tag_width) ok = false;
+            }
+            for (int i = 0; ok && i < 4; i++) {
+                int i0 = i, i1 = (i + 1) & 3, i2 = (i + 2) & 3;
+                double dx1 = (double)__fsub_rn(q.p[i1][0], q.p[i0][0]), dy1 = (double)__fsub_rn(q.p[i1][1], q.p[i0][1]);
+                double dx2 = (double)__fsub_rn(q.p[i2][0], q.p[i1][0]), dy2 = (double)__fsub_rn(q.p[i2][1], q.p[i1][1]);
+                double den = sqrt((dx1 * dx1 + dy1 * dy1) * (dx2 * dx2 + dy2 * dy2));
+                if (den == 0.0) {
+                    ok = false;
+                    break;
+                }
+                double cs = (dx1 * dx2 + dy1 * dy2) / den;
+                if ((cs > prm.max_dot || cs < -prm.max_dot) || dx1 * dy2 < dy1 * dx2) ok = false;
+            }
+            if (ok) {
+                quads[c] = q;
+                quad_ok[c] = 1;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // 9. Decoding, one block per quad (fast/decode.c, fast/detector.c:83-139).
 
 struct DView {
@@ -2025,25 +2443,37 @@ void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *
     k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe);
 }
 
-void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const FrameDesc *frames,
-                      const GpuParams &prm, const uint8_t *qim, const uint64_t *pts, const uint32_t *cstart,
-                      const int32_t *cframe, int64_t nclusters, int64_t npoints, const FitScratch &scr, GpuQuad *quads,
-                      uint32_t *quad_ok, uint32_t *err) {
+void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
+                      cudaEvent_t join2, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+                      const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
+                      int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
     if (nclusters <= 0) return;
     const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL), large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
     cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
-    // the few large clusters on a side stream, beside the many small ones
+    // three size classes on three streams: the few large clusters (a block
+    // of 512 each), the middle ones (128), the many small ones (a warp each)
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
+    cudaStreamWaitEvent(side2, fork, 0);
     k_fit_quads<512><<<(unsigned)(nclusters < 148 * 2 ? nclusters : 148 * 2), 512, large, side>>>(
         frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, quads, quad_ok, err, FIT_SMALL + 1,
         INT64_MAX, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaEventRecord(join, side);
-    unsigned blocks = (unsigned)(nclusters < 148 * 64 ? nclusters : 148 * 64);
-    k_fit_quads<128><<<blocks, 128, small, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
-                                                quads, quad_ok, err, 0, FIT_SMALL, FIT_SMALL, FIT_CHUNK_SMALL);
+    unsigned mid = (unsigned)(nclusters < 148 * 16 ? nclusters : 148 * 16);
+    k_fit_quads<128><<<mid, 128, small, side2>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+                                                 quads, quad_ok, err, FIT_WARP + 1, FIT_SMALL, FIT_SMALL,
+                                                 FIT_CHUNK_SMALL);
+    cudaEventRecord(join2, side2);
+    const int mm = prm.max_nmaxima > 4 ? prm.max_nmaxima : 4;
+    const size_t wsm = fit_warp_smem(mm) * FIT_WPB;
+    cudaFuncSetAttribute(k_fit_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
+    unsigned wblocks = (unsigned)(wb < 148 * 32 ? wb : 148 * 32);
+    k_fit_warp<<<wblocks, FIT_WPB * 32, wsm, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+                                                  quads, quad_ok, mm);
     cudaStreamWaitEvent(s, join, 0);
+    cudaStreamWaitEvent(s, join2, 0);
 }
 
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,

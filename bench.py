@@ -218,7 +218,7 @@ def main():
 
     # --- batched, frames resident in HBM ---
     for s in range(args.warmup):
-        det.detect_batch(batch_at(s, dev))
+        det.detect_batch(batch_at(s, dev), as_arrays=True)
     stage = {k: 0.0 for k in det.timing}
     launches0 = int(det.diag("sizes")[5]) if len(det.diag("sizes")) > 5 else 0
     ndet = 0
@@ -227,7 +227,7 @@ def main():
     with Clocks(local) as clk:
         ev0.record()
         for s in range(args.steps):
-            out = det.detect_batch(batch_at(args.warmup + s, dev))
+            out = det.detect_batch(batch_at(args.warmup + s, dev), as_arrays=True)
             ndet += sum(len(o) for o in out)
             for k, v in det.timing.items():
                 stage[k] += v
@@ -244,13 +244,13 @@ def main():
 
     # --- e2e: the same call on pinned host frames ---
     for s in range(args.warmup):
-        det.detect_batch(batch_at(s, pinned))
+        det.detect_batch(batch_at(s, pinned), as_arrays=True)
     barrier()
     ndet_e2e = 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for s in range(args.steps):
-        out = det.detect_batch(batch_at(args.warmup + s, pinned))
+        out = det.detect_batch(batch_at(args.warmup + s, pinned), as_arrays=True)
         ndet_e2e += sum(len(o) for o in out)
     e1.record()
     barrier()
