@@ -59,48 +59,54 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total,
 #define FRAME_LOOP_END }
 
 // ---------------------------------------------------------------------------
-// 1. Decimation (fast/image.c:6-88). One thread per quad-image pixel.
+// 1. Decimation (fast/image.c:6-88). A block per output row, a thread per
+// output pixel.
 
 __global__ void k_decimate(const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor) {
     const FrameDesc f = frames[blockIdx.y];
-    const int64_t n = (int64_t)f.qw * f.qh;
     const uint8_t *src = img + f.img_off;
-    uint8_t *out = qim + f.q_off;
     const int64_t stride = f.w;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t y = i / f.qw, x = i - y * f.qw;
-        uint8_t o;
+    const int qw = (int)f.qw, qh = (int)f.qh;
+    for (int y = blockIdx.x; y < qh; y += gridDim.x) {
+        uint8_t *out = qim + f.q_off + (int64_t)y * qw;
         if (factor == 1.5f) {
             // 3x3 weights over 9; output pixel (2k+dx, 2m+dy) from input
             // block (3k.., 3m..) (fast/image.c:50-62)
-            int64_t k = x >> 1, m = y >> 1;
-            const uint8_t *r0 = src + (3 * m) * stride + 3 * k, *r1 = r0 + stride, *r2 = r1 + stride;
-            int e = r1[1];
-            int v;
-            if ((y & 1) == 0)
-                v = (x & 1) == 0 ? 4 * r0[0] + 2 * r0[1] + 2 * r1[0] + e : 4 * r0[2] + 2 * r0[1] + 2 * r1[2] + e;
-            else
-                v = (x & 1) == 0 ? 4 * r2[0] + 2 * r1[0] + 2 * r2[1] + e : 4 * r2[2] + 2 * r1[2] + 2 * r2[1] + e;
-            o = (uint8_t)(v / 9);
+            const int m = y >> 1;
+            const uint8_t *r0 = src + (int64_t)(3 * m) * stride, *r1 = r0 + stride, *r2 = r1 + stride;
+            for (int x = threadIdx.x; x < qw; x += blockDim.x) {
+                const int k3 = 3 * (x >> 1);
+                const int e = r1[k3 + 1];
+                int v;
+                if ((y & 1) == 0)
+                    v = (x & 1) == 0 ? 4 * r0[k3] + 2 * r0[k3 + 1] + 2 * r1[k3] + e
+                                     : 4 * r0[k3 + 2] + 2 * r0[k3 + 1] + 2 * r1[k3 + 2] + e;
+                else
+                    v = (x & 1) == 0 ? 4 * r2[k3] + 2 * r1[k3] + 2 * r2[k3 + 1] + e
+                                     : 4 * r2[k3 + 2] + 2 * r1[k3 + 2] + 2 * r2[k3 + 1] + e;
+                out[x] = (uint8_t)(v / 9);
+            }
         } else if (factor > 1.0f) {
-            int64_t k = (int64_t)factor;
+            const int k = (int)factor;
             if (k == 2) {
                 // 2x2 box; the part of the row below the largest multiple of
                 // 32 rounds twice (the C library's AVX2 path), the rest once
                 // (fast/image.c:26-46)
-                const uint8_t *r0 = src + 2 * y * stride + 2 * x, *r1 = r0 + stride;
-                int a = r0[0], b = r0[1], c = r1[0], d = r1[1];
-                if (x < f.qw - f.qw % 32)
-                    o = (uint8_t)((((a + c + 1) >> 1) + ((b + d + 1) >> 1) + 1) >> 1);
-                else
-                    o = (uint8_t)((a + b + c + d + 2) >> 2);
+                const uint8_t *r0 = src + (int64_t)(2 * y) * stride, *r1 = r0 + stride;
+                const int xv = qw - qw % 32;
+                for (int x = threadIdx.x; x < qw; x += blockDim.x) {
+                    const int a = r0[2 * x], b = r0[2 * x + 1], c = r1[2 * x], d = r1[2 * x + 1];
+                    out[x] = x < xv ? (uint8_t)((((a + c + 1) >> 1) + ((b + d + 1) >> 1) + 1) >> 1)
+                                    : (uint8_t)((a + b + c + d + 2) >> 2);
+                }
             } else {
-                o = src[y * k * stride + x * k];
+                const uint8_t *r0 = src + (int64_t)y * k * stride;
+                for (int x = threadIdx.x; x < qw; x += blockDim.x) out[x] = r0[(int64_t)x * k];
             }
         } else {
-            o = src[y * stride + x];
+            const uint8_t *r0 = src + (int64_t)y * stride;
+            for (int x = threadIdx.x; x < qw; x += blockDim.x) out[x] = r0[x];
         }
-        out[i] = o;
     }
 }
 
@@ -112,23 +118,26 @@ __global__ void k_decimate(const FrameDesc *frames, const uint8_t *img, uint8_t 
 
 __global__ void k_blur_pass(const FrameDesc *frames, const uint8_t *in, uint8_t *out, BlurTaps taps, int dir) {
     const FrameDesc f = frames[blockIdx.y];
-    const int64_t n = (int64_t)f.qw * f.qh;
-    const bool wide = n >= 65536;
+    const int qw = (int)f.qw, qh = (int)f.qh;
+    const bool wide = (int64_t)qw * qh >= 65536;
     const int nk = taps.n, r = nk / 2;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t y = i / f.qw, x = i - y * f.qw;
-        int64_t len = dir == 0 ? f.qw : f.qh, pos = dir == 0 ? x : y, step = dir == 0 ? 1 : f.qw;
-        const uint8_t *line = in + f.q_off + (dir == 0 ? y * f.qw : x);
-        int64_t m = wide ? len - nk + 1 : len - nk;
-        uint8_t v;
-        if (pos >= r && pos - r < m) {
-            uint32_t acc = 0;
-            for (int j = 0; j < nk; j++) acc += (uint32_t)taps.k[j] * line[(pos - r + j) * step];
-            v = (uint8_t)(acc >> 8);
-        } else {
-            v = line[pos * step];
+    const int len = dir == 0 ? qw : qh;
+    const int m = wide ? len - nk + 1 : len - nk;
+    const int64_t step = dir == 0 ? 1 : qw;
+    for (int y = blockIdx.x; y < qh; y += gridDim.x) {
+        for (int x = threadIdx.x; x < qw; x += blockDim.x) {
+            const int pos = dir == 0 ? x : y;
+            const uint8_t *line = in + f.q_off + (dir == 0 ? (int64_t)y * qw : (int64_t)x);
+            uint8_t v;
+            if (pos >= r && pos - r < m) {
+                uint32_t acc = 0;
+                for (int j = 0; j < nk; j++) acc += (uint32_t)taps.k[j] * line[(int64_t)(pos - r + j) * step];
+                v = (uint8_t)(acc >> 8);
+            } else {
+                v = line[(int64_t)pos * step];
+            }
+            out[f.q_off + (int64_t)y * qw + x] = v;
         }
-        out[f.q_off + i] = v;
     }
 }
 
@@ -171,16 +180,21 @@ __global__ void k_tile_minmax(const FrameDesc *frames, const uint8_t *qim, uint8
     }
 }
 
-// Pixels right of the last whole tile column use that column and are never
-// 127; rows below the last whole tile row use that row and are never 127
-// (fast/threshold.c:85-91, 144-148).
+// A thread per 4x4 tile: the max and min of its 3x3 tile neighbourhood
+// (cells outside the grid left out) once, then its 16 pixels. Pixels right
+// of the last whole tile column use that column and are never 127; rows
+// below the last whole tile row use that row and are never 127
+// (fast/threshold.c:85-91, 144-148): the partial tiles there clamp.
 __global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const uint8_t *tmax, const uint8_t *tmin,
                             uint8_t *thr, int32_t diff) {
     const FrameDesc f = frames[blockIdx.y];
-    const int64_t tw = f.qw / 4, th = f.qh / 4, n = (int64_t)f.qw * f.qh;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t y = i / f.qw, x = i - y * f.qw;
-        int64_t ty = y >> 2, tx = x >> 2;
+    const int qw = (int)f.qw, qh = (int)f.qh;
+    const int tw = qw / 4, th = qh / 4, cw = (qw + 3) / 4, ch = (qh + 3) / 4;
+    const int n = cw * ch;
+    const uint8_t *tx_max = tmax + f.tile_off, *tx_min = tmin + f.tile_off;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int cy = i / cw, cx = i - cy * cw;
+        int ty = cy, tx = cx;
         bool may_flat = true;
         if (ty >= th) {
             ty = th - 1;
@@ -191,14 +205,21 @@ __global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const u
             may_flat = false;
         }
         uint32_t hi = 0, lo = 255;
-        for (int64_t yy = dmax(ty - 1, 0); yy <= dmin(ty + 1, th - 1); yy++)
-            for (int64_t xx = dmax(tx - 1, 0); xx <= dmin(tx + 1, tw - 1); xx++) {
-                hi = max(hi, (uint32_t)tmax[f.tile_off + yy * tw + xx]);
-                lo = min(lo, (uint32_t)tmin[f.tile_off + yy * tw + xx]);
+        const int y0t = ty - 1 > 0 ? ty - 1 : 0, y1t = ty + 1 < th - 1 ? ty + 1 : th - 1;
+        const int x0t = tx - 1 > 0 ? tx - 1 : 0, x1t = tx + 1 < tw - 1 ? tx + 1 : tw - 1;
+        for (int yy = y0t; yy <= y1t; yy++)
+            for (int xx = x0t; xx <= x1t; xx++) {
+                hi = max(hi, (uint32_t)tx_max[yy * tw + xx]);
+                lo = min(lo, (uint32_t)tx_min[yy * tw + xx]);
             }
-        uint32_t t = lo + (hi - lo) / 2;
-        uint8_t v = qim[f.q_off + i] > t ? 255 : 0;
-        thr[f.q_off + i] = may_flat && (int32_t)(hi - lo) < diff ? 127 : v;
+        const uint32_t t = lo + (hi - lo) / 2;
+        const bool flat = may_flat && (int32_t)(hi - lo) < diff;
+        const int x0 = 4 * cx, y0 = 4 * cy;
+        const int xe = x0 + 4 < qw ? x0 + 4 : qw, ye = y0 + 4 < qh ? y0 + 4 : qh;
+        for (int y = y0; y < ye; y++) {
+            const int64_t o = f.q_off + (int64_t)y * qw;
+            for (int x = x0; x < xe; x++) thr[o + x] = flat ? 127 : (qim[o + x] > t ? 255 : 0);
+        }
     }
 }
 
@@ -206,21 +227,23 @@ __global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const u
 // zero), then 3x3 erode back; the image border keeps its values.
 __global__ void k_morph(const FrameDesc *frames, const uint8_t *in, uint8_t *out, int dilate) {
     const FrameDesc f = frames[blockIdx.y];
-    const int64_t n = (int64_t)f.qw * f.qh;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t y = i / f.qw, x = i - y * f.qw;
-        bool border = x == 0 || y == 0 || x == f.qw - 1 || y == f.qh - 1;
-        if (border) {
-            if (dilate) out[f.q_off + i] = 0;
-            continue;
-        }
-        uint32_t m = dilate ? 0 : 255;
-        for (int dy = -1; dy <= 1; dy++)
-            for (int dx = -1; dx <= 1; dx++) {
-                uint32_t v = in[f.q_off + (y + dy) * f.qw + x + dx];
-                m = dilate ? max(m, v) : min(m, v);
+    const int qw = (int)f.qw, qh = (int)f.qh;
+    for (int y = blockIdx.x; y < qh; y += gridDim.x) {
+        const int64_t row = f.q_off + (int64_t)y * qw;
+        for (int x = threadIdx.x; x < qw; x += blockDim.x) {
+            const bool border = x == 0 || y == 0 || x == qw - 1 || y == qh - 1;
+            if (border) {
+                if (dilate) out[row + x] = 0;
+                continue;
             }
-        out[f.q_off + i] = (uint8_t)m;
+            uint32_t m = dilate ? 0 : 255;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const uint32_t v = in[row + (int64_t)dy * qw + x + dx];
+                    m = dilate ? max(m, v) : min(m, v);
+                }
+            out[row + x] = (uint8_t)m;
+        }
     }
 }
 
@@ -420,7 +443,7 @@ __device__ __forceinline__ uint32_t uf_root(const uint32_t *par, uint32_t x) {
 }
 
 // Each node adds its pixels and offers its id to its root (one atomic per
-// distinct root of a warp).
+// distinct root of a warp), and from here on points at its root.
 __global__ void __launch_bounds__(256) k_row_sums(const FrameDesc *frames, RunArrays runs, const uint32_t *row_nruns) {
     const FrameDesc f = frames[blockIdx.y];
     const int lane = threadIdx.x & 31;
@@ -434,6 +457,9 @@ __global__ void __launch_bounds__(256) k_row_sums(const FrameDesc *frames, RunAr
             if (!valid) continue;
             const int64_t node = i < n ? base + i : f.node_off + (int64_t)f.qw * f.qh + y;
             const uint32_t r = uf_root(runs.parent, (uint32_t)node);
+            // no unions run any more: pointing straight at the root is safe
+            // for the walks of other threads, and the labels read it once
+            if (r != (uint32_t)node) runs.parent[node] = r;
             const uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
             const uint32_t peers = __match_any_sync(live, r);
             uint32_t sum = 0, mn = 0xffffffffu;
@@ -452,34 +478,81 @@ __global__ void __launch_bounds__(256) k_row_sums(const FrameDesc *frames, RunAr
 }
 
 // Per pixel: its component's label if the component has at least
-// min_cluster_pixels pixels, else AT_NOK (no run: 127, or too small).
-__global__ void k_labels(const FrameDesc *frames, const RunArrays runs, const uint32_t *row_nruns, uint32_t *lab,
-                         int32_t min_px) {
+// min_cluster_pixels pixels, else AT_NOK (no run: 127, or too small). A
+// block per row: each run's label once (every node points at its root after
+// k_row_sums), spread over the run's pixels by a max-scan of the run starts;
+// the last column is the row's extra node.
+#define LAB_THREADS 256
+__global__ void __launch_bounds__(LAB_THREADS) k_labels(const FrameDesc *frames, const RunArrays runs,
+                                                        const uint32_t *row_nruns, uint32_t *lab, int32_t min_px) {
+    __shared__ uint32_t s_run[ROW_STAGE];
+    __shared__ uint32_t s_rlab[ROW_STAGE];
+    __shared__ uint16_t s_end[ROW_STAGE];
+    __shared__ uint32_t s_wmax[LAB_THREADS / 32];
     const FrameDesc f = frames[blockIdx.y];
-    const int64_t n = (int64_t)f.qw * f.qh;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t y = i / f.qw, x = i - y * f.qw;
-        int64_t node = -1;
-        if (x == f.qw - 1) {
-            node = f.node_off + (int64_t)f.qw * f.qh + y;
-        } else {
-            const int64_t base = f.node_off + y * f.qw;
-            int64_t lo = 0, hi = row_nruns[f.row0 + y];
-            while (lo < hi) {  // the first run with start > x
-                int64_t mid = (lo + hi) >> 1;
-                if ((int64_t)runs.start[base + mid] <= x)
-                    lo = mid + 1;
-                else
-                    hi = mid;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int qw = (int)f.qw, W = qw - 1;
+    for (int y = blockIdx.x; y < (int)f.qh; y += gridDim.x) {
+        const int64_t base = f.node_off + (int64_t)y * qw;
+        const int nr = (int)row_nruns[f.row0 + y];
+        uint32_t *out = lab + f.q_off + (int64_t)y * qw;
+        if (tid == 0) {
+            const uint32_t r = runs.parent[f.node_off + (int64_t)qw * f.qh + y];
+            out[W] = (int64_t)runs.px[r] >= min_px ? runs.minid[r] : AT_NOK;
+        }
+        if (W > ROW_STAGE) {
+            // rows too wide to stage: a binary search per pixel
+            for (int x = tid; x < W; x += LAB_THREADS) {
+                int lo = 0, hi = nr;
+                while (lo < hi) {  // the first run with start > x
+                    const int mid = (lo + hi) >> 1;
+                    if ((int)runs.start[base + mid] <= x)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                uint32_t l = AT_NOK;
+                if (lo > 0 && (int)runs.end[base + lo - 1] >= x) {
+                    const uint32_t r = runs.parent[base + lo - 1];
+                    if ((int64_t)runs.px[r] >= min_px) l = runs.minid[r];
+                }
+                out[x] = l;
             }
-            if (lo > 0 && (int64_t)runs.end[base + lo - 1] >= x) node = base + lo - 1;
+            continue;
         }
-        uint32_t l = AT_NOK;
-        if (node >= 0) {
-            uint32_t r = uf_root(runs.parent, (uint32_t)node);
-            if ((int64_t)runs.px[r] >= min_px) l = runs.minid[r];
+        __syncthreads();
+        for (int x = tid; x < W; x += LAB_THREADS) s_run[x] = 0;
+        __syncthreads();
+        for (int i = tid; i < nr; i += LAB_THREADS) {
+            s_run[runs.start[base + i]] = (uint32_t)i + 1;
+            s_end[i] = runs.end[base + i];
+            const uint32_t r = runs.parent[base + i];
+            s_rlab[i] = (int64_t)runs.px[r] >= min_px ? runs.minid[r] : AT_NOK;
         }
-        lab[f.q_off + i] = l;
+        __syncthreads();
+        // thread t owns pixels [t * seg, t * seg + seg): the largest run
+        // number started at or before each of them
+        const int seg = (W + LAB_THREADS - 1) / LAB_THREADS;
+        const int x0 = tid * seg, x1 = x0 + seg < W ? x0 + seg : W;
+        uint32_t m = 0;
+        for (int x = x0; x < x1; x++) m = max(m, s_run[x]);
+        uint32_t incl = m;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl = max(incl, t);
+        }
+        if (lane == 31) s_wmax[wid] = incl;
+        uint32_t run = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) run = 0;
+        __syncthreads();
+        for (int w = 0; w < wid; w++) run = max(run, s_wmax[w]);
+        for (int x = x0; x < x1; x++) {
+            run = max(run, s_run[x]);
+            s_run[x] = run && x <= (int)s_end[run - 1] ? s_rlab[run - 1] : AT_NOK;
+        }
+        __syncthreads();
+        for (int x = tid; x < W; x += LAB_THREADS) out[x] = s_run[x];
     }
 }
 
@@ -814,14 +887,21 @@ __host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk) {
 
 // Optional phase timers of the fit kernel (a -DAT_FIT_PROF build only).
 #ifdef AT_FIT_PROF
-__device__ long long g_fitprof[16384][12];
+#define FIT_PROF_N 32768
+__device__ long long g_fitprof[FIT_PROF_N][12];
 #define FIT_PROF(k)                                              \
-    if (tid == 0 && c < 16384) g_fitprof[c][k] = clock64();
+    if (tid == 0 && c < FIT_PROF_N) g_fitprof[c][k] = clock64();
+#define FITW_PROF(k)                                             \
+    if (lane == 0 && c < FIT_PROF_N) g_fitprof[c][k] = clock64();
+#define FITW_SIZE(n)                                             \
+    if (lane == 0 && c < FIT_PROF_N) g_fitprof[c][0] = (n);
 extern "C" int at_fit_prof_copy(void *dst, int n) {
     return (int)cudaMemcpyFromSymbol(dst, g_fitprof, (size_t)n * 12 * 8);
 }
 #else
 #define FIT_PROF(k)
+#define FITW_PROF(k)
+#define FITW_SIZE(n)
 #endif
 
 template <int NT>
@@ -1294,101 +1374,128 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
 }
 
 // ---------------------------------------------------------------------------
-// Clusters of at most FIT_WARP points: one warp each, FIT_WPB per block, no
-// block barriers. The same steps as k_fit_quads, with warp primitives.
-#define FIT_WARP 256
-#define FIT_WPB 4
+// Clusters of at most 32 * R points: one warp each, FIT_WPB per block, no
+// block barriers. The same steps as k_fit_quads; the angle sort is a bitonic
+// sort in registers, the prefix moments stay in shared memory.
+#define FIT_WPB 2
 
-// per warp: sort keys and values (region A), the sort's second buffer reused
-// for the moment staging (region B), and the pair fits (4 * mm * mm)
-__host__ __device__ constexpr size_t fit_warp_smem(int mm) {
-    return (size_t)FIT_WARP * 36 + (size_t)4 * mm * mm * 8;
+// The 4-subsets {m0 < m1 < m2 < m3} of {0..15} in colex order (by m3, then
+// m2, m1, m0), one per entry as nibbles m0 | m1 << 4 | m2 << 8 | m3 << 12:
+// the first C(n, 4) entries are the 4-subsets of {0..n-1}.
+struct Quad4Table {
+    uint16_t v[1820];
+};
+constexpr Quad4Table make_quad4() {
+    Quad4Table t{};
+    int k = 0;
+    for (int d = 3; d < 16; d++)
+        for (int c = 2; c < d; c++)
+            for (int b = 1; b < c; b++)
+                for (int a = 0; a < b; a++) t.v[k++] = (uint16_t)(a | b << 4 | c << 8 | d << 12);
+    return t;
+}
+__device__ const Quad4Table g_quad4 = make_quad4();
+static_assert(AT_MAX_NMAXIMA <= 16, "the 4-subset table covers 16 maxima");
+
+__host__ __device__ constexpr int binom4(int n) { return n < 4 ? 0 : n * (n - 1) * (n - 2) * (n - 3) / 24; }
+
+// per warp: six prefix arrays, then region x0 (angle keys; errors; the
+// maxima) and region x1 (dot terms; filtered errors; the pair fits)
+__host__ __device__ constexpr size_t fit_warp_x1(int cap, int mm) {
+    return (size_t)8 * cap > (size_t)32 * mm * mm ? (size_t)8 * cap : (size_t)32 * mm * mm;
+}
+__host__ __device__ constexpr size_t fit_warp_smem(int cap, int mm) {
+    return (size_t)56 * cap + fit_warp_x1(cap, mm);
 }
 
-// merge sort of one warp (see block_merge_sort)
-__device__ void warp_merge_sort(uint64_t *ka, uint32_t *va, uint64_t *kb, uint32_t *vb, int n, int lane) {
-    uint64_t *sk = ka, *dk = kb;
-    uint32_t *sv = va, *dv = vb;
-    const int ipt = (n + 31) / 32;
-    for (int w = 1; w < n; w <<= 1) {
-        const int o1 = min(n, lane * ipt + ipt);
-        int o = lane * ipt;
-        while (o < o1) {
-            const int lo = (o / (2 * w)) * (2 * w);
-            const int la = min(w, n - lo), lb = max(0, min(w, n - lo - la));
-            const uint64_t *A = sk + lo, *B = sk + lo + la;
-            const int k = o - lo, seg_end = min(o1, lo + la + lb);
-            int l = max(0, k - lb), h = min(k, la);
-            while (l < h) {
-                const int m = (l + h) >> 1;
-                if (A[m] < B[k - m - 1])
-                    l = m + 1;
-                else
-                    h = m;
-            }
-            int i = l, j = k - l;
-            for (; o < seg_end; o++) {
-                const bool take_a = j >= lb || (i < la && A[i] < B[j]);
-                if (take_a) {
-                    dk[o] = A[i];
-                    dv[o] = sv[lo + i];
-                    i++;
-                } else {
-                    dk[o] = B[j];
-                    dv[o] = sv[lo + la + j];
-                    j++;
+// The leaf of position p of n (see leaf_of), in 32-bit arithmetic.
+__device__ __forceinline__ void leaf_of32(int n, int p, int &lo, int &len) {
+    int l = 0, sz = n;
+    while (sz / 2 > 5) {
+        const int half = sz / 2, q1 = half / 2, q3 = half + (sz - half) / 2;
+        const int r = p - l;
+        if (r < q1) {
+            sz = q1;
+        } else if (r < half) {
+            l += q1;
+            sz = half - q1;
+        } else if (r < q3) {
+            l += half;
+            sz = q3 - half;
+        } else {
+            l += q3;
+            sz = sz - q3;
+        }
+    }
+    while (sz > 5) {
+        const int half = sz / 2;
+        if (p - l >= half) {
+            l += half;
+            sz -= half;
+        } else {
+            sz = half;
+        }
+    }
+    lo = l;
+    len = sz;
+}
+
+// Bitonic sort, ascending, of a warp's keys k[0, np) in shared memory (np
+// a power of two): log2(np) (log2(np) + 1) / 2 steps of np / 2 exchanges.
+__device__ void warp_bitonic(uint64_t *k, int np, int lane) {
+    for (int kk = 2; kk <= np; kk <<= 1) {
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            for (int q = lane; q < np / 2; q += 32) {
+                const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1)), l = i + j;
+                const uint64_t a = k[i], b = k[l];
+                if (((i & kk) == 0) == (a > b)) {
+                    k[i] = b;
+                    k[l] = a;
                 }
             }
+            __syncwarp();
         }
-        __syncwarp();
-        uint64_t *tk = sk;
-        sk = dk;
-        dk = tk;
-        uint32_t *tv = sv;
-        sv = dv;
-        dv = tv;
-    }
-    if (sk != ka) {
-        for (int t = lane; t < n; t += 32) {
-            ka[t] = sk[t];
-            va[t] = sv[t];
-        }
-        __syncwarp();
     }
 }
 
+template <int R>
 __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
                                                           const uint64_t *pts, const uint32_t *cstart,
                                                           const int32_t *cframe, int64_t nclusters, int64_t npoints,
-                                                          FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, int mm) {
+                                                          GpuQuad *quads, uint32_t *quad_ok, int64_t class_lo, int mm) {
+    constexpr int CAP = 32 * R;
     extern __shared__ __align__(16) unsigned char fw_smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
-    unsigned char *base = fw_smem + fit_warp_smem(mm) * wid;
-    uint64_t *ka = reinterpret_cast<uint64_t *>(base);
-    uint32_t *va = reinterpret_cast<uint32_t *>(ka + FIT_WARP);
-    unsigned char *rb = base + FIT_WARP * 12;
-    uint64_t *kb = reinterpret_cast<uint64_t *>(rb);
-    uint32_t *vb = reinterpret_cast<uint32_t *>(kb + FIT_WARP);
-    double *s_w = reinterpret_cast<double *>(rb), *s_fx = s_w + FIT_WARP, *s_fy = s_fx + FIT_WARP;
-    float *s_term = reinterpret_cast<float *>(rb);
-    double *s_perr = reinterpret_cast<double *>(base + FIT_WARP * 36);
-    double *s_pmse = s_perr + mm * mm, *s_pnx = s_pmse + mm * mm, *s_pny = s_pnx + mm * mm;
+    unsigned char *base = fw_smem + fit_warp_smem(CAP, mm) * wid;
+    double *pm = reinterpret_cast<double *>(base);  // prefix array q at pm + q * CAP
+    unsigned char *x0 = base + 48 * CAP, *x1 = x0 + 8 * CAP;
+    uint64_t *s_akey = reinterpret_cast<uint64_t *>(x0);
+    double *s_err = reinterpret_cast<double *>(x0);
+    double *s_mxe = reinterpret_cast<double *>(x0);
+    int32_t *s_mxi = reinterpret_cast<int32_t *>(x0 + 4 * CAP);
+    float *s_term = reinterpret_cast<float *>(x1);
+    double *s_filt = reinterpret_cast<double *>(x1);
+    double *s_perr = reinterpret_cast<double *>(x1), *s_pmse = s_perr + mm * mm, *s_pnx = s_pmse + mm * mm,
+           *s_pny = s_pnx + mm * mm;
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
 
     for (int64_t c = (int64_t)blockIdx.x * FIT_WPB + wid; c < nclusters; c += (int64_t)gridDim.x * FIT_WPB) {
         const int64_t s0 = cstart[c];
         const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
-        if (sz > FIT_WARP) continue;  // the block kernels' clusters
+        if (sz < class_lo || sz > CAP) continue;  // another class's kernel
         const FrameDesc f = frames[cframe[c]];
         if (lane == 0) quad_ok[c] = 0;
         if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
         const int n = (int)sz;
+        FITW_SIZE(n)
+        FITW_PROF(1)
         const uint64_t *P = pts + s0;
         // bounding box (fast/quads.c:515-528)
         uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
         for (int i = lane; i < n; i += 32) {
-            uint32_t x = (uint32_t)(P[i] & 0xffff), y = (uint32_t)(P[i] >> 16 & 0xffff);
+            const uint64_t pt = P[i];
+            const uint32_t x = (uint32_t)(pt & 0xffff), y = (uint32_t)(pt >> 16 & 0xffff);
             xmin = min(xmin, x);
             xmax = max(xmax, x);
             ymin = min(ymin, y);
@@ -1401,35 +1508,43 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             ymax = max(ymax, __shfl_xor_sync(FULL, ymax, o));
         }
         if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < prm.tag_width) continue;
+        FITW_PROF(2)
         const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
         const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
 
-        // the dot product of offsets and gradients: lane l < 8 sums terms
-        // l, l+8, ... of the whole groups of 8; then the rest in order
+        // angle keys (fast/quads.c:429-453) and the dot product of offsets
+        // and gradients (fast/quads.c:467-512): lane l < 8 sums terms l,
+        // l+8, ... of the whole groups of 8; then the rest in order
         const int nv = n - n % 8;
-        for (int i = lane; i < nv; i += 32) {
-            uint64_t pt = P[i];
-            float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
-            float gx = (float)(int16_t)(pt >> 32 & 0xffff), gy = (float)(int16_t)(pt >> 48);
+        for (int i = lane; i < n; i += 32) {
+            const uint64_t pt = P[i];
+            const float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
+            s_akey[i] = angle_key(dx, dy, (uint32_t)i);
+            const float gx = (float)(int16_t)(pt >> 32 & 0xffff), gy = (float)(int16_t)(pt >> 48);
             s_term[i] = __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy));
         }
         __syncwarp();
         float acc = 0.0f;
-        if (lane < 8)
-            for (int i = lane; i < nv; i += 8) acc = __fadd_rn(acc, s_term[i]);
-        float l[8];
+        if (lane < 8) {
+            int i = lane;
+            for (; i + 56 < nv; i += 64) {
+                float v[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) l[k] = __shfl_sync(FULL, acc, k);
+                for (int u = 0; u < 8; u++) v[u] = s_term[i + 8 * u];
+#pragma unroll
+                for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, v[u]);
+            }
+            for (; i < nv; i += 8) acc = __fadd_rn(acc, s_term[i]);
+        }
+        float l8[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) l8[k] = __shfl_sync(FULL, acc, k);
         int okrev = 0;
         if (lane == 0) {
-            float dot = __fadd_rn(__fadd_rn(__fadd_rn(l[0], l[4]), __fadd_rn(l[2], l[6])),
-                                  __fadd_rn(__fadd_rn(l[1], l[5]), __fadd_rn(l[3], l[7])));
-            for (int i = nv; i < n; i++) {
-                float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
-                float gx = (float)(int16_t)(P[i] >> 32 & 0xffff), gy = (float)(int16_t)(P[i] >> 48);
-                dot = __fadd_rn(dot, __fadd_rn(__fmul_rn(dx, gx), __fmul_rn(dy, gy)));
-            }
-            int rev = dot < 0.0f;
+            float dot = __fadd_rn(__fadd_rn(__fadd_rn(l8[0], l8[4]), __fadd_rn(l8[2], l8[6])),
+                                  __fadd_rn(__fadd_rn(l8[1], l8[5]), __fadd_rn(l8[3], l8[7])));
+            for (int i = nv; i < n; i++) dot = __fadd_rn(dot, s_term[i]);
+            const int rev = dot < 0.0f;
             int ok = 1;
             if (!prm.reversed_border && rev) ok = 0;
             if (!prm.normal_border && !rev) ok = 0;
@@ -1438,66 +1553,80 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         okrev = __shfl_sync(FULL, okrev, 0);
         if (!(okrev & 1)) continue;
         const int rev = okrev >> 1;
-        __syncwarp();
+        FITW_PROF(3)
 
-        // the angle sort: per leaf, its network order, block heads and
-        // places; then a sort by (head, place) (see k_fit_quads)
-        for (int p = lane; p < n; p += 32) {
-            uint32_t lf = leaf_of(n, p);
-            int lo = (int)(lf >> 8), len = (int)(lf & 255);
-            if (p != lo) continue;
-            uint64_t k5[5];
-            for (int t = 0; t < len; t++) {
-                uint64_t pt = P[lo + t];
-                float dx = __fsub_rn((float)(pt & 0xffff), cx), dy = __fsub_rn((float)(pt >> 16 & 0xffff), cy);
-                k5[t] = angle_key(dx, dy, (uint32_t)(lo + t));
+        // The angle sort (see k_fit_quads): position i of leaf (lo, len)
+        // takes place t = i - lo of the leaf's network order; its sort key
+        // packs the slope bits of its block head, 0xffff - the head's index,
+        // t, and (below the order, since the rest is distinct) the index of
+        // its point. The keys live in the last prefix array until the moments.
+        uint64_t *s_skey = reinterpret_cast<uint64_t *>(pm + 5 * CAP);
+        int np = 32;
+        while (np < n) np <<= 1;
+        for (int i = lane; i < np; i += 32) {
+            uint64_t key = ~0ull;
+            if (i < n) {
+                int lo, len;
+                leaf_of32(n, i, lo, len);
+                uint64_t a[5];
+#pragma unroll
+                for (int t = 0; t < 5; t++) a[t] = t < len ? s_akey[lo + t] : ~0ull;
+                leaf_network(a, len);
+                const int tp = i - lo;
+                uint64_t head = a[0], e = a[0];
+#pragma unroll
+                for (int t = 1; t < 5; t++) {
+                    if (t <= tp) {
+                        if (a[t] > head) head = a[t];
+                        e = a[t];
+                    }
+                }
+                const uint32_t hidx = ~(uint32_t)head;
+                key = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 16 | (uint64_t)tp << 13 |
+                      (uint64_t)(~(uint32_t)e & 0x1fffu);
             }
-            leaf_network(k5, len);
-            uint64_t head = 0;
-            for (int t = 0; t < len; t++) {
-                if (t == 0 || k5[t] > head) head = k5[t];
-                uint32_t hidx = ~(uint32_t)head;
-                ka[lo + t] = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 3 | (uint64_t)t;
-                va[lo + t] = ~(uint32_t)k5[t];
-            }
+            s_skey[i] = key;
         }
         __syncwarp();
-        warp_merge_sort(ka, va, kb, vb, n, lane);
+        FITW_PROF(4)
+        warp_bitonic(s_skey, np, lane);
+        FITW_PROF(5)
 
-        // cumulative weighted moments in angle order (fast/quads.c:968-1035)
+        // cumulative weighted moments in angle order (fast/quads.c:968-1035):
+        // every lane stages the six terms of its positions, then lane q < 6
+        // turns array q into its prefix sums in place
         const uint8_t *im = qim + f.q_off;
         for (int k = lane; k < n; k += 32) {
-            uint32_t src = va[k];
-            int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
-            int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
+            const uint64_t p = P[s_skey[k] & 0x1fffu];
+            const int32_t px = (int32_t)(p & 0xffff), py = (int32_t)(p >> 16 & 0xffff);
+            const int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
             int32_t g2 = 0;
             if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
-                int64_t cc = (int64_t)iy * f.qw + ix;
-                int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
-                int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
+                const int64_t cc = (int64_t)iy * f.qw + ix;
+                const int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
+                const int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
                 g2 = gx * gx + gy * gy;
             }
-            s_w[k] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
-            s_fx[k] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
-            s_fy[k] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+            const double w = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
+            const double fx = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
+            const double fy = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+            const double wx = __dmul_rn(w, fx), wy = __dmul_rn(w, fy);
+            pm[0 * CAP + k] = wx;
+            pm[1 * CAP + k] = wy;
+            pm[2 * CAP + k] = __dmul_rn(wx, fx);
+            pm[3 * CAP + k] = __dmul_rn(wx, fy);
+            pm[4 * CAP + k] = __dmul_rn(wy, fy);
+            pm[5 * CAP + k] = w;
         }
         __syncwarp();
-        double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
         if (lane < 6) {
-            const int ca = lane == 1 || lane == 4 ? 1 : lane == 5 ? 2 : 0;  // 0 fx, 1 fy, 2 one
-            const int cb = lane == 2 ? 0 : lane == 3 || lane == 4 ? 1 : 2;
-            const double *A = ca == 0 ? s_fx : s_fy, *Bv = cb == 0 ? s_fx : s_fy;
-            double *o = M[lane];
+            double *o = pm + lane * CAP;
             double run = 0.0;
             int t = 0;
             for (; t + 8 <= n; t += 8) {
                 double v[8];
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    double a = ca == 2 ? 1.0 : A[t + u];
-                    double b = cb == 2 ? 1.0 : Bv[t + u];
-                    v[u] = __dmul_rn(__dmul_rn(s_w[t + u], a), b);
-                }
+                for (int u = 0; u < 8; u++) v[u] = o[t + u];
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
                     run = __dadd_rn(run, v[u]);
@@ -1505,66 +1634,63 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
                 }
             }
             for (; t < n; t++) {
-                double a = ca == 2 ? 1.0 : A[t];
-                double b = cb == 2 ? 1.0 : Bv[t];
-                run = __dadd_rn(run, __dmul_rn(__dmul_rn(s_w[t], a), b));
+                run = __dadd_rn(run, o[t]);
                 o[t] = run;
             }
         }
         __syncwarp();
-        const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
+        FITW_PROF(6)
+        const Moments mo = {pm, pm + CAP, pm + 2 * CAP, pm + 3 * CAP, pm + 4 * CAP, pm + 5 * CAP};
 
         // corner search (fast/quads.c:788-959)
-        const int64_t ksz = dmin(20, sz / 12);
+        const int ksz = min(20, n / 12);
         if (ksz < 2) continue;
         const double nn = (double)(2 * ksz + 1);
-        double *errs = scr.errs + s0, *filt = scr.filt + s0;
         for (int i = lane; i < n; i += 32) {
-            int64_t i0 = i - ksz, i1 = i + ksz;
+            const int i0 = i - ksz, i1 = i + ksz;
             MSum s;
             if (i0 < 0)
-                s = seg_moments(mo, sz, i0 + sz, i1);
-            else if (i1 < sz)
-                s = seg_moments(mo, sz, i0, i1);
+                s = seg_moments(mo, n, i0 + n, i1);
+            else if (i1 < n)
+                s = seg_moments(mo, n, i0, i1);
             else
-                s = seg_moments(mo, sz, i0, i1 - sz);
-            errs[i] = window_error(s, nn);
+                s = seg_moments(mo, n, i0, i1 - n);
+            s_err[i] = window_error(s, nn);
         }
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
             double a;
             if (i >= 3 && i < n - 3) {
-                a = errs[i - 3] * prm.qsm[0];
-                for (int t = 1; t < 7; t++) a = a + errs[i - 3 + t] * prm.qsm[t];
+                a = s_err[i - 3] * prm.qsm[0];
+                for (int t = 1; t < 7; t++) a = a + s_err[i - 3 + t] * prm.qsm[t];
             } else {
                 a = 0.0;
                 for (int t = 0; t < 7; t++) {
                     int j = i - 3 + t;
                     if (j < 0) j += n;
                     if (j >= n) j -= n;
-                    a = a + errs[j] * prm.qsm[t];
+                    a = a + s_err[j] * prm.qsm[t];
                 }
             }
-            filt[i] = a;
+            s_filt[i] = a;
         }
         __syncwarp();
-        int32_t *mxi = scr.mxi + s0;
-        double *mxe = scr.mxe + s0;
+        FITW_PROF(7)
         int nm = 0;
         for (int i0 = 0; i0 < n; i0 += 32) {
             const int i = i0 + lane;
             bool is_max = false;
             double e = 0.0;
             if (i < n) {
-                e = filt[i];
-                double lft = filt[i == 0 ? n - 1 : i - 1], rgt = filt[i + 1 == n ? 0 : i + 1];
+                e = s_filt[i];
+                const double lft = s_filt[i == 0 ? n - 1 : i - 1], rgt = s_filt[i + 1 == n ? 0 : i + 1];
                 is_max = e > lft && e > rgt;
             }
             const uint32_t bal = __ballot_sync(FULL, is_max);
             if (is_max) {
                 const int at = nm + __popc(bal & ((1u << lane) - 1u));
-                mxi[at] = i;
-                mxe[at] = e;
+                s_mxi[at] = i;
+                s_mxe[at] = e;
             }
             nm += __popc(bal);
         }
@@ -1579,27 +1705,28 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
                 bool keep = false;
                 int32_t mi = 0;
                 if (i < nm) {
-                    const double ei = mxe[i];
+                    const double ei = s_mxe[i];
                     int ge = 0;
-                    for (int j = 0; j < nm && ge <= k; j++) ge += mxe[j] >= ei;
+                    for (int j = 0; j < nm && ge <= k; j++) ge += s_mxe[j] >= ei;
                     keep = ge <= k;
-                    mi = mxi[i];
+                    mi = s_mxi[i];
                 }
                 const uint32_t bal = __ballot_sync(FULL, keep);
                 __syncwarp();
-                if (keep) mxi[kept + __popc(bal & ((1u << lane) - 1u))] = mi;
+                if (keep) s_mxi[kept + __popc(bal & ((1u << lane) - 1u))] = mi;
                 kept += __popc(bal);
             }
             __syncwarp();
             nm = kept;
         }
+        FITW_PROF(8)
         // line fits of pairs of maxima
         for (int t = lane; t < nm * nm; t += 32) {
             const int p = t / nm, q = t - p * nm;
             if (!(p < q || p >= q + 3)) continue;
-            const int64_t i0 = mxi[p], i1 = mxi[q];
-            MSum s = seg_moments(mo, sz, i0, i1);
-            double cnt = (double)(i0 <= i1 ? i1 - i0 + 1 : sz - i0 + i1 + 1);
+            const int i0 = s_mxi[p], i1 = s_mxi[q];
+            const MSum s = seg_moments(mo, n, i0, i1);
+            const double cnt = (double)(i0 <= i1 ? i1 - i0 + 1 : n - i0 + i1 + 1);
             double lp[4], mse;
             line_of(s, lp, &mse);
             s_perr[t] = cnt * mse;
@@ -1608,43 +1735,45 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             s_pny[t] = lp[3];
         }
         __syncwarp();
-        // the first smallest total error in (m0, m1, m2, m3) order
+        FITW_PROF(9)
+        // the first smallest total error in (m0, m1, m2, m3) order: the
+        // smallest (error, m0 m1 m2 m3) over the 4-subsets of the maxima
         double be = inf;
-        int64_t bo = INT64_MAX;
-        for (int t = lane; t < nm * nm * nm; t += 32) {
-            const int m0 = t / (nm * nm), m1 = (t / nm) % nm, m2 = t % nm;
-            if (!(m0 < m1 && m1 < m2 && m2 < nm - 1)) continue;
+        int bo = 0xffff;
+        const int nsub = binom4(nm);
+        for (int t = lane; t < nsub; t += 32) {
+            const int v = g_quad4.v[t];
+            const int m0 = v & 15, m1 = v >> 4 & 15, m2 = v >> 8 & 15, m3 = v >> 12;
             const int p01 = m0 * nm + m1, p12 = m1 * nm + m2;
             if (s_pmse[p01] > prm.max_mse || s_pmse[p12] > prm.max_mse) continue;
             const double dot = s_pnx[p01] * s_pnx[p12] + s_pny[p01] * s_pny[p12];
             if (fabs(dot) > prm.max_dot) continue;
+            const int p23 = m2 * nm + m3, p30 = m3 * nm + m0;
             const double e012 = s_perr[p01] + s_perr[p12];
-            for (int m3 = m2 + 1; m3 < nm; m3++) {
-                const int p23 = m2 * nm + m3, p30 = m3 * nm + m0;
-                const double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
-                const double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
-                const double e = e012 + e23 + e30;
-                if (e < be) {
-                    be = e;
-                    bo = (int64_t)t * nm + m3;
-                }
+            const double e23 = s_pmse[p23] > prm.max_mse ? inf : s_perr[p23];
+            const double e30 = s_pmse[p30] > prm.max_mse ? inf : s_perr[p30];
+            const double e = e012 + e23 + e30;
+            const int ord = m0 << 12 | m1 << 8 | m2 << 4 | m3;
+            if (e < be || (e == be && ord < bo)) {
+                be = e;
+                bo = ord;
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
-            double e2 = __shfl_xor_sync(FULL, be, o);
-            int64_t o2 = __shfl_xor_sync(FULL, bo, o);
+            const double e2 = __shfl_xor_sync(FULL, be, o);
+            const int o2 = __shfl_xor_sync(FULL, bo, o);
             if (e2 < be || (e2 == be && o2 < bo)) {
                 be = e2;
                 bo = o2;
             }
         }
+        FITW_PROF(10)
         if (!(be != inf && be / (double)sz < prm.max_mse)) continue;
         // the 4 line fits, lanes 0-3 (quads.c:1069-1075)
         double ln[4] = {0.0, 0.0, 0.0, 0.0}, lmse = 0.0;
         if (lane < 4) {
-            const int64_t t = bo / nm, m3 = bo % nm;
-            const int64_t mi[4] = {t / (nm * nm), (t / nm) % nm, t % nm, m3};
-            line_of(seg_moments(mo, sz, mxi[mi[lane]], mxi[mi[(lane + 1) & 3]]), ln, &lmse);
+            const int ma = bo >> (12 - 4 * lane) & 15, mb = bo >> (12 - 4 * ((lane + 1) & 3)) & 15;
+            line_of(seg_moments(mo, n, s_mxi[ma], s_mxi[mb]), ln, &lmse);
         }
         double lines[4][4], lm[4];
 #pragma unroll
@@ -2420,7 +2549,7 @@ int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr,
     k_row_runs<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
     k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
     k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
-    k_labels<<<frame_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+    k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
     return 4;
 }
 
@@ -2443,6 +2572,21 @@ void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *
     k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe);
 }
 
+// One size class of the warp fit kernel on stream s: enough blocks to fill
+// every SM as far as shared memory allows.
+template <int R>
+static void launch_fit_warp(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+                            const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
+                            int64_t npoints, GpuQuad *quads, uint32_t *quad_ok, int64_t class_lo, int mm) {
+    const size_t wsm = fit_warp_smem(32 * R, mm) * FIT_WPB;
+    cudaFuncSetAttribute(k_fit_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    const int64_t per_sm = (int64_t)(225 * 1024 / (wsm + 1024));
+    const int64_t full = 148 * (per_sm < 1 ? 1 : per_sm > 32 ? 32 : per_sm);
+    const int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
+    k_fit_warp<R><<<(unsigned)(wb < full ? wb : full), FIT_WPB * 32, wsm, s>>>(
+        frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, class_lo, mm);
+}
+
 void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
                       cudaEvent_t join2, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
@@ -2451,8 +2595,10 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
     const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL), large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
     cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
-    // three size classes on three streams: the few large clusters (a block
-    // of 512 each), the middle ones (128), the many small ones (a warp each)
+    const int mm = prm.max_nmaxima > 4 ? prm.max_nmaxima : 4;
+    // size classes on three streams: the few large clusters (a block of 512
+    // each); the middle ones (a warp each up to 512 points, then a block of
+    // 128); the many small ones (a warp each)
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     cudaStreamWaitEvent(side2, fork, 0);
@@ -2460,18 +2606,13 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
         frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, quads, quad_ok, err, FIT_SMALL + 1,
         INT64_MAX, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaEventRecord(join, side);
+    launch_fit_warp<16>(side2, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 257, mm);
     unsigned mid = (unsigned)(nclusters < 148 * 16 ? nclusters : 148 * 16);
     k_fit_quads<128><<<mid, 128, small, side2>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
-                                                 quads, quad_ok, err, FIT_WARP + 1, FIT_SMALL, FIT_SMALL,
-                                                 FIT_CHUNK_SMALL);
+                                                 quads, quad_ok, err, 513, FIT_SMALL, FIT_SMALL, FIT_CHUNK_SMALL);
     cudaEventRecord(join2, side2);
-    const int mm = prm.max_nmaxima > 4 ? prm.max_nmaxima : 4;
-    const size_t wsm = fit_warp_smem(mm) * FIT_WPB;
-    cudaFuncSetAttribute(k_fit_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
-    int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
-    unsigned wblocks = (unsigned)(wb < 148 * 32 ? wb : 148 * 32);
-    k_fit_warp<<<wblocks, FIT_WPB * 32, wsm, s>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
-                                                  quads, quad_ok, mm);
+    launch_fit_warp<4>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 0, mm);
+    launch_fit_warp<8>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 129, mm);
     cudaStreamWaitEvent(s, join, 0);
     cudaStreamWaitEvent(s, join2, 0);
 }
