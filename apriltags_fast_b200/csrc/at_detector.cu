@@ -83,7 +83,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -461,16 +461,18 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_QUADS].ensure(ncl * sizeof(GpuQuad)));
         CK(B[B_QOK].ensure(ncl * 4));
         CK(B[B_QSCAN].ensure(ncl * 4));
+        CK(B[B_FLIST].ensure(ncl * 4 * 5));
+        CK(B[B_FCNT].ensure(64));
         FitScratch scr{B[B_SKEYS].as<uint64_t>(), B[B_SSKEY].as<uint64_t>(), B[B_SSVAL].as<uint32_t>(),
                        B[B_SW].as<double>(),      B[B_SFX].as<double>(),    B[B_SFY].as<double>(),
                        B[B_SMX].as<double>(),     B[B_SMY].as<double>(),    B[B_SMXX].as<double>(),
                        B[B_SMXY].as<double>(),    B[B_SMYY].as<double>(),   B[B_SMW].as<double>(),
                        B[B_SERRS].as<double>(),   B[B_SFILT].as<double>(),  B[B_SMXE].as<double>(),
-                       B[B_SMXI].as<int32_t>()};
+                       B[B_SMXI].as<int32_t>(),   B[B_FLIST].as<uint32_t>(), B[B_FCNT].as<uint32_t>()};
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
         launch_fit_quads(st, in->side, in->side2, in->fork, in->join, in->join2, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
-        in->launches += 2;
+        in->launches += 7;
         CK(cudaGetLastError());
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);

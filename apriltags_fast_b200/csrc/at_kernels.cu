@@ -895,6 +895,8 @@ __device__ long long g_fitprof[FIT_PROF_N][12];
     if (lane == 0 && c < FIT_PROF_N) g_fitprof[c][k] = clock64();
 #define FITW_SIZE(n)                                             \
     if (lane == 0 && c < FIT_PROF_N) g_fitprof[c][0] = (n);
+#define FITB_SIZE(n)                                             \
+    if (tid == 0 && c < FIT_PROF_N) g_fitprof[c][0] = (n);
 extern "C" int at_fit_prof_copy(void *dst, int n) {
     return (int)cudaMemcpyFromSymbol(dst, g_fitprof, (size_t)n * 12 * 8);
 }
@@ -902,6 +904,7 @@ extern "C" int at_fit_prof_copy(void *dst, int n) {
 #define FIT_PROF(k)
 #define FITW_PROF(k)
 #define FITW_SIZE(n)
+#define FITB_SIZE(n)
 #endif
 
 template <int NT>
@@ -909,7 +912,8 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
                                                    const uint64_t *pts, const uint32_t *cstart,
                                                    const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                    FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err,
-                                                   int64_t class_lo, int64_t class_hi, int sort_cap, int chunk) {
+                                                   const uint32_t *list, const uint32_t *count, uint32_t *next,
+                                                   int sort_cap, int chunk) {
     extern __shared__ __align__(16) unsigned char fit_smem[];
     uint64_t *s_key = reinterpret_cast<uint64_t *>(fit_smem);
     double *s_w = reinterpret_cast<double *>(fit_smem + (size_t)sort_cap * 8);
@@ -923,20 +927,26 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         s_pnx[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA], s_pny[AT_MAX_NMAXIMA * AT_MAX_NMAXIMA];
     __shared__ double s_be[NT / 32], s_lines[4][4], s_lmse[4], s_best;
     __shared__ int64_t s_bo[NT / 32];
+    __shared__ uint32_t s_next;
     const int tid = threadIdx.x;
+    const uint32_t ncl = *count;
 
-    for (int64_t c = blockIdx.x; c < nclusters; c += gridDim.x) {
+    // the class's clusters, largest first, each to the next free block
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_next = atomicAdd(next, 1u);
+        __syncthreads();
+        if (s_next >= ncl) break;
+        const int64_t c = list[s_next];
         const int64_t s0 = cstart[c];
         const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
-        if (sz < class_lo || sz > class_hi) continue;  // the other class's kernel
         const FrameDesc f = frames[cframe[c]];
-        if (tid == 0) quad_ok[c] = 0;
-        if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
         if (sz > 65535) {
             if (tid == 0) atomicOr(err, AT_ERR_CLUSTER_TOO_BIG);
             continue;
         }
         FIT_PROF(1)
+        FITB_SIZE(sz)
         const uint64_t *P = pts + s0;
         // bounding box (fast/quads.c:515-528)
         uint32_t xmin = 0xffff, xmax = 0, ymin = 0xffff, ymax = 0;
@@ -1374,6 +1384,79 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
 }
 
 // ---------------------------------------------------------------------------
+// The fit's size classes: clusters of at most 128, 256, 512 points (a warp
+// each), at most 1024 (a block of 128), and larger (a block of 512). Each
+// class gets a list of its clusters; clusters outside [min_cluster_pixels,
+// max_px] of their frame get none (fast/quads.c:1180-1190). Every cluster's
+// quad flag starts at 0.
+#define FIT_NCLASS 5
+__device__ __forceinline__ int fit_class(int64_t sz) {
+    return sz <= 128 ? 0 : sz <= 256 ? 1 : sz <= 512 ? 2 : sz <= 1024 ? 3 : 4;
+}
+
+__global__ void k_fit_classify(const FrameDesc *frames, const uint32_t *cstart, const int32_t *cframe,
+                               int64_t nclusters, int64_t npoints, int32_t min_px, uint32_t *quad_ok,
+                               uint32_t *lists, uint32_t *counts) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t c0 = (int64_t)blockIdx.x * blockDim.x; c0 < nclusters; c0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = c0 + threadIdx.x;
+        int k = -1;
+        if (c < nclusters) {
+            quad_ok[c] = 0;
+            const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - cstart[c];
+            if (sz >= min_px && sz <= frames[cframe[c]].max_px) k = fit_class(sz);
+        }
+#pragma unroll
+        for (int q = 0; q < FIT_NCLASS; q++) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, k == q);
+            if (!bal) continue;
+            uint32_t at = 0;
+            if (lane == __ffs(bal) - 1) at = atomicAdd(counts + q, (uint32_t)__popc(bal));
+            at = __shfl_sync(0xffffffffu, at, __ffs(bal) - 1);
+            if (k == q) lists[(int64_t)q * nclusters + at + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)c;
+        }
+    }
+}
+
+// One block per list: the list by size, largest first (then by cluster),
+// when it has at most FIT_ORDER_CAP clusters; a bitonic sort in shared
+// memory.
+#define FIT_ORDER_CAP 8192
+__global__ void __launch_bounds__(1024) k_fit_order(const uint32_t *cstart, int64_t nclusters, int64_t npoints,
+                                                   uint32_t *lists, const uint32_t *counts, int first_class) {
+    extern __shared__ __align__(16) uint64_t s_ord[];
+    const int q = first_class + blockIdx.x;
+    const uint32_t n = counts[q];
+    if (n < 2 || n > FIT_ORDER_CAP) return;
+    uint32_t *list = lists + (int64_t)q * nclusters;
+    uint32_t np = 2;
+    while (np < n) np <<= 1;
+    for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) {
+        uint64_t key = ~0ull;
+        if (i < n) {
+            const uint32_t c = list[i];
+            const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - cstart[c];
+            key = (uint64_t)(0xffffffffu - (uint32_t)sz) << 32 | c;
+        }
+        s_ord[i] = key;
+    }
+    __syncthreads();
+    for (uint32_t kk = 2; kk <= np; kk <<= 1)
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < np / 2; t += blockDim.x) {
+                const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1)), l = i + j;
+                const uint64_t a = s_ord[i], b = s_ord[l];
+                if (((i & kk) == 0) == (a > b)) {
+                    s_ord[i] = b;
+                    s_ord[l] = a;
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) list[i] = (uint32_t)s_ord[i];
+}
+
+// ---------------------------------------------------------------------------
 // Clusters of at most 32 * R points: one warp each, FIT_WPB per block, no
 // block barriers. The same steps as k_fit_quads; the angle sort is a bitonic
 // sort in registers, the prefix moments stay in shared memory.
@@ -1462,7 +1545,8 @@ template <int R>
 __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
                                                           const uint64_t *pts, const uint32_t *cstart,
                                                           const int32_t *cframe, int64_t nclusters, int64_t npoints,
-                                                          GpuQuad *quads, uint32_t *quad_ok, int64_t class_lo, int mm) {
+                                                          const uint32_t *list, const uint32_t *count,
+                                                          GpuQuad *quads, uint32_t *quad_ok, int mm) {
     constexpr int CAP = 32 * R;
     extern __shared__ __align__(16) unsigned char fw_smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1480,13 +1564,12 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
            *s_pny = s_pnx + mm * mm;
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
 
-    for (int64_t c = (int64_t)blockIdx.x * FIT_WPB + wid; c < nclusters; c += (int64_t)gridDim.x * FIT_WPB) {
+    const uint32_t ncl = *count;
+    for (uint32_t li = blockIdx.x * FIT_WPB + wid; li < ncl; li += gridDim.x * FIT_WPB) {
+        const int64_t c = list[li];
         const int64_t s0 = cstart[c];
         const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
-        if (sz < class_lo || sz > CAP) continue;  // another class's kernel
         const FrameDesc f = frames[cframe[c]];
-        if (lane == 0) quad_ok[c] = 0;
-        if (sz < prm.min_cluster_pixels || sz > f.max_px) continue;
         const int n = (int)sz;
         FITW_SIZE(n)
         FITW_PROF(1)
@@ -2577,14 +2660,15 @@ void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *
 template <int R>
 static void launch_fit_warp(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                             const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
-                            int64_t npoints, GpuQuad *quads, uint32_t *quad_ok, int64_t class_lo, int mm) {
+                            int64_t npoints, const FitScratch &scr, int q, GpuQuad *quads, uint32_t *quad_ok, int mm) {
     const size_t wsm = fit_warp_smem(32 * R, mm) * FIT_WPB;
     cudaFuncSetAttribute(k_fit_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
     const int64_t per_sm = (int64_t)(225 * 1024 / (wsm + 1024));
     const int64_t full = 148 * (per_sm < 1 ? 1 : per_sm > 32 ? 32 : per_sm);
     const int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
     k_fit_warp<R><<<(unsigned)(wb < full ? wb : full), FIT_WPB * 32, wsm, s>>>(
-        frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, class_lo, mm);
+        frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr.lists + (int64_t)q * nclusters,
+        scr.counts + q, quads, quad_ok, mm);
 }
 
 void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
@@ -2595,24 +2679,33 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
     const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL), large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
     cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
+    cudaFuncSetAttribute(k_fit_order, cudaFuncAttributeMaxDynamicSharedMemorySize, FIT_ORDER_CAP * 8);
     const int mm = prm.max_nmaxima > 4 ? prm.max_nmaxima : 4;
-    // size classes on three streams: the few large clusters (a block of 512
-    // each); the middle ones (a warp each up to 512 points, then a block of
-    // 128); the many small ones (a warp each)
+    // the size classes' lists, the two block classes' largest first
+    cudaMemsetAsync(scr.counts, 0, 2 * FIT_NCLASS * sizeof(uint32_t), s);
+    k_fit_classify<<<flat_blocks(nclusters, 256), 256, 0, s>>>(frames, cstart, cframe, nclusters, npoints,
+                                                                prm.min_cluster_pixels, quad_ok, scr.lists,
+                                                                scr.counts);
+    k_fit_order<<<2, 1024, FIT_ORDER_CAP * 8, s>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 3);
+    // three streams: the large clusters (a block of 512 each); the middle
+    // ones (a warp each up to 512 points, then a block of 128); the many
+    // small ones (a warp each)
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     cudaStreamWaitEvent(side2, fork, 0);
-    k_fit_quads<512><<<(unsigned)(nclusters < 148 * 2 ? nclusters : 148 * 2), 512, large, side>>>(
-        frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, quads, quad_ok, err, FIT_SMALL + 1,
-        INT64_MAX, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
+    const unsigned nbig = (unsigned)(nclusters < 148 ? nclusters : 148);
+    k_fit_quads<512><<<nbig, 512, large, side>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+                                                 quads, quad_ok, err, scr.lists + 4 * nclusters, scr.counts + 4,
+                                                 scr.counts + FIT_NCLASS + 4, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaEventRecord(join, side);
-    launch_fit_warp<16>(side2, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 257, mm);
-    unsigned mid = (unsigned)(nclusters < 148 * 16 ? nclusters : 148 * 16);
+    launch_fit_warp<16>(side2, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 2, quads, quad_ok, mm);
+    const unsigned mid = (unsigned)(nclusters < 148 * 4 ? nclusters : 148 * 4);
     k_fit_quads<128><<<mid, 128, small, side2>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
-                                                 quads, quad_ok, err, 513, FIT_SMALL, FIT_SMALL, FIT_CHUNK_SMALL);
+                                                 quads, quad_ok, err, scr.lists + 3 * nclusters, scr.counts + 3,
+                                                 scr.counts + FIT_NCLASS + 3, FIT_SMALL, FIT_CHUNK_SMALL);
     cudaEventRecord(join2, side2);
-    launch_fit_warp<4>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 0, mm);
-    launch_fit_warp<8>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, quads, quad_ok, 129, mm);
+    launch_fit_warp<4>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 0, quads, quad_ok, mm);
+    launch_fit_warp<8>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 1, quads, quad_ok, mm);
     cudaStreamWaitEvent(s, join, 0);
     cudaStreamWaitEvent(s, join2, 0);
 }

@@ -22,6 +22,8 @@ struct FitScratch {
     double *mx, *my, *mxx, *mxy, *myy, *mw;
     double *errs, *filt, *mxe;
     int32_t *mxi;
+    uint32_t *lists;   // one list of cluster ids per size class, nclusters apart
+    uint32_t *counts;  // per class: list length, then the next list index to take
 };
 
 struct BlurTaps {
