@@ -83,7 +83,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -525,10 +525,14 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         }
         CK(cudaMemcpyAsync(B[B_QSTART].p, hs, (n + 1) * 8, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(B[B_OUTOFF].p, hs + n + 1, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+        CK(B[B_QCORN].ensure(nq * 8 * sizeof(float)));
+        CK(B[B_QH].ensure(nq * 9 * sizeof(double)));
+        CK(B[B_QHOK].ensure(nq * sizeof(uint32_t)));
+        const DecodeScratch dscr{B[B_QCORN].as<float>(), B[B_QH].as<double>(), B[B_QHOK].as<uint32_t>()};
         launch_decode(st, dfr, prm, in->dfam.as<GpuFamily>(), B[B_IMG].as<uint8_t>(), qim, B[B_QUADSC].as<GpuQuad>(),
-                      nq, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
+                      nq, dscr, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
         CK(cudaEventRecord(in->ev[7], st));
-        in->launches += 2;
+        in->launches += 4;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
                         B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),

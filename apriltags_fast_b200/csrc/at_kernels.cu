@@ -897,6 +897,12 @@ __device__ long long g_fitprof[FIT_PROF_N][12];
     if (lane == 0 && c < FIT_PROF_N) g_fitprof[c][0] = (n);
 #define FITB_SIZE(n)                                             \
     if (tid == 0 && c < FIT_PROF_N) g_fitprof[c][0] = (n);
+__device__ long long g_decprof[8192][8];
+#define DEC_PROF(k)                                              \
+    if (tid == 0 && qi < 8192) g_decprof[qi][k] = clock64();
+extern "C" int at_dec_prof_copy(void *dst, int n) {
+    return (int)cudaMemcpyFromSymbol(dst, g_decprof, (size_t)n * 8 * 8);
+}
 extern "C" int at_fit_prof_copy(void *dst, int n) {
     return (int)cudaMemcpyFromSymbol(dst, g_fitprof, (size_t)n * 12 * 8);
 }
@@ -905,6 +911,7 @@ extern "C" int at_fit_prof_copy(void *dst, int n) {
 #define FITW_PROF(k)
 #define FITW_SIZE(n)
 #define FITB_SIZE(n)
+#define DEC_PROF(k)
 #endif
 
 template <int NT>
@@ -1931,34 +1938,65 @@ struct DView {
     int64_t s, w, h;
 };
 
-__device__ __forceinline__ double bil_pair(double a, double b, const uint8_t *p, int64_t s) {
-    double na = 1.0 - a, nb = 1.0 - b;
-    return ((na * nb) * p[0] + (a * nb) * p[1]) + ((na * b) * p[s] + (a * b) * p[s + 1]);
-}
 __device__ __forceinline__ double bil_seq(double a, double b, const uint8_t *p, int64_t s) {
     return (1.0 - a) * (1.0 - b) * p[0] + a * (1.0 - b) * p[1] + (1.0 - a) * b * p[s] + a * b * p[s + 1];
 }
 
 // One sample point of edge refinement (fast/decode.c:549-735): the
 // weighted mean step n0 along the normal, or false when no step counts.
+// The first vsteps steps (a multiple of 4) sum into 4 interleaved partial
+// sums. They go 4 at a time, each step's 8 pixels loaded before any is
+// used (a step outside the image loads pixel (0, 0) and counts 0), so the
+// loads of the 4 steps overlap; the rest of the steps follow in order.
+__device__ __forceinline__ double bil_vals(double a, double b, int p00, int p01, int p10, int p11) {
+    double na = 1.0 - a, nb = 1.0 - b;
+    return ((na * nb) * p00 + (a * nb) * p01) + ((na * b) * p10 + (a * b) * p11);
+}
+
 __device__ bool refine_sample(const DView &v, double x0, double y0, double nx, double ny, int64_t range,
                               int64_t vsteps, int64_t nsteps, double *n0) {
     const double wl = (double)(v.w - 1), hl = (double)(v.h - 1);
     double ln[4] = {0.0, 0.0, 0.0, 0.0}, lc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int64_t k = 0; k < vsteps; k++) {
-        double n = (double)-range + 0.25 * (double)k;
-        double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
-        double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
-        double wgt = 0.0;
-        if (x1 > -1.0 && x1 < wl && y1 > -1.0 && y1 < hl && x2 > -1.0 && x2 < wl && y2 > -1.0 && y2 < hl) {
-            double tx1 = trunc(x1), ty1 = trunc(y1), tx2 = trunc(x2), ty2 = trunc(y2);
-            double g1 = bil_pair(x1 - tx1, y1 - ty1, v.im + (int64_t)ty1 * v.s + (int64_t)tx1, v.s);
-            double g2 = bil_pair(x2 - tx2, y2 - ty2, v.im + (int64_t)ty2 * v.s + (int64_t)tx2, v.s);
-            double d = g2 - g1;
-            wgt = !(g1 < g2) ? d * d : 0.0;
+    const bool tiny = v.w < 2 || v.h < 2;
+    for (int64_t k0 = 0; k0 < vsteps; k0 += 4) {
+        bool in[4];
+        double fx1[4], fy1[4], fx2[4], fy2[4];
+        int px[4][8];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const double n = (double)-range + 0.25 * (double)(k0 + u);
+            const double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
+            const double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
+            in[u] = x1 > -1.0 && x1 < wl && y1 > -1.0 && y1 < hl && x2 > -1.0 && x2 < wl && y2 > -1.0 && y2 < hl;
+            const double tx1 = trunc(x1), ty1 = trunc(y1), tx2 = trunc(x2), ty2 = trunc(y2);
+            fx1[u] = x1 - tx1;
+            fy1[u] = y1 - ty1;
+            fx2[u] = x2 - tx2;
+            fy2[u] = y2 - ty2;
+            const bool safe = in[u] || !tiny;
+            const uint8_t *p1 = v.im + (in[u] ? (int64_t)ty1 * v.s + (int64_t)tx1 : 0);
+            const uint8_t *p2 = v.im + (in[u] ? (int64_t)ty2 * v.s + (int64_t)tx2 : 0);
+            if (safe) {
+                px[u][0] = p1[0], px[u][1] = p1[1], px[u][2] = p1[v.s], px[u][3] = p1[v.s + 1];
+                px[u][4] = p2[0], px[u][5] = p2[1], px[u][6] = p2[v.s], px[u][7] = p2[v.s + 1];
+            } else {
+#pragma unroll
+                for (int t = 0; t < 8; t++) px[u][t] = 0;
+            }
         }
-        ln[k & 3] = ln[k & 3] + wgt * n;
-        lc[k & 3] = lc[k & 3] + wgt;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const double n = (double)-range + 0.25 * (double)(k0 + u);
+            double wgt = 0.0;
+            if (in[u]) {
+                const double g1 = bil_vals(fx1[u], fy1[u], px[u][0], px[u][1], px[u][2], px[u][3]);
+                const double g2 = bil_vals(fx2[u], fy2[u], px[u][4], px[u][5], px[u][6], px[u][7]);
+                const double d = g2 - g1;
+                wgt = !(g1 < g2) ? d * d : 0.0;
+            }
+            ln[u] = ln[u] + wgt * n;
+            lc[u] = lc[u] + wgt;
+        }
     }
     double mn = 0.0 + ((ln[0] + ln[2]) + (ln[1] + ln[3]));
     double mc = 0.0 + ((lc[0] + lc[2]) + (lc[1] + lc[3]));
@@ -1988,56 +2026,97 @@ __device__ __forceinline__ float cr_atan2f(float y, float x) { return (float)ata
 __device__ __forceinline__ float cr_cosf(float x) { return (float)cos((double)x); }
 __device__ __forceinline__ float cr_sinf(float x) { return (float)sin((double)x); }
 
-// Homography of 4 correspondences: 8x9 Gaussian elimination with partial
-// pivoting (fast/decode.c:114-165).
-__device__ bool homography(const double c[4][4], double H[9]) {
-    double a[8][9];
-    for (int r = 0; r < 8; r++)
-        for (int i = 0; i < 9; i++) a[r][i] = 0.0;
-    for (int i = 0; i < 4; i++) {
-        double x = c[i][0], y = c[i][1], X = c[i][2], Y = c[i][3];
-        a[2 * i][0] = x;
-        a[2 * i][1] = y;
-        a[2 * i][2] = 1.0;
-        a[2 * i][6] = -x * X;
-        a[2 * i][7] = -y * X;
-        a[2 * i][8] = X;
-        a[2 * i + 1][3] = x;
-        a[2 * i + 1][4] = y;
-        a[2 * i + 1][5] = 1.0;
-        a[2 * i + 1][6] = -x * Y;
-        a[2 * i + 1][7] = -y * Y;
-        a[2 * i + 1][8] = Y;
-    }
-    for (int col = 0; col < 8; col++) {
-        double best = 0.0;
-        int piv = -1;
-        for (int r = col; r < 8; r++)
-            if (fabs(a[r][col]) > best) {
-                best = fabs(a[r][col]);
-                piv = r;
+// Homography of 4 correspondences by one warp: the 8x9 Gaussian elimination
+// with partial pivoting of fast/decode.c:114-165. Lane l holds row l / 4,
+// columns l % 4 and l % 4 + 4 (and column 8 when l % 4 == 0). Each cell
+// takes the same operations as in the sequential elimination, so the result
+// is the same; the pivot is the first largest |a[r][col]|, r >= col, as the
+// scan for a strictly larger value finds it. The back substitution runs on
+// lane 0 from shared memory (m: 72 doubles). Returns false on a failed pivot
+// check, on every lane. The loops stay rolled: this runs once per quad, so
+// its code size is its cost.
+__device__ __noinline__ bool homography_warp(const float (*p)[2], double *m, double H[9], int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const int r = lane >> 2, g = lane & 3;
+    double cell[3];
+    {
+        const int i = r >> 1;
+        const double x = i == 0 || i == 3 ? -1.0 : 1.0, y = i == 0 || i == 1 ? -1.0 : 1.0;
+        const double X = (double)p[i][0], Y = (double)p[i][1];
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) {
+            const int col = sl == 2 ? 8 : g + 4 * sl;
+            double v = 0.0;
+            if ((r & 1) == 0) {
+                v = col == 0 ? x : col == 1 ? y : col == 2 ? 1.0 : col == 6 ? -x * X : col == 7 ? -y * X : col == 8 ? X : 0.0;
+            } else {
+                v = col == 3 ? x : col == 4 ? y : col == 5 ? 1.0 : col == 6 ? -x * Y : col == 7 ? -y * Y : col == 8 ? Y : 0.0;
             }
-        if (piv < 0 || best < 1e-10) return false;
-        if (piv != col)
-            for (int i = col; i < 9; i++) {
-                double t = a[col][i];
-                a[col][i] = a[piv][i];
-                a[piv][i] = t;
-            }
-        for (int r = col + 1; r < 8; r++) {
-            double fct = a[r][col] / a[col][col];
-            a[r][col] = 0.0;
-            for (int i = col + 1; i < 9; i++) a[r][i] = a[r][i] - fct * a[col][i];
+            cell[sl] = v;
         }
     }
-    for (int col = 7; col >= 0; col--) {
-        double s = 0.0;
-        for (int i = col + 1; i < 8; i++) s = s + a[col][i] * a[i][8];
-        a[col][8] = (a[col][8] - s) / a[col][col];
+    bool ok = true;
+#pragma unroll 1
+    for (int col = 0; col < 8; col++) {
+        const int cg = col & 3, cs = col >> 2;
+        // pivot: the largest |a[r][col]| over r >= col, first r on ties
+        double v = -1.0;
+        if (g == cg && r >= col) {
+            const double a = fabs(cs ? cell[1] : cell[0]);
+            if (a == a) v = a;
+        }
+        int pr = r;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_xor_sync(FULL, v, o);
+            const int r2 = __shfl_xor_sync(FULL, pr, o);
+            if (v2 > v || (v2 == v && r2 < pr)) {
+                v = v2;
+                pr = r2;
+            }
+        }
+        if (!(v > 0.0) || v < 1e-10) ok = false;
+        const int piv = v > 0.0 ? pr : col;
+        // swap rows col and piv (their columns left of col are zero in both)
+        const int src = r == col ? 4 * piv + g : r == piv ? 4 * col + g : lane;
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) cell[sl] = __shfl_sync(FULL, cell[sl], src);
+        // eliminate below the pivot
+        const double pv = __shfl_sync(FULL, cs ? cell[1] : cell[0], 4 * col + cg);
+        const double mine = cs ? cell[1] : cell[0];
+        const double fct = __shfl_sync(FULL, mine / pv, 4 * r + cg);
+        double prow[3];
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) prow[sl] = __shfl_sync(FULL, cell[sl], 4 * col + g);
+        if (r > col) {
+#pragma unroll
+            for (int sl = 0; sl < 3; sl++) {
+                const int cc = sl == 2 ? 8 : g + 4 * sl;
+                if (sl == 2 && g != 0) continue;
+                if (cc == col)
+                    cell[sl] = 0.0;
+                else if (cc > col)
+                    cell[sl] = cell[sl] - fct * prow[sl];
+            }
+        }
     }
-    for (int i = 0; i < 8; i++) H[i] = a[i][8];
+    m[r * 9 + g] = cell[0];
+    m[r * 9 + g + 4] = cell[1];
+    if (g == 0) m[r * 9 + 8] = cell[2];
+    __syncwarp();
+    if (ok && lane == 0) {
+#pragma unroll 1
+        for (int col = 7; col >= 0; col--) {
+            double s = 0.0;
+#pragma unroll 1
+            for (int i = col + 1; i < 8; i++) s = s + m[col * 9 + i] * m[i * 9 + 8];
+            m[col * 9 + 8] = (m[col * 9 + 8] - s) / m[col * 9 + col];
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; i++) H[i] = m[i * 9 + 8];
     H[8] = 1.0;
-    return true;
+    return ok;
 }
 
 // Invertibility as the C library's PLU decomposition decides it
@@ -2084,7 +2163,7 @@ struct GrayModel {
 };
 
 // mat33_sym_solve as the C library does it (fast/decode.c:241-265).
-__device__ void gm_solve(GrayModel *g) {
+__device__ __forceinline__ void gm_solve(GrayModel *g) {
     const double *a = g->a;
     double L0 = sqrt(a[0]);
     double L3 = a[1] / L0;
@@ -2129,45 +2208,46 @@ __device__ __forceinline__ uint64_t rot90(uint64_t w0, int64_t nbits) {
 
 // The first code within maxham bits, by rotation, then chunk, then code
 // index (fast/decode.c:87-107). Returns id | hamming << 16 | rot << 24.
-__device__ uint32_t qd_lookup(const GpuFamily &F, uint64_t rcode) {
-    uint64_t mask = (uint64_t)F.cap - 1;
-    for (int r = 0; r < 4; r++) {
-        for (int j = 0; j < 4; j++) {
-            int64_t val = (int64_t)((rcode >> (j * F.chunk)) & mask);
-            int64_t ob = j * (F.cap + 1) + val;
-            int64_t base = j * F.ncodes;
-            for (int64_t e = base + F.off[ob]; e < base + F.off[ob + 1]; e++) {
-                int hd = __popcll(F.codes[e] ^ rcode);
-                if (hd <= F.maxham) return (uint32_t)F.idx[e] | (uint32_t)hd << 16 | (uint32_t)r << 24;
+__device__ uint32_t qd_lookup(const GpuFamily &F, uint64_t rcode, int lane) {
+    // lane 4 r + j (r rotations, chunk j) scans its bucket; the first lane
+    // with a match holds the first match in the sequential order
+    const uint64_t mask = (uint64_t)F.cap - 1;
+    uint32_t res = 0xffffffffu;
+    if (lane < 16) {
+        const int r = lane >> 2, j = lane & 3;
+        uint64_t rc = rcode;
+        for (int t = 0; t < r; t++) rc = rot90(rc, F.nbits);
+        const int64_t val = (int64_t)((rc >> (j * F.chunk)) & mask);
+        const int64_t ob = j * (F.cap + 1) + val, base = j * F.ncodes;
+        for (int64_t e = base + F.off[ob]; e < base + F.off[ob + 1]; e++) {
+            const int hd = __popcll(F.codes[e] ^ rc);
+            if (hd <= F.maxham) {
+                res = (uint32_t)F.idx[e] | (uint32_t)hd << 16 | (uint32_t)r << 24;
+                break;
             }
         }
-        rcode = rot90(rcode, F.nbits);
     }
-    return 65535u | 255u << 16;
+    const uint32_t found = __ballot_sync(0xffffffffu, res != 0xffffffffu);
+    if (!found) return 65535u | 255u << 16;
+    return __shfl_sync(0xffffffffu, res, __ffs(found) - 1);
 }
 
 #define REF_CHUNK 128
 
-__global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *frames, GpuParams prm,
-                                                              const GpuFamily *fams, const uint8_t *img,
-                                                              const uint8_t *qim, const GpuQuad *quads,
-                                                              int64_t nquads, GpuDetection *dets, uint32_t *det_ok) {
+__global__ void __launch_bounds__(AT_DEC_THREADS) k_refine(const FrameDesc *frames, GpuParams prm,
+                                                              const uint8_t *img, const uint8_t *qim,
+                                                              const GpuQuad *quads, int64_t nquads, float *corners,
+                                                              uint32_t *det_ok) {
     __shared__ float s_p[4][2];
     __shared__ double s_lines[4][4];
-    __shared__ double s_bx[4][REF_CHUNK], s_by[4][REF_CHUNK];
-    __shared__ int s_bok[4][REF_CHUNK];
+    __shared__ double s_bx[REF_CHUNK], s_by[REF_CHUNK];
+    __shared__ int s_bok[REF_CHUNK];
     __shared__ double s_enx[4], s_eny[4];
     __shared__ int64_t s_ens[4];
-    __shared__ double s_H[9];
-    __shared__ int s_hok;
-    __shared__ double s_gx[8 * AT_MAX_TW], s_gy[8 * AT_MAX_TW], s_gv[8 * AT_MAX_TW];
-    __shared__ int s_gk[8 * AT_MAX_TW];
-    __shared__ double s_wc[3], s_bc[3];
-    __shared__ int s_pol;
-    __shared__ double s_vals[AT_MAX_TW * AT_MAX_TW], s_sharp[AT_MAX_TW * AT_MAX_TW];
     const int tid = threadIdx.x;
     for (int64_t qi = blockIdx.x; qi < nquads; qi += gridDim.x) {
         const GpuQuad q = quads[qi];
+        DEC_PROF(0)
         const FrameDesc f = frames[q.frame];
         DView v;
         if (prm.decode_blurred)
@@ -2183,8 +2263,8 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
         __syncthreads();
         if (prm.refine_edges) {
             // fast/decode.c:657-761. The 4 edges are independent until the
-            // corners are moved: their sample points are refined together,
-            // and thread e < 4 sums edge e's samples in order.
+            // corners are moved: their sample points, one per thread, are
+            // refined together, and thread e < 4 sums edge e's in order.
             const int64_t range = (int64_t)__fadd_rn(prm.quad_decimate, 1.0f);
             const int64_t nsteps = 2 * 4 * range + 1;
             const int64_t vsteps = nsteps - nsteps % 4;
@@ -2204,13 +2284,15 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 s_ens[tid] = dmax(16, c_int(mag / 8.0));
             }
             __syncthreads();
-            const int64_t maxns = dmax(dmax(s_ens[0], s_ens[1]), dmax(s_ens[2], s_ens[3]));
+            // the 4 edges' samples in one packed range, edge after edge
+            const int64_t o1 = s_ens[0], o2 = o1 + s_ens[1], o3 = o2 + s_ens[2], total = o3 + s_ens[3];
             double mx = 0.0, my = 0.0, mxx = 0.0, mxy = 0.0, myy = 0.0, cnt = 0.0;
-            for (int64_t s0 = 0; s0 < maxns; s0 += REF_CHUNK) {
-                for (int w = tid; w < 4 * REF_CHUNK; w += blockDim.x) {
-                    const int e = w / REF_CHUNK, t = w - e * REF_CHUNK;
-                    const int64_t si = s0 + t, ns = s_ens[e];
-                    if (si >= ns) continue;
+            for (int64_t c0 = 0; c0 < total; c0 += REF_CHUNK) {
+                for (int w = tid; w < REF_CHUNK; w += blockDim.x) {
+                    const int64_t gi = c0 + w;
+                    if (gi >= total) continue;
+                    const int e = gi < o1 ? 0 : gi < o2 ? 1 : gi < o3 ? 2 : 3;
+                    const int64_t si = gi - (e == 0 ? 0 : e == 1 ? o1 : e == 2 ? o2 : o3), ns = s_ens[e];
                     const int a = e, b = (e + 1) & 3;
                     const double nx = s_enx[e], ny = s_eny[e];
                     double alpha = (1.0 + (double)si) / (double)(ns + 1);
@@ -2218,18 +2300,20 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                     double y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
                     double n0;
                     bool ok = refine_sample(v, x0, y0, nx, ny, range, vsteps, nsteps, &n0);
-                    s_bok[e][t] = ok;
+                    s_bok[w] = ok;
                     if (ok) {
-                        s_bx[e][t] = x0 + n0 * nx;
-                        s_by[e][t] = y0 + n0 * ny;
+                        s_bx[w] = x0 + n0 * nx;
+                        s_by[w] = y0 + n0 * ny;
                     }
                 }
                 __syncthreads();
                 if (tid < 4) {
-                    const int64_t m = dmin((int64_t)REF_CHUNK, s_ens[tid] - s0);
-                    for (int64_t t = 0; t < m; t++) {
-                        if (!s_bok[tid][t]) continue;
-                        double bx = s_bx[tid][t], by = s_by[tid][t];
+                    const int64_t eo = tid == 0 ? 0 : tid == 1 ? o1 : tid == 2 ? o2 : o3, ee = eo + s_ens[tid];
+                    const int64_t lo = dmax(eo, c0), hi = dmin(ee, c0 + REF_CHUNK);
+                    for (int64_t gi = lo; gi < hi; gi++) {
+                        const int64_t t = gi - c0;
+                        if (!s_bok[t]) continue;
+                        double bx = s_bx[t], by = s_by[t];
                         mx = mx + bx;
                         my = my + by;
                         mxx = mxx + bx * bx;
@@ -2240,6 +2324,7 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 }
                 __syncthreads();
             }
+            DEC_PROF(1)
             if (tid < 4) {
                 double ex = mx / cnt, ey = my / cnt;
                 double cxx = mxx / cnt - ex * ex, cxy = mxy / cnt - ex * ey, cyy = myy / cnt - ey * ey;
@@ -2265,21 +2350,60 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 }
             }
             __syncthreads();
+            DEC_PROF(2)
         }
-        if (tid == 0) {
-            double corr[4][4];
-            for (int i = 0; i < 4; i++) {
-                corr[i][0] = i == 0 || i == 3 ? -1.0 : 1.0;
-                corr[i][1] = i == 0 || i == 1 ? -1.0 : 1.0;
-                corr[i][2] = s_p[i][0];
-                corr[i][3] = s_p[i][1];
-            }
-            double H[9];
-            s_hok = homography(corr, H) && invertible3(H);
-            for (int i = 0; i < 9; i++) s_H[i] = H[i];
-        }
+        if (tid < 8) corners[qi * 8 + tid] = s_p[tid >> 1][tid & 1];
         __syncthreads();
-        if (!s_hok) continue;
+    }
+}
+
+// The homography of each quad's corners (fast/decode.c:114-196), a warp
+// per quad: H, and whether it was found and is invertible.
+#define QH_WARPS 4
+__global__ void __launch_bounds__(QH_WARPS * 32) k_quad_homography(const float *corners, int64_t nquads, double *hs,
+                                                                     uint32_t *hok) {
+    __shared__ float s_p[QH_WARPS][4][2];
+    __shared__ double s_hm[QH_WARPS][72];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t qi = (int64_t)blockIdx.x * QH_WARPS + w; qi < nquads; qi += (int64_t)gridDim.x * QH_WARPS) {
+        if (lane < 8) s_p[w][lane >> 1][lane & 1] = corners[qi * 8 + lane];
+        __syncwarp();
+        double H[9];
+        const bool ok = homography_warp(s_p[w], s_hm[w], H, lane);
+        if (lane == 0) {
+            hok[qi] = ok && invertible3(H);
+#pragma unroll
+            for (int i = 0; i < 9; i++) hs[qi * 9 + i] = H[i];
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *frames, GpuParams prm,
+                                                              const GpuFamily *fams, const uint8_t *img,
+                                                              const uint8_t *qim, const GpuQuad *quads,
+                                                              int64_t nquads, const double *hs, const uint32_t *hok,
+                                                              GpuDetection *dets, uint32_t *det_ok) {
+    __shared__ double s_H[9];
+    __shared__ double s_gx[8 * AT_MAX_TW], s_gy[8 * AT_MAX_TW], s_gv[8 * AT_MAX_TW];
+    __shared__ int s_gk[8 * AT_MAX_TW];
+    __shared__ double s_wc[3], s_bc[3];
+    __shared__ int s_pol;
+    __shared__ double s_vals[AT_MAX_TW * AT_MAX_TW], s_sharp[AT_MAX_TW * AT_MAX_TW];
+    const int tid = threadIdx.x;
+    for (int64_t qi = blockIdx.x; qi < nquads; qi += gridDim.x) {
+        if (!hok[qi]) continue;
+        const GpuQuad q = quads[qi];
+        const FrameDesc f = frames[q.frame];
+        DView v;
+        if (prm.decode_blurred)
+            v = DView{qim + f.q_off, (int64_t)f.qw, (int64_t)f.qw, (int64_t)f.qh};
+        else
+            v = DView{img + f.img_off, (int64_t)f.w, (int64_t)f.w, (int64_t)f.h};
+        __syncthreads();
+        if (tid < 9) s_H[tid] = hs[qi * 9 + tid];
+        __syncthreads();
+        DEC_PROF(3)
         for (int fi = 0; fi < prm.nfam; fi++) {
             const GpuFamily &F = fams[fi];
             if (F.reversed_border != q.reversed_border) continue;
@@ -2314,45 +2438,47 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 s_gv[t] = keep ? (double)v.im[iy * v.s + ix] : 0.0;
             }
             __syncthreads();
-            if (tid == 0) {
-                GrayModel gm[2];
-                for (int g = 0; g < 2; g++) {
-                    for (int i = 0; i < 9; i++) gm[g].a[i] = 0.0;
-                    for (int i = 0; i < 3; i++) gm[g].b[i] = 0.0;
+            if (tid < 32) {
+                // lane 0 the white model (even patterns), lane 1 the black one
+                // (odd patterns), each summed in pattern order in registers
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a4 = 0.0, a5 = 0.0, a8 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+                if (tid < 2) {
+                    for (int pi = tid; pi < 8; pi += 2)
+                        for (int i = 0; i < wab; i++) {
+                            const int t = pi * wab + i;
+                            if (!s_gk[t]) continue;
+                            const double x = s_gx[t], y = s_gy[t], val = s_gv[t];
+                            a0 = a0 + x * x;
+                            a1 = a1 + x * y;
+                            a2 = a2 + x;
+                            a4 = a4 + y * y;
+                            a5 = a5 + y;
+                            a8 = a8 + 1.0;
+                            b0 = b0 + x * val;
+                            b1 = b1 + y * val;
+                            b2 = b2 + val;
+                        }
                 }
-                for (int t = 0; t < 8 * wab; t++) {
-                    if (!s_gk[t]) continue;
-                    int pi = t / wab;
-                    GrayModel *g = &gm[(pi & 1) ? 1 : 0];  // even patterns white
-                    double x = s_gx[t], y = s_gy[t], val = s_gv[t];
-                    g->a[0] = g->a[0] + x * x;
-                    g->a[1] = g->a[1] + x * y;
-                    g->a[2] = g->a[2] + x;
-                    g->a[4] = g->a[4] + y * y;
-                    g->a[5] = g->a[5] + y;
-                    g->a[8] = g->a[8] + 1.0;
-                    g->b[0] = g->b[0] + x * val;
-                    g->b[1] = g->b[1] + y * val;
-                    g->b[2] = g->b[2] + val;
-                }
-                gm_solve(&gm[0]);
-                if (wab > 1) {
-                    gm_solve(&gm[1]);
+                GrayModel gm;
+                gm.a[0] = a0, gm.a[1] = a1, gm.a[2] = a2, gm.a[4] = a4, gm.a[5] = a5, gm.a[8] = a8;
+                gm.a[3] = gm.a[6] = gm.a[7] = 0.0;
+                gm.b[0] = b0, gm.b[1] = b1, gm.b[2] = b2;
+                if (tid == 0 || (tid == 1 && wab > 1)) {
+                    gm_solve(&gm);
                 } else {
-                    gm[1].c[0] = 0.0;
-                    gm[1].c[1] = 0.0;
-                    gm[1].c[2] = gm[1].b[2] / 4.0;
+                    gm.c[0] = 0.0;
+                    gm.c[1] = 0.0;
+                    gm.c[2] = gm.b[2] / 4.0;
                 }
-                double wi = gm[0].c[0] * 0.0 + gm[0].c[1] * 0.0 + gm[0].c[2];
-                double bi = gm[1].c[0] * 0.0 + gm[1].c[1] * 0.0 + gm[1].c[2];
-                s_pol = (wi - bi < 0.0) == (F.reversed_border != 0);
-                for (int i = 0; i < 3; i++) {
-                    s_wc[i] = gm[0].c[i];
-                    s_bc[i] = gm[1].c[i];
-                }
+                const double ci = gm.c[0] * 0.0 + gm.c[1] * 0.0 + gm.c[2];
+                const double bi = __shfl_sync(0xffffffffu, ci, 1);
+                if (tid == 0) s_pol = (ci - bi < 0.0) == (F.reversed_border != 0);
+                if (tid < 2)
+                    for (int i = 0; i < 3; i++) (tid == 0 ? s_wc : s_bc)[i] = gm.c[i];
             }
             __syncthreads();
             if (!s_pol) continue;
+            DEC_PROF(4)
             // bit values less the local threshold, sharpened (decode.c:340-377)
             const int64_t tw = F.tw;
             const int64_t minc = (wab - tw) / 2;
@@ -2381,9 +2507,11 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 s_sharp[t] = acc;
             }
             __syncthreads();
-            if (tid == 0) {
+            DEC_PROF(5)
+            if (tid < 32) {
                 float bs = 0.0f, ws = 0.0f, bc = 1.0f, wc = 1.0f;
                 uint64_t rcode = 0;
+                if (tid == 0) {
                 for (int64_t i = 0; i < F.nbits; i++) {
                     rcode <<= 1;
                     int64_t cell = (F.bit_y[i] - minc) * tw + (F.bit_x[i] - minc);
@@ -2397,12 +2525,15 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                         bc = __fadd_rn(bc, 1.0f);
                     }
                 }
+                }
+                rcode = (uint64_t)__shfl_sync(0xffffffffu, (uint32_t)(rcode >> 32), 0) << 32 |
+                        __shfl_sync(0xffffffffu, (uint32_t)rcode, 0);
+                const uint32_t lk = qd_lookup(F, rcode, tid);
                 double x = (double)__fdiv_rn(ws, wc), y = (double)__fdiv_rn(bs, bc);
                 double m = x != x ? y : y != y ? x : x < y ? x : y;  // fmin
                 float margin = (float)m;
-                uint32_t lk = qd_lookup(F, rcode);
                 int64_t id = lk & 0xffff, ham = (lk >> 16) & 0xff, rot = lk >> 24;
-                if (margin >= 0.0f && ham < 255) {
+                if (tid == 0 && margin >= 0.0f && ham < 255) {
                     // H = qH * R(rot * pi/2) (fast/detector.c:83-107)
                     double c = prm.rot_cs[rot][0], s = prm.rot_cs[rot][1];
                     const double r[9] = {c, -s, 0.0, s, c, 0.0, 0.0, 0.0, 1.0};
@@ -2428,6 +2559,7 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
                 }
             }
             __syncthreads();
+            DEC_PROF(6)
         }
         __syncthreads();
     }
@@ -2717,11 +2849,16 @@ void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *o
 }
 
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
-                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads, GpuDetection *dets,
-                   uint32_t *det_ok) {
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads,
+                   const DecodeScratch &scr, GpuDetection *dets, uint32_t *det_ok) {
     if (nquads <= 0) return;
-    unsigned blocks = (unsigned)(nquads < 148 * 64 ? nquads : 148 * 64);
-    k_decode<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, fams, img, qim, quads, nquads, dets, det_ok);
+    const unsigned blocks = (unsigned)(nquads < 148 * 64 ? nquads : 148 * 64);
+    k_refine<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, img, qim, quads, nquads, scr.corners, det_ok);
+    const int64_t hb = (nquads + QH_WARPS - 1) / QH_WARPS;
+    k_quad_homography<<<(unsigned)(hb < 148 * 16 ? hb : 148 * 16), QH_WARPS * 32, 0, s>>>(scr.corners, nquads,
+                                                                                        scr.h, scr.hok);
+    k_decode<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, fams, img, qim, quads, nquads, scr.h, scr.hok, dets,
+                                               det_ok);
 }
 
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,

@@ -59,9 +59,16 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
                          GpuQuad *out);
+// per quad: refined corners (8 floats), homography (9 doubles), and whether
+// the homography was found and is invertible
+struct DecodeScratch {
+    float *corners;
+    double *h;
+    uint32_t *hok;
+};
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
-                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads, GpuDetection *dets,
-                   uint32_t *det_ok);
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads,
+                   const DecodeScratch &scr, GpuDetection *dets, uint32_t *det_ok);
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
                      const int64_t *out_off, int64_t *out_n);
