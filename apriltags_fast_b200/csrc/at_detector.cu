@@ -298,6 +298,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
 
     // frame layout
     std::vector<FrameDesc> fd(n);
+    std::vector<char> copied(n, 0);  // frames copied into the input arena
     int64_t img = 0, qpx = 0, nodes = 0, rows = 0, tiles = 0;
     uint32_t all = in->nfam >= 32 ? 0xffffffffu : ((1u << in->nfam) - 1u);
     for (int64_t i = 0; i < n; i++) {
@@ -312,14 +313,32 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         f.h = live ? (int32_t)fr.height : 0;
         f.qw = live ? (int32_t)qw : 0;
         f.qh = live ? (int32_t)qh : 0;
-        f.img_off = img;
+        // frames already in this device's memory are read in place; the
+        // others are copied into the input arena (packed, stride w)
+        f.img = nullptr;
+        f.stride = f.w;
+        if (live) {
+            cudaPointerAttributes pa;
+            int dev = -1;
+            cudaGetDevice(&dev);
+            if (cudaPointerGetAttributes(&pa, fr.pixels) == cudaSuccess &&
+                (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged) && pa.device == dev &&
+                pa.devicePointer != nullptr) {
+                f.img = static_cast<const uint8_t *>(pa.devicePointer);
+                f.stride = fr.stride;
+            } else {
+                cudaGetLastError();  // clear the error an unregistered host pointer leaves
+                f.img = reinterpret_cast<const uint8_t *>((uintptr_t)img);  // an offset until the arena exists
+                img += (int64_t)f.w * f.h;
+                copied[i] = 1;
+            }
+        }
         f.q_off = qpx;
         f.node_off = nodes;
         f.row0 = rows;
         f.tile_off = tiles;
         f.fam_mask = fr.family_mask ? (fr.family_mask & all) : all;
         f.max_px = (int32_t)(2 * (2 * f.qw + 2 * f.qh));
-        img += (int64_t)f.w * f.h;
         qpx += (int64_t)f.qw * f.qh;
         nodes += (int64_t)f.qw * f.qh + f.qh;
         rows += f.qh;
@@ -345,7 +364,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     // arenas
     DBuf *B = in->buf;
     CK(B[B_FRAMES].ensure(n * sizeof(FrameDesc)));
-    CK(B[B_IMG].ensure(img));
+    CK(B[B_IMG].ensure(img + 1));
     CK(B[B_QIM].ensure(qpx));
     CK(B[B_THR].ensure(qpx));
     CK(B[B_TMPA].ensure(qpx));
@@ -362,6 +381,9 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(B[B_ROWPTS].ensure((rows + 1) * 8));
     CK(B[B_ROWOFF].ensure((rows + 1) * 8));
     CK(B[B_ERR].ensure(4));
+    // copied frames: their offsets into the arena become pointers
+    for (int64_t i = 0; i < n; i++)
+        if (copied[i]) fd[i].img = B[B_IMG].as<uint8_t>() + (uintptr_t)fd[i].img;
     CK(in->h_frames.ensure(n * sizeof(FrameDesc)));
     memcpy(in->h_frames.p, fd.data(), n * sizeof(FrameDesc));
     const FrameDesc *dfr = B[B_FRAMES].as<FrameDesc>();
@@ -371,9 +393,9 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(cudaMemcpyAsync(B[B_FRAMES].p, in->h_frames.p, n * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(B[B_ERR].p, 0, 4, st));
     for (int64_t i = 0; i < n; i++) {
-        if (fd[i].qw == 0) continue;
-        CK(cudaMemcpy2DAsync(B[B_IMG].as<uint8_t>() + fd[i].img_off, fd[i].w, frames[i].pixels, frames[i].stride,
-                             fd[i].w, fd[i].h, cudaMemcpyDefault, st));
+        if (!copied[i]) continue;
+        CK(cudaMemcpy2DAsync(const_cast<uint8_t *>(fd[i].img), fd[i].w, frames[i].pixels, frames[i].stride, fd[i].w,
+                             fd[i].h, cudaMemcpyDefault, st));
     }
     uint8_t *qim = B[B_QIM].as<uint8_t>(), *thr = B[B_THR].as<uint8_t>();
     launch_decimate(L, dfr, B[B_IMG].as<uint8_t>(), qim, td->quad_decimate);

@@ -23,9 +23,10 @@
 #define AT_ERR_CAPACITY 2u
 
 struct FrameDesc {
-    int32_t w, h;          // input frame (device copy is packed: stride w)
+    int32_t w, h;          // input frame
     int32_t qw, qh;        // quad image
-    int64_t img_off;       // into the input image arena
+    const uint8_t *img;    // input pixels in device memory: the caller's, or a copy in the arena
+    int64_t stride;        // bytes between rows of img
     int64_t q_off;         // into the quad-pixel arenas
     int64_t node_off;      // first union-find node id of the frame
     int64_t row0;          // global index of quad row 0

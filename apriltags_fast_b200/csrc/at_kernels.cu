@@ -64,8 +64,8 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total,
 
 __global__ void k_decimate(const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor) {
     const FrameDesc f = frames[blockIdx.y];
-    const uint8_t *src = img + f.img_off;
-    const int64_t stride = f.w;
+    const uint8_t *src = f.img;
+    const int64_t stride = f.stride;
     const int qw = (int)f.qw, qh = (int)f.qh;
     for (int y = blockIdx.x; y < qh; y += gridDim.x) {
         uint8_t *out = qim + f.q_off + (int64_t)y * qw;
@@ -2253,7 +2253,7 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_refine(const FrameDesc *fram
         if (prm.decode_blurred)
             v = DView{qim + f.q_off, (int64_t)f.qw, (int64_t)f.qw, (int64_t)f.qh};
         else
-            v = DView{img + f.img_off, (int64_t)f.w, (int64_t)f.w, (int64_t)f.h};
+            v = DView{f.img, f.stride, (int64_t)f.w, (int64_t)f.h};
         if (tid < 8) {
             float val = q.p[tid >> 1][tid & 1];
             if (prm.quad_decimate > 1.0f) val = __fmul_rn(val, prm.quad_decimate);
@@ -2399,7 +2399,7 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *fram
         if (prm.decode_blurred)
             v = DView{qim + f.q_off, (int64_t)f.qw, (int64_t)f.qw, (int64_t)f.qh};
         else
-            v = DView{img + f.img_off, (int64_t)f.w, (int64_t)f.w, (int64_t)f.h};
+            v = DView{f.img, f.stride, (int64_t)f.w, (int64_t)f.h};
         __syncthreads();
         if (tid < 9) s_H[tid] = hs[qi * 9 + tid];
         __syncthreads();
