@@ -83,7 +83,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -448,30 +448,85 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_HSCAN].ensure(npts * 4));
         launch_point_emit(L, dfr, thr, lab, row_off, B[B_KEY].as<uint64_t>(), B[B_VAL].as<uint64_t>(), nb);
         in->launches += 1;
-        if (!cub_call(in, [&](void *t, size_t &b) {
-                return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
-                                                       B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
-                                                       (int64_t)npts, 0, 2 * nb, st);
-            }))
-            return false;
-        const uint64_t *skey = B[B_KEY2].as<uint64_t>(), *spts = B[B_VAL2].as<uint64_t>();
-        uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
-        launch_cluster_heads(st, skey, npts, head);
-        in->launches += 1;
-        if (!cub_call(in, [&](void *t, size_t &b) {
-                return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
-            }))
-            return false;
-        uint32_t last[2];
-        CK(cudaMemcpyAsync(&last[0], hscan + npts - 1, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&last[1], head + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+        const uint64_t *spts = B[B_VAL2].as<uint64_t>();
+        // group by hashing the label pairs (the full sort if the table overflows)
+        uint32_t hsize = 1u << 16;
+        while (hsize < (uint64_t)npts / 16 && hsize < (1u << 30)) hsize <<= 1;
+        CK(B[B_HKEYS].ensure((size_t)hsize * 8));
+        CK(B[B_HCOUNT].ensure((size_t)hsize * 4));
+        CK(B[B_HRANK].ensure((size_t)hsize * 4));
+        CK(B[B_HMISC].ensure(16));
+        uint64_t *tkeys = B[B_HKEYS].as<uint64_t>();
+        uint32_t *tcount = B[B_HCOUNT].as<uint32_t>(), *misc = B[B_HMISC].as<uint32_t>();
+        CK(cudaMemsetAsync(tkeys, 0xff, (size_t)hsize * 8, st));
+        CK(cudaMemsetAsync(tcount, 0, (size_t)hsize * 4, st));
+        CK(cudaMemsetAsync(misc, 0, 16, st));
+        launch_cluster_hash(st, B[B_KEY].as<uint64_t>(), (int64_t)npts, tkeys, tcount, hsize - 1, misc);
+        CK(B[B_HOKEYS].ensure((size_t)hsize * 8));
+        CK(B[B_HOSLOTS].ensure((size_t)hsize * 4));
+        launch_cluster_collect(st, tkeys, hsize, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), misc + 1);
+        in->launches += 2;
+        uint32_t hm[2];
+        CK(cudaMemcpyAsync(hm, misc, 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        ncl = (int64_t)last[0] + last[1];
-        CK(B[B_CSTART].ensure(ncl * 4));
-        CK(B[B_CFRAME].ensure(ncl * 4));
-        launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
-                              B[B_CFRAME].as<int32_t>());
-        in->launches += 1;
+        const bool hashed = hm[0] == 0;
+        if (hashed) {
+            ncl = hm[1];
+            CK(B[B_CSTART].ensure(ncl * 4 + 4));
+            CK(B[B_CFRAME].ensure(ncl * 4 + 4));
+            CK(B[B_HSKEYS].ensure(ncl * 8 + 8));
+            CK(B[B_HSSLOTS].ensure(ncl * 4 + 4));
+            CK(B[B_HCCOUNT].ensure(ncl * 4 + 4));
+            uint64_t *sk = B[B_HSKEYS].as<uint64_t>();
+            uint32_t *ss = B[B_HSSLOTS].as<uint32_t>(), *cc = B[B_HCCOUNT].as<uint32_t>();
+            if (!cub_call(in, [&](void *t, size_t &b) {
+                    return cub::DeviceRadixSort::SortPairs(t, b, B[B_HOKEYS].as<uint64_t>(), sk,
+                                                           B[B_HOSLOTS].as<uint32_t>(), ss, ncl, 0, 2 * nb, st);
+                }))
+                return false;
+            launch_cluster_rank(st, sk, ss, ncl, tcount, B[B_HRANK].as<uint32_t>(), cc, nb, dfr, (int)n,
+                                B[B_CFRAME].as<int32_t>());
+            if (!cub_call(in, [&](void *t, size_t &b) {
+                    return cub::DeviceScan::ExclusiveSum(t, b, cc, B[B_CSTART].as<uint32_t>(), ncl, st);
+                }))
+                return false;
+            uint32_t *cidx = B[B_HEAD].as<uint32_t>(), *cidx2 = B[B_HSCAN].as<uint32_t>();
+            launch_cluster_assign(st, B[B_KEY].as<uint64_t>(), (int64_t)npts, tkeys, hsize - 1,
+                                  B[B_HRANK].as<uint32_t>(), cidx);
+            in->launches += 2;
+            const int cb = bits_for((uint64_t)ncl);
+            if (!cub_call(in, [&](void *t, size_t &b) {
+                    return cub::DeviceRadixSort::SortPairs(t, b, cidx, cidx2, B[B_VAL].as<uint64_t>(),
+                                                           B[B_VAL2].as<uint64_t>(), (int64_t)npts, 0,
+                                                           cb > 0 ? cb : 1, st);
+                }))
+                return false;
+        } else {
+            if (!cub_call(in, [&](void *t, size_t &b) {
+                    return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
+                                                           B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
+                                                           (int64_t)npts, 0, 2 * nb, st);
+                }))
+                return false;
+            const uint64_t *skey = B[B_KEY2].as<uint64_t>();
+            uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
+            launch_cluster_heads(st, skey, npts, head);
+            in->launches += 1;
+            if (!cub_call(in, [&](void *t, size_t &b) {
+                    return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
+                }))
+                return false;
+            uint32_t last[2];
+            CK(cudaMemcpyAsync(&last[0], hscan + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&last[1], head + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ncl = (int64_t)last[0] + last[1];
+            CK(B[B_CSTART].ensure(ncl * 4));
+            CK(B[B_CFRAME].ensure(ncl * 4));
+            launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
+                                  B[B_CFRAME].as<int32_t>());
+            in->launches += 1;
+        }
         CK(cudaEventRecord(in->ev[5], st));
 
         // quads
@@ -500,6 +555,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
             }))
             return false;
+        uint32_t last[2];
         CK(cudaMemcpyAsync(&last[0], qscan + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&last[1], qok + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

@@ -628,9 +628,112 @@ __global__ void k_point_emit(const FrameDesc *frames, const uint8_t *thr, const 
     }
 }
 
+// 7. Clusters, by hashing (fast/clusters.c:318-382 groups points by their
+// label pair in a hash table too). The distinct pairs go into an
+// open-addressing table (each warp inserts each distinct pair of its 32
+// points once and adds its count); the few distinct pairs are sorted, which
+// gives every cluster its index in (larger, smaller) label order; each point
+// then carries its cluster index, and a stable radix sort on that index of
+// only log2(clusters) bits groups the points in emission order. A probe
+// that runs past CH_PROBES slots sets *full: the caller then groups by the
+// full sort instead.
+#define CH_EMPTY 0xffffffffffffffffull
+#define CH_PROBES 64
+
+__device__ __forceinline__ uint32_t ch_hash(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    return (uint32_t)k;
+}
+
+__global__ void k_cluster_hash(const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount, uint32_t mask,
+                               uint32_t *full) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        const uint64_t k = valid ? key[i] : CH_EMPTY;
+        const uint32_t peers = __match_any_sync(0xffffffffu, k);
+        if (!valid || lane != __ffs(peers) - 1) continue;
+        uint32_t slot = ch_hash(k) & mask;
+        bool found = false;
+        for (int p = 0; p < CH_PROBES; p++) {
+            uint64_t cur = *(volatile uint64_t *)(tkeys + slot);
+            if (cur == CH_EMPTY) {
+                const unsigned long long old =
+                    atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + slot), CH_EMPTY, k);
+                cur = old == CH_EMPTY ? k : old;
+            }
+            if (cur == k) {
+                found = true;
+                break;
+            }
+            slot = (slot + 1) & mask;
+        }
+        if (found)
+            atomicAdd(tcount + slot, (uint32_t)__popc(peers));
+        else
+            atomicOr(full, 1u);
+    }
+}
+
+// The occupied slots, in no particular order: (pair, slot).
+__global__ void k_cluster_collect(const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
+                                  uint32_t *count) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s0 = blockIdx.x * blockDim.x; s0 < size; s0 += gridDim.x * blockDim.x) {
+        const uint32_t s = s0 + threadIdx.x;
+        const uint64_t k = s < size ? tkeys[s] : CH_EMPTY;
+        const bool occ = k != CH_EMPTY;
+        const uint32_t bal = __ballot_sync(0xffffffffu, occ);
+        if (!bal) continue;
+        uint32_t at = 0;
+        if (lane == __ffs(bal) - 1) at = atomicAdd(count, (uint32_t)__popc(bal));
+        at = __shfl_sync(0xffffffffu, at, __ffs(bal) - 1) + __popc(bal & ((1u << lane) - 1u));
+        if (occ) {
+            okeys[at] = k;
+            oslots[at] = s;
+        }
+    }
+}
+
+// Cluster r (in pair order): its table slot gets r; its point count and
+// its frame (the frame whose node range holds the larger label).
+__global__ void k_cluster_rank(const uint64_t *skeys, const uint32_t *sslots, int64_t ncl, const uint32_t *tcount,
+                               uint32_t *rank_of_slot, uint32_t *ccount, int nb, const FrameDesc *frames,
+                               int nframes, int32_t *cframe) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < ncl; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = sslots[r];
+        rank_of_slot[s] = (uint32_t)r;
+        ccount[r] = tcount[s];
+        const int64_t node = (int64_t)(skeys[r] >> nb);
+        int lo = 0, hi = nframes - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (frames[mid].node_off <= node)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        cframe[r] = lo;
+    }
+}
+
+// Each point's cluster index (its pair is in the table).
+__global__ void k_cluster_assign(const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
+                                 const uint32_t *rank_of_slot, uint32_t *cidx) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = key[i];
+        uint32_t slot = ch_hash(k) & mask;
+        for (int p = 0; p < CH_PROBES && tkeys[slot] != k; p++) slot = (slot + 1) & mask;
+        cidx[i] = rank_of_slot[slot];
+    }
+}
+
 // ---------------------------------------------------------------------------
-// 7. Clusters: after the stable sort by key, each run of equal keys is a
-// cluster (points in emission order).
+// 7b. Clusters by the full sort (the fallback): after the stable sort by
+// key, each run of equal keys is a cluster (points in emission order).
 
 __global__ void k_cluster_heads(const uint64_t *key, int64_t n, uint32_t *head) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -2776,6 +2879,28 @@ void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t 
 void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                        const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb) {
     k_point_emit<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
+}
+
+void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount,
+                         uint32_t mask, uint32_t *full) {
+    k_cluster_hash<<<flat_blocks(n, 256), 256, 0, s>>>(key, n, tkeys, tcount, mask, full);
+}
+
+void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
+                            uint32_t *count) {
+    k_cluster_collect<<<flat_blocks(size, 256), 256, 0, s>>>(tkeys, size, okeys, oslots, count);
+}
+
+void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
+                         const uint32_t *tcount, uint32_t *rank_of_slot, uint32_t *ccount, int nb,
+                         const FrameDesc *frames, int nframes, int32_t *cframe) {
+    k_cluster_rank<<<flat_blocks(ncl, 256), 256, 0, s>>>(skeys, sslots, ncl, tcount, rank_of_slot, ccount, nb, frames,
+                                                        nframes, cframe);
+}
+
+void launch_cluster_assign(cudaStream_t s, const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
+                           const uint32_t *rank_of_slot, uint32_t *cidx) {
+    k_cluster_assign<<<flat_blocks(n, 256), 256, 0, s>>>(key, n, tkeys, mask, rank_of_slot, cidx);
 }
 
 void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head) {

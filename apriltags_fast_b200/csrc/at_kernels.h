@@ -51,6 +51,15 @@ void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t 
 void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                        const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb);
 void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head);
+void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount,
+                         uint32_t mask, uint32_t *full);
+void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
+                            uint32_t *count);
+void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
+                         const uint32_t *tcount, uint32_t *rank_of_slot, uint32_t *ccount, int nb,
+                         const FrameDesc *frames, int nframes, int32_t *cframe);
+void launch_cluster_assign(cudaStream_t s, const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
+                           const uint32_t *rank_of_slot, uint32_t *cidx);
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
                            int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe);
 void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
