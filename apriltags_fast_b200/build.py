@@ -28,6 +28,7 @@ FP = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 CUFLAGS = ARCH + FP + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                        "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 SOURCES = ["at_kernels.cu", "at_detector.cu", "at_noalloc.cu"]
+C_SOURCES = ["at_upstream.c"]
 
 
 def _run(cmd):
@@ -57,6 +58,14 @@ def build(reference: str | None = None, force: bool = False) -> str:
         if force or _newer(fam_o, [fam_c]):
             _run(["gcc", "-O1", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c", fam_c, "-o", fam_o])
         objs.append(fam_o)
+    # the upstream API shim (plain C over the native API)
+    for src in C_SOURCES:
+        c = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".c", ".o"))
+        if force or _newer(o, [c] + [os.path.join(ROOT, "include", "apriltag.h"), os.path.join(ROOT, "include", "apriltag_fast.h")]):
+            _run(["gcc", "-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
+                  "-c", c, "-o", o])
+        objs.append(o)
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -64,7 +73,7 @@ def build(reference: str | None = None, force: bool = False) -> str:
             _run([NVCC] + CUFLAGS + ["-c", s, "-o", o])
         objs.append(o)
     if force or _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm"])
     return LIB
 
 

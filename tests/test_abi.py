@@ -12,12 +12,16 @@ from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "apriltag_fast.h")
+UPSTREAM_HEADERS = [os.path.join(ROOT, "include", h) for h in (
+    "apriltag.h", "common/matd.h", "common/image_u8.h", "tag16h5.h", "tag25h9.h", "tag36h10.h", "tag36h11.h",
+    "tagCircle21h7.h", "tagCircle49h12.h", "tagCustom48h12.h", "tagStandard41h12.h", "tagStandard52h13.h")]
 
 
-def declared_functions():
-    src = open(HEADER).read()
+def declared_functions(path=HEADER, prefix=r"at_\w+"):
+    src = open(path).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(at_\w+)\s*\(", src, flags=re.M)
+    src = re.sub(r"static inline[^{]*\{.*?\n\}", "", src, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(" + prefix + r")\s*\(", src, flags=re.M)
     return sorted(set(names))
 
 
@@ -27,6 +31,35 @@ def test_library_loads_and_exports_all_declared_symbols():
     assert len(names) >= 23
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
+
+
+def test_library_exports_the_upstream_api():
+    L = C.CDLL(AT.LIB_PATH)
+    names = []
+    for h in UPSTREAM_HEADERS:
+        names += declared_functions(h, r"(?:apriltag|matd|image_u8|tag)\w+")
+    assert "apriltag_detector_detect" in names and "tag36h11_create" in names and len(names) >= 35
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_upstream_struct_layouts_match_reference(tmp_path):
+    """include/apriltag.h keeps the reference apriltag.h layouts (x86-64):
+    the numbers below were printed by tests/upstream_layout.c compiled
+    against the reference's own apriltag.h."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    exe = str(tmp_path / "layout")
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                           os.path.join(ROOT, "tests", "upstream_layout.c")])
+    out = subprocess.check_output([exe]).decode().split("\n")
+    assert out[0] == ("family 72 ncodes 0 codes 8 wab 16 tw 20 rb 24 nbits 28 bx 32 by 40 h 48 name 56 impl 64")
+    assert out[1] == ("detector 160 nthreads 0 qd 4 qs 8 re 12 ds 16 debug 24 qtp 28 tp 56 nedges 64 nsegments 68 "
+                      "nquads 72 tf 80 wp 88 mutex 96 fast 136 fb 144 fc 152")
+    assert out[2] == "detection 112 family 0 id 8 hamming 12 dm 16 H 24 c 32 p 48"
+    assert out[3] == "qtp 28 zarray 24 matd 16 image_u8 24 timeprofile 16"
 
 
 def test_struct_layouts_match_reference():

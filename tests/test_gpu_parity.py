@@ -2,6 +2,8 @@
 oracle on the same inputs. Integer, byte and index results must be equal;
 the floating point results too (bit-exact: the tolerance is zero), since
 the kernels round every operation as the reference does."""
+import os
+
 import numpy as np
 import pytest
 
@@ -11,6 +13,7 @@ from oracle import oracle as O
 from tests import helpers as H
 
 pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CASES = H.golden_cases()
 
 
@@ -166,3 +169,35 @@ def test_parameter_limits_fail_loudly():
     with pytest.raises(RuntimeError):
         det.detect(H.golden_images()[0])
     assert not det.add_family("tag25h9", 4)
+
+
+@pytest.mark.parametrize("family,bits", [("tag36h11", 2), ("tagStandard41h12", 1)])
+def test_upstream_api_equals_native(tmp_path, family, bits):
+    """apriltag_detector_detect (include/apriltag.h) returns exactly the
+    native at_detect's detections, in the same order (apriltag.c:152-208 of
+    the reference is the same wrapper), from a C program linked against the
+    library."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    libdir = os.path.dirname(AT.LIB_PATH)
+    exe = str(tmp_path / "upstream_detect")
+    subprocess.check_call(["gcc", "-O1", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                           os.path.join(ROOT, "tests", "upstream_detect.c"), "-L", libdir, "-lapriltag_b200",
+                           "-Wl,-rpath," + libdir])
+    out = []
+    for img in ("synth_640x480_000.pgm", "synth_640x480_001.pgm"):
+        txt = subprocess.check_output([exe, os.path.join(H.GOLDEN, img), family, str(bits)]).decode()
+        lines = txt.strip().split("\n")
+        up = [l[2:] for l in lines if l.startswith("U ")]
+        nat = [l[2:] for l in lines if l.startswith("N ")]
+        assert up == nat and len(up) > 0
+        nq = [l for l in lines if l.startswith("nquads")][0].split()
+        assert nq[1] == [l for l in lines if l.startswith("native nquads")][0].split()[2]
+        assert nq[3] == "9"
+        assert "after clear 0" in lines
+        tw = AT.family(family).total_width
+        assert f"tag image {tw} {tw}" in lines
+        out += up
+    assert len(out) > 0
