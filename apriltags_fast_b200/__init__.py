@@ -114,6 +114,23 @@ FAMILY_NAMES = ("tag16h5", "tag25h9", "tag36h10", "tag36h11", "tagCircle21h7", "
 _lib = None
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("workers", C.c_int32), ("max_batch", C.c_int32), ("memory_budget", C.c_int64)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("user", C.c_uint64), ("status", C.c_int32), ("batch_frames", C.c_int32),
+                ("worker", C.c_int32), ("pad", C.c_int32), ("ndetections", C.c_int64), ("nquads", C.c_int64),
+                ("detections", C.POINTER(CDetection)), ("t_submit", C.c_double), ("t_start", C.c_double),
+                ("t_done", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("admitted", C.c_int64), ("rejected", C.c_int64), ("completed", C.c_int64), ("batches", C.c_int64),
+                ("in_flight", C.c_int64), ("pending", C.c_int64), ("peak_arena_bytes", C.c_int64),
+                ("bytes_per_pixel", C.c_double)]
+
+
 def lib():
     """The loaded library (raises if it was not built)."""
     global _lib
@@ -135,6 +152,15 @@ def lib():
         L.at_detector_last_error.restype = C.c_int
         L.at_detector_diag.argtypes = [C.POINTER(CDetector), C.c_int, C.c_void_p, C.c_int64]
         L.at_detector_diag.restype = C.c_int64
+        L.at_server_create.argtypes = [C.POINTER(CDetector), C.POINTER(ServerConfig)]
+        L.at_server_create.restype = C.c_void_p
+        L.at_server_submit.argtypes = [C.c_void_p, C.POINTER(Frame), C.c_uint64]
+        L.at_server_submit.restype = C.c_uint64
+        L.at_server_poll.argtypes = [C.c_void_p, C.POINTER(ServerResult), C.c_int64, C.c_int32]
+        L.at_server_poll.restype = C.c_int64
+        L.at_server_free_result.argtypes = [C.POINTER(ServerResult)]
+        L.at_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.at_server_destroy.argtypes = [C.c_void_p]
         L.at_family_by_name.argtypes = [C.c_char_p]
         L.at_family_by_name.restype = C.POINTER(Family)
         for n in FAMILY_NAMES:
@@ -295,6 +321,65 @@ class Detector:
         if getattr(self, "_td", None):
             self._L.at_detector_destroy(self._td)
             self._td = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Mirror of at_server: continuous batching over `workers` detectors made
+    from `detector` (its parameters and families). submit() returns a ticket
+    (0: rejected); the image must stay alive and unchanged until its result
+    has been polled. poll() returns finished results as dicts with the
+    detections as a numpy record array (DETECTION_DTYPE)."""
+
+    def __init__(self, detector: "Detector", workers: int = 2, max_batch: int = 16, memory_budget: int = 24 << 30):
+        self._L = lib()
+        cfg = ServerConfig(workers, max_batch, memory_budget)
+        self._s = self._L.at_server_create(detector._td, C.byref(cfg))
+        if not self._s:
+            raise RuntimeError("at_server_create failed")
+        self._keep = {}
+
+    def submit(self, img, user: int = 0, family_mask: int = 0) -> int:
+        ptr, w, h, s = _image_arg(img, None)
+        f = Frame(ptr, w, h, s, family_mask)
+        t = int(self._L.at_server_submit(self._s, C.byref(f), user))
+        if t:
+            self._keep[t] = img
+        return t
+
+    def poll(self, max_results: int = 256, wait_ms: int = 0) -> list:
+        buf = (ServerResult * max_results)()
+        n = int(self._L.at_server_poll(self._s, buf, max_results, wait_ms))
+        out = []
+        for i in range(n):
+            r = buf[i]
+            nd = int(r.ndetections)
+            if nd:
+                raw = C.cast(r.detections, C.POINTER(C.c_uint8 * (168 * nd))).contents
+                dets = np.frombuffer(raw, DETECTION_DTYPE, nd).copy()
+            else:
+                dets = np.zeros(0, DETECTION_DTYPE)
+            out.append({"ticket": int(r.ticket), "user": int(r.user), "status": int(r.status),
+                        "detections": dets, "nquads": int(r.nquads), "batch_frames": int(r.batch_frames),
+                        "worker": int(r.worker), "t_submit": r.t_submit, "t_start": r.t_start, "t_done": r.t_done})
+            self._L.at_server_free_result(C.byref(buf[i]))
+            self._keep.pop(int(r.ticket), None)
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._L.at_server_get_stats(self._s, C.byref(st))
+        return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_s", None):
+            self._L.at_server_destroy(self._s)
+            self._s = None
 
     def __del__(self):
         try:

@@ -38,7 +38,9 @@ namespace {
 struct DBuf {
     void *p = nullptr;
     size_t cap = 0;
+    size_t want = 0;  // the largest request of the current call
     cudaError_t ensure(size_t bytes) {
+        if (bytes > want) want = bytes;
         if (bytes <= cap) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
@@ -363,6 +365,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
 
     // arenas
     DBuf *B = in->buf;
+    for (int k = 0; k < B_NBUF; k++) B[k].want = 0;
     CK(B[B_FRAMES].ensure(n * sizeof(FrameDesc)));
     CK(B[B_IMG].ensure(img + 1));
     CK(B[B_QIM].ensure(qpx));
@@ -790,6 +793,29 @@ void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_fram
     int64_t nq = 0;
     for (int64_t i = 0; i < n; i++) nq += results[i].nquads;
     td->nquads = nq;
+}
+
+// For the server (at_server.cu): a detector with src's parameters and
+// families, and the device bytes a detector's arenas hold.
+at_detector *at_detector_clone(const at_detector *src) {
+    at_detector *td = at_detector_create();
+    at_internal *in = td->in;
+    in->device = src->in->device;
+    td->nthreads = src->nthreads;
+    td->quad_decimate = src->quad_decimate;
+    td->quad_sigma = src->quad_sigma;
+    td->refine_edges = src->refine_edges;
+    td->decode_sharpening = src->decode_sharpening;
+    td->debug = false;
+    td->qtp = src->qtp;
+    for (int i = 0; i < src->in->nfam; i++) at_add_family(td, &src->in->families[i], src->in->bits[i]);
+    return td;
+}
+
+int64_t at_detector_arena_bytes(const at_detector *td) {
+    int64_t b = 0;
+    for (int k = 0; k < B_NBUF; k++) b += (int64_t)td->in->buf[k].want;
+    return b;
 }
 
 void at_detect(at_detector *td, const uint8_t *pixels, int64_t width, int64_t height, int64_t stride) {

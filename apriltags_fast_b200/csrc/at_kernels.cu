@@ -979,14 +979,93 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
 // memory), 512 threads for the larger ones (dynamic shared memory; sorts
 // beyond FIT_LARGE_SORT points fall back to global scratch).
 #define FIT_SMALL 1024
-#define FIT_LARGE_SORT 8192
-#define FIT_CHUNK_SMALL 1024
-#define FIT_CHUNK_LARGE 4096
+#define FIT_LARGE_SORT 14336
+#define FIT_CHUNK_SMALL 512
+#define FIT_CHUNK_LARGE 1024
 
 // dynamic shared memory of one block of the fit kernel
-__host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk) {
-    return (size_t)sort_cap * 12 + (size_t)chunk * 24;
+// Shared memory of the block fit kernel for clusters of up to sort_cap
+// points: region X (the angle keys; then the radix sort's second buffers;
+// then the staged moment terms of a chunk of points), the sort keys (4 B)
+// and point indices (2 B), and the radix histograms (256 per warp).
+__host__ __device__ constexpr size_t fit_x_bytes(int sort_cap, int chunk) {
+    return (size_t)sort_cap * 8 > (size_t)chunk * 48 ? (size_t)sort_cap * 8 : (size_t)chunk * 48;
 }
+__host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk, int nwarps) {
+    return fit_x_bytes(sort_cap, chunk) + (size_t)sort_cap * 6 + (size_t)256 * nwarps * 4;
+}
+
+// Stable sort of n (32-bit key, 16-bit value) pairs by key: four passes of
+// 8 bits. Each pass counts digits per warp over the warp's contiguous range,
+// scans the counts in (digit, warp) order, and scatters each warp's range in
+// order, 32 at a time, ranking equal digits by lane (match_any). ka/va hold
+// the input and get the result; kb/vb are the second buffers; hist holds
+// 256 counters per warp.
+__device__ void block_radix_sort32(uint32_t *ka, uint16_t *va, uint32_t *kb, uint16_t *vb, int n, uint32_t *hist) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+    const int per = ((n + nw - 1) / nw + 31) & ~31;
+    const int w0 = w * per < n ? w * per : n, w1 = w0 + per < n ? w0 + per : n;
+    const int nh = 256 * nw;
+    __shared__ uint32_t s_part[32];
+    for (int shift = 0; shift < 32; shift += 8) {
+        for (int i = tid; i < nh; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for (int i = w0 + lane; i < w1; i += 32) atomicAdd(hist + (int)(ka[i] >> shift & 255u) * nw + w, 1u);
+        __syncthreads();
+        // exclusive scan of hist: thread t owns entries [t * e, t * e + e)
+        const int e = (nh + blockDim.x - 1) / blockDim.x;
+        const int h0 = tid * e < nh ? tid * e : nh, h1 = h0 + e < nh ? h0 + e : nh;
+        uint32_t sum = 0;
+        for (int i = h0; i < h1; i++) sum += hist[i];
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_part[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t v = lane < nw ? s_part[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (lane < nw) s_part[lane] = v;
+        }
+        __syncthreads();
+        uint32_t run = (w > 0 ? s_part[w - 1] : 0) + incl - sum;
+        for (int i = h0; i < h1; i++) {
+            const uint32_t c = hist[i];
+            hist[i] = run;
+            run += c;
+        }
+        __syncthreads();
+        for (int i0 = w0; i0 < w1; i0 += 32) {
+            const int i = i0 + lane;
+            const bool valid = i < w1;
+            const uint32_t k = valid ? ka[i] : 0;
+            const int d = valid ? (int)(k >> shift & 255u) : 256 + lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t base = valid ? hist[d * nw + w] : 0;
+            if (valid) {
+                const uint32_t at = base + __popc(peers & ((1u << lane) - 1u));
+                kb[at] = k;
+                vb[at] = va[i];
+            }
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) hist[d * nw + w] = base + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t *tk = ka;
+        ka = kb;
+        kb = tk;
+        uint16_t *tv = va;
+        va = vb;
+        vb = tv;
+    }
+}
+
 
 // Optional phase timers of the fit kernel (a -DAT_FIT_PROF build only).
 #ifdef AT_FIT_PROF
@@ -1018,17 +1097,21 @@ extern "C" int at_fit_prof_copy(void *dst, int n) {
 #endif
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
+__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
                                                    const uint64_t *pts, const uint32_t *cstart,
                                                    const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                    FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err,
                                                    const uint32_t *list, const uint32_t *count, uint32_t *next,
                                                    int sort_cap, int chunk) {
     extern __shared__ __align__(16) unsigned char fit_smem[];
-    uint64_t *s_key = reinterpret_cast<uint64_t *>(fit_smem);
-    double *s_w = reinterpret_cast<double *>(fit_smem + (size_t)sort_cap * 8);
-    double *s_fx = s_w + chunk, *s_fy = s_fx + chunk;
-    uint32_t *s_val = reinterpret_cast<uint32_t *>(fit_smem + (size_t)sort_cap * 8 + (size_t)chunk * 24);
+    const size_t xb = fit_x_bytes(sort_cap, chunk);
+    uint64_t *s_key = reinterpret_cast<uint64_t *>(fit_smem);  // X: angle keys
+    uint32_t *s_kb = reinterpret_cast<uint32_t *>(fit_smem);   // X: the sort's second buffers
+    uint16_t *s_vb = reinterpret_cast<uint16_t *>(fit_smem + (size_t)sort_cap * 4);
+    double *s_w = reinterpret_cast<double *>(fit_smem);        // X: six terms per staged point
+    uint32_t *s_ka = reinterpret_cast<uint32_t *>(fit_smem + xb);
+    uint16_t *s_val = reinterpret_cast<uint16_t *>(fit_smem + xb + (size_t)sort_cap * 4);
+    uint32_t *s_hist = reinterpret_cast<uint32_t *>(fit_smem + xb + (size_t)sort_cap * 6);
     __shared__ float s_lane[8];
     __shared__ int s_rev, s_ok;
     __shared__ uint32_t s_bb[4][NT / 32];
@@ -1094,7 +1177,10 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         FIT_PROF(2)
         // angle keys, and the dot product of offsets and gradients: 8 lanes
         // over the whole groups of 8, then the rest (fast/quads.c:467-512)
-        uint64_t *keys = scr.keys + s0;
+        // clusters that fit keep their keys in shared memory, where the
+        // leaf step turns them into sort keys in place
+        const bool in_smem = sz <= sort_cap;
+        uint64_t *keys = in_smem ? s_key : scr.keys + s0;
         for (int64_t i = tid; i < sz; i += NT) {
             float dx = __fsub_rn((float)(P[i] & 0xffff), cx), dy = __fsub_rn((float)(P[i] >> 16 & 0xffff), cy);
             keys[i] = angle_key(dx, dy, (uint32_t)i);
@@ -1104,8 +1190,8 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
             // the terms dx*gx + dy*gy by all threads into shared memory (the
             // moment staging area, free here), then lane l < 8 sums terms
             // l, l+8, ... in order
-            float *s_term = reinterpret_cast<float *>(s_w);
-            const int64_t tcap = 6 * (int64_t)chunk;  // a multiple of 8
+            float *s_term = reinterpret_cast<float *>(s_ka);
+            const int64_t tcap = sort_cap;  // a multiple of 8
             float acc = 0.0f;
             for (int64_t c0 = 0; c0 < nv; c0 += tcap) {
                 const int64_t cn = dmin(tcap, nv - c0);
@@ -1159,41 +1245,82 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         // place), packed into 64 bits as head's slope bits, 0xffff - head's
         // index, and the place.
         FIT_PROF(3)
-        const bool in_smem = sz <= sort_cap;
-        uint64_t *sk = in_smem ? s_key : scr.skey + s0;
-        uint32_t *sv = in_smem ? s_val : scr.sval + s0;
-        for (int64_t p = tid; p < sz; p += NT) {
-            uint32_t lf = leaf_of(sz, p);
-            int64_t lo = lf >> 8, len = lf & 255;
-            if (p != lo) continue;
-            uint64_t k5[5];
-            for (int t = 0; t < len; t++) k5[t] = keys[lo + t];
-            leaf_network(k5, (int)len);
-            uint64_t head = 0;
-            for (int t = 0; t < len; t++) {
-                if (t == 0 || k5[t] > head) head = k5[t];
-                uint32_t hidx = ~(uint32_t)head;
-                sk[lo + t] = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 3 | (uint64_t)t;
-                sv[lo + t] = ~(uint32_t)k5[t];
+        uint64_t *sk = scr.skey + s0;
+        uint32_t *sv = scr.sval + s0;
+        if (in_smem) {
+            // Lay the points out in (head index descending, place) order:
+            // leaves in reverse order, and in each leaf its blocks by head
+            // index descending, each block in network order. A stable sort
+            // by the head's slope bits then gives the (head, place) order.
+            for (int64_t p = tid; p < sz; p += NT) {
+                uint32_t lf = leaf_of(sz, p);
+                const int lo = (int)(lf >> 8), len = (int)(lf & 255);
+                if (p != lo) continue;
+                // everything indexed by constants: registers only
+                uint64_t k5[5];
+#pragma unroll
+                for (int t = 0; t < 5; t++) k5[t] = t < len ? keys[lo + t] : ~0ull;
+                leaf_network(k5, len);
+                uint32_t hid[5], hkey[5];
+                int bs[5];
+                uint64_t head = k5[0];
+                int start = 0;
+#pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    if (t > 0 && k5[t] > head) {
+                        head = k5[t];
+                        start = t;
+                    }
+                    hid[t] = ~(uint32_t)head;
+                    hkey[t] = (uint32_t)(head >> 32);
+                    bs[t] = start;
+                }
+                const int base = (int)sz - lo - len;
+#pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    if (t >= len) continue;
+                    int before = 0;  // points of blocks with a larger head index
+#pragma unroll
+                    for (int t2 = 0; t2 < 5; t2++) before += t2 < len && hid[t2] > hid[t];
+                    const int pos = base + before + (t - bs[t]);
+                    s_ka[pos] = hkey[t];
+                    s_val[pos] = (uint16_t)~(uint32_t)k5[t];
+                }
             }
-        }
-        __syncthreads();
-        FIT_PROF(4)
-        {
-            // the merge's second buffer: the moment staging area (free now)
-            // in shared memory, or two scratch arrays beside them
-            uint64_t *kb = in_smem ? reinterpret_cast<uint64_t *>(s_w) : reinterpret_cast<uint64_t *>(scr.w + s0);
-            uint32_t *vb = in_smem ? reinterpret_cast<uint32_t *>(kb + sort_cap) : reinterpret_cast<uint32_t *>(scr.fx + s0);
+            __syncthreads();
+            FIT_PROF(4)
+            block_radix_sort32(s_ka, s_val, s_kb, s_vb, (int)sz, s_hist);
+        } else {
+            for (int64_t p = tid; p < sz; p += NT) {
+                uint32_t lf = leaf_of(sz, p);
+                int64_t lo = lf >> 8, len = lf & 255;
+                if (p != lo) continue;
+                uint64_t k5[5];
+                for (int t = 0; t < len; t++) k5[t] = keys[lo + t];
+                leaf_network(k5, (int)len);
+                uint64_t head = 0;
+                for (int t = 0; t < len; t++) {
+                    if (t == 0 || k5[t] > head) head = k5[t];
+                    uint32_t hidx = ~(uint32_t)head;
+                    sk[lo + t] = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 3 | (uint64_t)t;
+                    sv[lo + t] = ~(uint32_t)k5[t];
+                }
+            }
+            __syncthreads();
+            FIT_PROF(4)
+            // the merge's second buffer: two scratch arrays
+            uint64_t *kb = reinterpret_cast<uint64_t *>(scr.w + s0);
+            uint32_t *vb = reinterpret_cast<uint32_t *>(scr.fx + s0);
             block_merge_sort(sk, sv, kb, vb, (int)sz);
         }
         FIT_PROF(5)
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
         // w = sqrt(gx^2 + gy^2) + 1 on the quad image (1 at its border),
-        // fx = x/2 + 1/2. Each chunk of points is staged in shared memory,
-        // then lane c of warp 0 (c < 6) runs prefix sum c in point order:
-        // the term of sum c is (w * a) * b with a, b in {fx, fy, 1} (a
-        // product with 1.0 is exact), so no lane branches.
+        // fx = x/2 + 1/2. Each chunk of points has its six terms (w fx, w fy,
+        // w fx fx, w fx fy, w fy fy, w; the reference's products) staged
+        // in shared memory by all threads, then lane q of warp 0 (q < 6)
+        // runs prefix sum q in point order.
         const uint8_t *im = qim + f.q_off;
         double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
         double run = 0.0;
@@ -1202,37 +1329,37 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
         for (int64_t k0 = 0; k0 < sz; k0 += chunk) {
             const int64_t kn = dmin((int64_t)chunk, sz - k0);
             for (int64_t t = tid; t < kn; t += NT) {
-                uint32_t src = sv[k0 + t];
-                int32_t px = (int32_t)(P[src] & 0xffff), py = (int32_t)(P[src] >> 16 & 0xffff);
-                int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
+                const uint32_t src = in_smem ? (uint32_t)s_val[k0 + t] : sv[k0 + t];
+                const uint64_t pt = P[src];
+                const int32_t px = (int32_t)(pt & 0xffff), py = (int32_t)(pt >> 16 & 0xffff);
+                const int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
                 int32_t g2 = 0;
                 if (ix > 0 && ix + 1 < f.qw && iy > 0 && iy + 1 < f.qh) {
-                    int64_t cc = (int64_t)iy * f.qw + ix;
-                    int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
-                    int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
+                    const int64_t cc = (int64_t)iy * f.qw + ix;
+                    const int32_t gx = (int32_t)im[cc + 1] - im[cc - 1];
+                    const int32_t gy = (int32_t)im[cc + f.qw] - im[cc - f.qw];
                     g2 = gx * gx + gy * gy;
                 }
-                s_w[t] = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
-                s_fx[t] = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
-                s_fy[t] = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+                const double w = __dadd_rn(__dsqrt_rn((double)g2), 1.0);
+                const double fx = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
+                const double fy = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
+                const double wx = __dmul_rn(w, fx), wy = __dmul_rn(w, fy);
+                s_w[0 * chunk + t] = wx;
+                s_w[1 * chunk + t] = wy;
+                s_w[2 * chunk + t] = __dmul_rn(wx, fx);
+                s_w[3 * chunk + t] = __dmul_rn(wx, fy);
+                s_w[4 * chunk + t] = __dmul_rn(wy, fy);
+                s_w[5 * chunk + t] = w;
             }
             __syncthreads();
             if (tid < 6) {
-                const int ca = tid == 1 || tid == 4 ? 1 : tid == 5 ? 2 : 0;  // 0 fx, 1 fy, 2 one
-                const int cb = tid == 2 ? 0 : tid == 3 || tid == 4 ? 1 : 2;
-                const double *A = ca == 0 ? s_fx : s_fy, *Bv = cb == 0 ? s_fx : s_fy;
+                const double *src = s_w + tid * chunk;
                 double *o = mout + k0;
-                // 8 terms at a time: their loads and products first, then the
-                // 8 dependent additions (the terms do not depend on the sum)
                 int64_t t = 0;
                 for (; t + 8 <= kn; t += 8) {
                     double v[8];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        double a = ca == 2 ? 1.0 : A[t + u];
-                        double b = cb == 2 ? 1.0 : Bv[t + u];
-                        v[u] = __dmul_rn(__dmul_rn(s_w[t + u], a), b);
-                    }
+                    for (int u = 0; u < 8; u++) v[u] = src[t + u];
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         run = __dadd_rn(run, v[u]);
@@ -1240,9 +1367,7 @@ __global__ void __launch_bounds__(NT) k_fit_quads(const FrameDesc *frames, GpuPa
                     }
                 }
                 for (; t < kn; t++) {
-                    double a = ca == 2 ? 1.0 : A[t];
-                    double b = cb == 2 ? 1.0 : Bv[t];
-                    run = __dadd_rn(run, __dmul_rn(__dmul_rn(s_w[t], a), b));
+                    run = __dadd_rn(run, src[t]);
                     o[t] = run;
                 }
             }
@@ -2933,7 +3058,8 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
     if (nclusters <= 0) return;
-    const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL), large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE);
+    const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL, 128 / 32),
+                 large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE, 512 / 32);
     cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
     cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
     cudaFuncSetAttribute(k_fit_order, cudaFuncAttributeMaxDynamicSharedMemorySize, FIT_ORDER_CAP * 8);

@@ -43,7 +43,46 @@ CONFIGS = {
     # per-tag blur 0.5-1.5, ramp 0.4-1.0, 1000 distractors
     "4032x3024": Config(4032, 3024, families=("tagStandard52h13", "tag36h11"), ntags=(80, 80), side=(16, 400),
                         tilt_deg=65.0, noise=6.0, blur=(0.5, 1.5), distractors=1000, ramp=(0.4, 1.0)),
+    # served request loop: 0-30 tag36h11 tags, otherwise as 640x480
+    "serve_720p": Config(1280, 720, ntags=(0, 30)),
+    "serve_1080p": Config(1920, 1080, ntags=(0, 30)),
+    "serve_2160p": Config(3840, 2160, ntags=(0, 30)),
+    # batched uneven frames: 0-40 tags of one family (tag36h11 or tag25h9)
+    "mixed_640x480_36h11": Config(640, 480, ntags=(0, 40)),
+    "mixed_640x480_25h9": Config(640, 480, families=("tag25h9",), ntags=(0, 40)),
+    "mixed_1280x720_36h11": Config(1280, 720, ntags=(0, 40)),
+    "mixed_1280x720_25h9": Config(1280, 720, families=("tag25h9",), ntags=(0, 40)),
+    "mixed_1920x1080_36h11": Config(1920, 1080, ntags=(0, 40)),
+    "mixed_1920x1080_25h9": Config(1920, 1080, families=("tag25h9",), ntags=(0, 40)),
+    "mixed_3840x2160_36h11": Config(3840, 2160, ntags=(0, 40)),
+    "mixed_3840x2160_25h9": Config(3840, 2160, families=("tag25h9",), ntags=(0, 40)),
 }
+
+
+def serve_mix(n: int, seed: int):
+    """n frames of the served mix: 60% 1280x720, 30% 1920x1080, 10%
+    3840x2160 (drawn per frame), each with 0-30 tag36h11 tags."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        u = rng.uniform()
+        name = "serve_720p" if u < 0.6 else "serve_1080p" if u < 0.9 else "serve_2160p"
+        out.append(make_frame(CONFIGS[name], seed * 100003 + i)[0])
+    return out
+
+
+def uneven_batch(n: int, seed: int):
+    """n frames of sizes drawn uniformly from 640x480, 1280x720, 1920x1080 and
+    3840x2160, each with 0-40 tags of tag36h11 or of tag25h9; returns
+    (frames, family names)."""
+    rng = np.random.default_rng(seed)
+    frames, fams = [], []
+    for i in range(n):
+        size = ("640x480", "1280x720", "1920x1080", "3840x2160")[int(rng.integers(4))]
+        fam = ("36h11", "25h9")[int(rng.integers(2))]
+        frames.append(make_frame(CONFIGS[f"mixed_{size}_{fam}"], seed * 100003 + i)[0])
+        fams.append("tag" + fam)
+    return frames, fams
 
 
 def tag_pattern(code: int, nbits: int, bit_x, bit_y, wab: int, tw: int, reversed_border: bool) -> np.ndarray:

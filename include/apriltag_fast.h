@@ -161,6 +161,49 @@ typedef struct at_frame_result {
    detections, frame by frame; td->ndetections their total. */
 void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *results);
 
+/* Serving (no counterpart in the reference, which detects one frame per
+   call). A server owns `workers` detectors made from `params` (its
+   parameters and families at creation), each with its own stream and
+   device arenas, and one thread each. Submitted frames queue oldest first;
+   a free worker takes every queued frame, up to max_batch frames and its
+   share (memory_budget / workers) of device memory at the learned bytes
+   per pixel, and detects them as one batch, so frames that arrive while a
+   batch is on the GPU are admitted to the next one and overlap it. A frame
+   that alone exceeds a worker's share is rejected. Each frame's
+   detections equal at_detect's for that frame alone. The pixels must stay
+   valid and unchanged until the frame's result has been polled. */
+typedef struct at_server at_server;
+typedef struct at_server_config {
+    int32_t workers;       /* concurrent batches (default 2) */
+    int32_t max_batch;     /* frames per batch (default 16) */
+    int64_t memory_budget; /* device bytes for all workers' frames (default 24 GiB) */
+} at_server_config;
+typedef struct at_server_result {
+    uint64_t ticket, user;   /* from at_server_submit */
+    int32_t status;          /* 0, or the worker detector's at_detector_last_error */
+    int32_t batch_frames;    /* frames in the batch it ran in */
+    int32_t worker;
+    int32_t pad;
+    int64_t ndetections, nquads;
+    at_detection *detections; /* owned by the result: at_server_free_result */
+    double t_submit, t_start, t_done; /* seconds, steady clock */
+} at_server_result;
+typedef struct at_server_stats {
+    int64_t admitted, rejected, completed, batches, in_flight, pending;
+    int64_t peak_arena_bytes; /* the largest worker arena seen */
+    double bytes_per_pixel;   /* the admission estimate in use */
+} at_server_stats;
+at_server *at_server_create(const at_detector *params, const at_server_config *cfg);
+/* Returns the request's ticket, or 0 when the frame is invalid or rejected. */
+uint64_t at_server_submit(at_server *s, const at_frame *frame, uint64_t user);
+/* Copies up to max finished results (waiting up to wait_ms for the first);
+   returns how many. */
+int64_t at_server_poll(at_server *s, at_server_result *out, int64_t max, int32_t wait_ms);
+void at_server_free_result(at_server_result *r);
+void at_server_get_stats(at_server *s, at_server_stats *out);
+/* Finishes the queued frames, stops the workers, frees everything. */
+void at_server_destroy(at_server *s);
+
 /* Diagnostics: copy an intermediate array of the last at_detect (or of
    frame 0 of the last batch) to host memory `dst` of `cap` bytes. Returns
    the array's size in bytes (copying min(size, cap)), or -1. `what`:

@@ -1,0 +1,104 @@
+"""GPU tests of the serving form (at_server_*) and of batches of uneven
+frames: each frame's result is the same alone and in the mix."""
+import time
+
+import numpy as np
+import pytest
+
+import apriltags_fast_b200 as AT
+from apriltags_fast_b200 import synth
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(det, frames):
+    out = []
+    for f in frames:
+        d = det.detect_batch([f], as_arrays=True)[0]
+        out.append((d.tobytes(), det.last_batch_nquads[0]))
+    return out
+
+
+def _drain(srv, n, timeout_s=60.0):
+    got = []
+    t0 = time.time()
+    while len(got) < n and time.time() - t0 < timeout_s:
+        got += srv.poll(64, wait_ms=50)
+    return got
+
+
+def test_server_results_equal_alone():
+    frames = synth.serve_mix(6, 11) + H.golden_images()
+    det = AT.Detector(["tag36h11"], 2)
+    alone = _alone(det, frames)
+    srv = AT.Server(det, workers=2, max_batch=4)
+    try:
+        tickets = []
+        for rep in range(3):
+            for i, f in enumerate(frames):
+                t = srv.submit(f, user=i)
+                assert t > 0
+                tickets.append(t)
+        res = _drain(srv, len(tickets))
+        assert len(res) == len(tickets)
+        assert sorted(r["ticket"] for r in res) == sorted(tickets)
+        assert any(r["batch_frames"] > 1 for r in res)  # frames were batched together
+        for r in res:
+            assert r["status"] == 0
+            assert (r["detections"].tobytes(), r["nquads"]) == alone[r["user"]]
+            assert r["t_submit"] <= r["t_start"] <= r["t_done"]
+        st = srv.stats()
+        assert st["completed"] == len(tickets) and st["rejected"] == 0 and st["pending"] == 0
+    finally:
+        srv.close()
+
+
+def test_server_single_request_equals_at_detect():
+    img = H.golden_images()[0]
+    det = AT.Detector(["tag36h11"], 2)
+    ref = det.detect(img)
+    srv = AT.Server(det, workers=1, max_batch=8)
+    try:
+        assert srv.submit(img, user=7) > 0
+        (r,) = _drain(srv, 1)
+        assert r["user"] == 7 and r["batch_frames"] == 1
+        assert len(r["detections"]) == len(ref)
+        for a, b in zip(r["detections"], ref):
+            assert int(a["id"]) == b.id and float(a["decision_margin"]) == b.decision_margin
+            assert tuple(a["H"]) == b.H
+    finally:
+        srv.close()
+
+
+def test_server_admission_by_memory_budget():
+    """A frame that alone needs more than a worker's share of the budget is
+    rejected; smaller frames are admitted and finish."""
+    det = AT.Detector(["tag36h11"], 2)
+    srv = AT.Server(det, workers=2, max_batch=4, memory_budget=64 << 20)
+    try:
+        big = np.zeros((2160, 3840), np.uint8)
+        small = H.golden_images()[0]
+        assert srv.submit(big) == 0
+        assert srv.submit(small) > 0
+        res = _drain(srv, 1)
+        assert len(res) == 1 and res[0]["status"] == 0
+        st = srv.stats()
+        assert st["rejected"] == 1 and st["admitted"] == 1
+    finally:
+        srv.close()
+
+
+def test_uneven_batch_with_family_sets_equals_single():
+    """Frames of four sizes with per-frame family sets in one batch: each
+    frame's detections equal the same frame run alone."""
+    frames, fams = synth.uneven_batch(8, 5)
+    det = AT.Detector(["tag36h11", "tag25h9"], 2)
+    masks = [1 if f == "tag36h11" else 2 for f in fams]
+    batch = det.detect_batch(frames, family_masks=masks, as_arrays=True)
+    nq = list(det.last_batch_nquads)
+    for i, f in enumerate(frames):
+        one = det.detect_batch([f], family_masks=[masks[i]], as_arrays=True)[0]
+        assert one.tobytes() == batch[i].tobytes()
+        assert det.last_batch_nquads[0] == nq[i]
+        assert all(int(x["family"]) == (0 if masks[i] == 1 else 1) for x in one)
