@@ -980,16 +980,17 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
 // beyond FIT_LARGE_SORT points fall back to global scratch).
 #define FIT_SMALL 1024
 #define FIT_LARGE_SORT 14336
-#define FIT_CHUNK_SMALL 512
+#define FIT_CHUNK_SMALL 256
 #define FIT_CHUNK_LARGE 1024
 
 // dynamic shared memory of one block of the fit kernel
 // Shared memory of the block fit kernel for clusters of up to sort_cap
 // points: region X (the angle keys; then the radix sort's second buffers;
 // then the staged moment terms of a chunk of points), the sort keys (4 B)
-// and point indices (2 B), and the radix histograms (256 per warp).
+// and point indices (2 B), and the radix histograms (256 per warp). The
+// moment terms take two chunks of six doubles per point.
 __host__ __device__ constexpr size_t fit_x_bytes(int sort_cap, int chunk) {
-    return (size_t)sort_cap * 8 > (size_t)chunk * 48 ? (size_t)sort_cap * 8 : (size_t)chunk * 48;
+    return (size_t)sort_cap * 8 > (size_t)chunk * 96 ? (size_t)sort_cap * 8 : (size_t)chunk * 96;
 }
 __host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk, int nwarps) {
     return fit_x_bytes(sort_cap, chunk) + (size_t)sort_cap * 6 + (size_t)256 * nwarps * 4;
@@ -1317,18 +1318,17 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
         // w = sqrt(gx^2 + gy^2) + 1 on the quad image (1 at its border),
-        // fx = x/2 + 1/2. Each chunk of points has its six terms (w fx, w fy,
-        // w fx fx, w fx fy, w fy fy, w; the reference's products) staged
-        // in shared memory by all threads, then lane q of warp 0 (q < 6)
-        // runs prefix sum q in point order.
+        // fx = x/2 + 1/2. Chunks of points get their six terms (w fx, w fy,
+        // w fx fx, w fx fy, w fy fy, w; the reference's products) staged in
+        // shared memory, two buffers deep: while lane q < 6 of warp 0 runs
+        // prefix sum q over chunk c in point order, the other warps stage
+        // chunk c + 1.
         const uint8_t *im = qim + f.q_off;
         double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
         double run = 0.0;
-        const int ln = tid & 31;
-        double *mout = M[ln < 6 ? ln : 5];
-        for (int64_t k0 = 0; k0 < sz; k0 += chunk) {
+        auto stage = [&](int64_t k0, double *buf, int first, int stride) {
             const int64_t kn = dmin((int64_t)chunk, sz - k0);
-            for (int64_t t = tid; t < kn; t += NT) {
+            for (int64_t t = first; t < kn; t += stride) {
                 const uint32_t src = in_smem ? (uint32_t)s_val[k0 + t] : sv[k0 + t];
                 const uint64_t pt = P[src];
                 const int32_t px = (int32_t)(pt & 0xffff), py = (int32_t)(pt >> 16 & 0xffff);
@@ -1344,35 +1344,61 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
                 const double fx = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
                 const double fy = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
                 const double wx = __dmul_rn(w, fx), wy = __dmul_rn(w, fy);
-                s_w[0 * chunk + t] = wx;
-                s_w[1 * chunk + t] = wy;
-                s_w[2 * chunk + t] = __dmul_rn(wx, fx);
-                s_w[3 * chunk + t] = __dmul_rn(wx, fy);
-                s_w[4 * chunk + t] = __dmul_rn(wy, fy);
-                s_w[5 * chunk + t] = w;
+                buf[0 * chunk + t] = wx;
+                buf[1 * chunk + t] = wy;
+                buf[2 * chunk + t] = __dmul_rn(wx, fx);
+                buf[3 * chunk + t] = __dmul_rn(wx, fy);
+                buf[4 * chunk + t] = __dmul_rn(wy, fy);
+                buf[5 * chunk + t] = w;
             }
-            __syncthreads();
-            if (tid < 6) {
-                const double *src = s_w + tid * chunk;
-                double *o = mout + k0;
-                int64_t t = 0;
-                for (; t + 8 <= kn; t += 8) {
-                    double v[8];
+        };
+        // the prefix sums are taken in place in shared memory; the other
+        // warps copy a finished chunk out before staging into its buffer
+        auto copy_out = [&](int64_t k0, const double *buf, int first, int stride) {
+            const int64_t kn = dmin((int64_t)chunk, sz - k0);
+            for (int64_t t = first; t < 6 * kn; t += stride) {
+                const int64_t q = t / kn, i = t - q * kn;
+                M[q][k0 + i] = buf[q * chunk + i];
+            }
+        };
+        stage(0, s_w, tid, NT);
+        __syncthreads();
+        int64_t ch = 0;
+        for (int64_t k0 = 0; k0 < sz; k0 += chunk, ch++) {
+            double *cur = s_w + (ch & 1) * 6 * chunk, *oth = s_w + ((ch + 1) & 1) * 6 * chunk;
+            if (tid < 32) {
+                if (tid < 6) {
+                    const int64_t kn = dmin((int64_t)chunk, sz - k0);
+                    double *src = cur + tid * chunk;
+                    int64_t t = 0;
+                    // 16 loads, the 16 dependent additions, then 16 stores:
+                    // stores between the additions would lengthen the chain
+                    for (; t + 16 <= kn; t += 16) {
+                        double v[16];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) v[u] = src[t + u];
+                        for (int u = 0; u < 16; u++) v[u] = src[t + u];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        run = __dadd_rn(run, v[u]);
-                        o[t + u] = run;
+                        for (int u = 0; u < 16; u++) {
+                            run = __dadd_rn(run, v[u]);
+                            v[u] = run;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 16; u++) src[t + u] = v[u];
+                    }
+                    for (; t < kn; t++) {
+                        run = __dadd_rn(run, src[t]);
+                        src[t] = run;
                     }
                 }
-                for (; t < kn; t++) {
-                    run = __dadd_rn(run, src[t]);
-                    o[t] = run;
-                }
+            } else {
+                if (ch > 0) copy_out(k0 - chunk, oth, tid - 32, NT - 32);
+                asm volatile("bar.sync 1, %0;" ::"r"(NT - 32));
+                if (k0 + chunk < sz) stage(k0 + chunk, oth, tid - 32, NT - 32);
             }
             __syncthreads();
         }
+        if (ch > 0) copy_out((ch - 1) * chunk, s_w + ((ch - 1) & 1) * 6 * chunk, tid, NT);
+        __syncthreads();
         const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
         FIT_PROF(6)
 
@@ -1941,15 +1967,17 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             double *o = pm + lane * CAP;
             double run = 0.0;
             int t = 0;
-            for (; t + 8 <= n; t += 8) {
-                double v[8];
+            for (; t + 16 <= n; t += 16) {
+                double v[16];
 #pragma unroll
-                for (int u = 0; u < 8; u++) v[u] = o[t + u];
+                for (int u = 0; u < 16; u++) v[u] = o[t + u];
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < 16; u++) {
                     run = __dadd_rn(run, v[u]);
-                    o[t + u] = run;
+                    v[u] = run;
                 }
+#pragma unroll
+                for (int u = 0; u < 16; u++) o[t + u] = v[u];
             }
             for (; t < n; t++) {
                 run = __dadd_rn(run, o[t]);
