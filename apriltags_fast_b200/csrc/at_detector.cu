@@ -85,7 +85,7 @@ enum {
     B_RSTART, B_REND, B_RV, B_PARENT, B_PX, B_ROWRUNS, B_ROWPTS, B_ROWOFF,
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
-    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
+    B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_QNUM, B_FIRST, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -440,8 +440,6 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(cudaMemcpyAsync(&npts, row_off + rows, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     int64_t ncl = 0, nq = 0;
-    std::vector<GpuQuad> hq;
-    std::vector<int64_t> qstart(n + 1, 0);
     if (npts > 0) {
         CK(B[B_KEY].ensure(npts * 8));
         CK(B[B_VAL].ensure(npts * 8));
@@ -558,38 +556,22 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
             }))
             return false;
-        uint32_t last[2];
-        CK(cudaMemcpyAsync(&last[0], qscan + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&last[1], qok + ncl - 1, 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        nq = (int64_t)last[0] + last[1];
-        if (nq > 0) {
-            CK(B[B_QUADSC].ensure(nq * sizeof(GpuQuad)));
-            launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>());
-            in->launches += 1;
-            hq.resize(nq);
-            CK(cudaMemcpyAsync(hq.data(), B[B_QUADSC].p, nq * sizeof(GpuQuad), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-        }
-    }
-    CK(cudaEventRecord(in->ev[6], st));
-    in->last_npts = (int64_t)npts;
-    in->last_ncl = ncl;
-    in->last_nq = nq;
-    // quads are in cluster order, so grouped by frame
-    for (int64_t i = 0, f = 0; f <= n; f++) {
-        while (i < nq && hq[i].frame < f) i++;
-        qstart[f] = i;
-    }
-    for (int64_t f = 0; f < n; f++) res[f].nquads = qstart[f + 1] - qstart[f];
-    if (nq > 0) {
+        // the quads in cluster order (grouped by frame), their count and each
+        // frame's first quad stay on the device: decode is sized by ncl
+        CK(B[B_QUADSC].ensure(ncl * sizeof(GpuQuad)));
+        CK(B[B_QNUM].ensure(8));
+        uint32_t *nq_dev = B[B_QNUM].as<uint32_t>();
+        CK(cudaMemsetAsync(nq_dev, 0, 4, st));
+        launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>(), nq_dev);
+        in->launches += 1;
+        CK(cudaEventRecord(in->ev[6], st));
         // decode
         if (in->fam_dirty) {
             CK(in->dfam.ensure(sizeof(GpuFamily) * AT_MAX_FAMILIES));
             CK(cudaMemcpyAsync(in->dfam.p, in->gfam, sizeof(GpuFamily) * AT_MAX_FAMILIES, cudaMemcpyHostToDevice, st));
             in->fam_dirty = false;
         }
-        const int64_t nd = nq * in->nfam;
+        const int64_t nd = ncl * in->nfam;
         CK(B[B_DETS].ensure(nd * sizeof(GpuDetection)));
         CK(B[B_DETOK].ensure(nd * 4));
         CK(B[B_OUT].ensure(nd * sizeof(GpuDetection)));
@@ -598,30 +580,28 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_QSTART].ensure((n + 1) * 8));
         CK(B[B_OUTOFF].ensure((n + 1) * 8));
         CK(B[B_OUTN].ensure((n + 1) * 8));
-        CK(in->h_small.ensure((3 * n + 3) * 8));
-        int64_t *hs = in->h_small.as<int64_t>();
-        for (int64_t f = 0; f <= n; f++) {
-            hs[f] = qstart[f];
-            hs[n + 1 + f] = qstart[f] * in->nfam;
-        }
-        CK(cudaMemcpyAsync(B[B_QSTART].p, hs, (n + 1) * 8, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(B[B_OUTOFF].p, hs + n + 1, (n + 1) * 8, cudaMemcpyHostToDevice, st));
-        CK(B[B_QCORN].ensure(nq * 8 * sizeof(float)));
-        CK(B[B_QH].ensure(nq * 9 * sizeof(double)));
-        CK(B[B_QHOK].ensure(nq * sizeof(uint32_t)));
-        const DecodeScratch dscr{B[B_QCORN].as<float>(), B[B_QH].as<double>(), B[B_QHOK].as<uint32_t>()};
+        CK(B[B_FIRST].ensure((n + 1) * 8));
+        launch_frame_bounds(st, B[B_QUADSC].as<GpuQuad>(), nq_dev, (int)n, in->nfam, B[B_QSTART].as<int64_t>(),
+                            B[B_OUTOFF].as<int64_t>());
+        CK(B[B_QCORN].ensure(ncl * 8 * sizeof(float)));
+        CK(B[B_QH].ensure(ncl * 9 * sizeof(double)));
+        CK(B[B_QHOK].ensure(ncl * sizeof(uint32_t)));
+        const DecodeScratch dscr{B[B_QCORN].as<float>(), B[B_QH].as<double>(), B[B_QHOK].as<uint32_t>(), nq_dev};
         launch_decode(st, dfr, prm, in->dfam.as<GpuFamily>(), B[B_IMG].as<uint8_t>(), qim, B[B_QUADSC].as<GpuQuad>(),
-                      nq, dscr, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
+                      ncl, dscr, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
         CK(cudaEventRecord(in->ev[7], st));
         in->launches += 4;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
-                        B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
-                        B[B_OUTN].as<int64_t>());
+                        B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(), B[B_OUTN].as<int64_t>());
+        // the frames' detections and counts straight into pinned host memory
+        CK(in->h_out.ensure(nd * sizeof(GpuDetection) + 16));
+        CK(in->h_small.ensure((3 * n + 4) * 8));
+        launch_output(st, (int)n, B[B_QSTART].as<int64_t>(), B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
+                      B[B_OUTN].as<int64_t>(), B[B_FIRST].as<int64_t>(), in->h_out.as<GpuDetection>(),
+                      in->h_small.as<int64_t>());
+        in->launches += 3;
         CK(cudaGetLastError());
-        CK(in->h_out.ensure(nd * sizeof(GpuDetection)));
-        CK(cudaMemcpyAsync(hs + 2 * n + 2, B[B_OUTN].p, n * 8, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(in->h_out.p, B[B_OUT].p, nd * sizeof(GpuDetection), cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecord(in->ev[8], st));
         uint32_t derr = 0;
         CK(cudaMemcpyAsync(&derr, B[B_ERR].p, 4, cudaMemcpyDeviceToHost, st));
@@ -630,23 +610,22 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
             set_error(in, 3, "device check failed (code " + std::to_string(derr) + ")");
             return false;
         }
+        const int64_t *meta = in->h_small.as<int64_t>();
+        nq = meta[3 * n + 1];
         const GpuDetection *ho = in->h_out.as<GpuDetection>();
-        for (int64_t f = 0; f < n; f++) {
-            int64_t cnt = hs[2 * n + 2 + f];
-            res[f].first = (int64_t)in->dets.size();
-            res[f].count = cnt;
-            const GpuDetection *src = ho + qstart[f] * in->nfam;
-            for (int64_t k = 0; k < cnt; k++) {
-                at_detection d;
-                memcpy(&d, &src[k], sizeof d);
-                in->dets.push_back(d);
-            }
-        }
+        const int64_t total = meta[3 * n];
+        in->dets.resize(total);
+        if (total) memcpy(in->dets.data(), ho, total * sizeof(at_detection));
+        for (int64_t f = 0; f < n; f++) res[f] = at_frame_result{meta[3 * f], meta[3 * f + 1], meta[3 * f + 2]};
     } else {
+        CK(cudaEventRecord(in->ev[6], st));
         CK(cudaEventRecord(in->ev[7], st));
         CK(cudaEventRecord(in->ev[8], st));
         CK(cudaStreamSynchronize(st));
     }
+    in->last_npts = (int64_t)npts;
+    in->last_ncl = ncl;
+    in->last_nq = nq;
     // stage times from the events (at_timing, fast/apriltag_fast.h:67-69)
     auto dt = [&](int a, int b) {
         float ms = 0.0f;

@@ -2492,8 +2492,9 @@ __device__ uint32_t qd_lookup(const GpuFamily &F, uint64_t rcode, int lane) {
 
 __global__ void __launch_bounds__(AT_DEC_THREADS) k_refine(const FrameDesc *frames, GpuParams prm,
                                                               const uint8_t *img, const uint8_t *qim,
-                                                              const GpuQuad *quads, int64_t nquads, float *corners,
+                                                              const GpuQuad *quads, const uint32_t *nq, float *corners,
                                                               uint32_t *det_ok) {
+    const int64_t nquads = *nq;
     __shared__ float s_p[4][2];
     __shared__ double s_lines[4][4];
     __shared__ double s_bx[REF_CHUNK], s_by[REF_CHUNK];
@@ -2616,8 +2617,9 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_refine(const FrameDesc *fram
 // The homography of each quad's corners (fast/decode.c:114-196), a warp
 // per quad: H, and whether it was found and is invertible.
 #define QH_WARPS 4
-__global__ void __launch_bounds__(QH_WARPS * 32) k_quad_homography(const float *corners, int64_t nquads, double *hs,
+__global__ void __launch_bounds__(QH_WARPS * 32) k_quad_homography(const float *corners, const uint32_t *nq, double *hs,
                                                                      uint32_t *hok) {
+    const int64_t nquads = *nq;
     __shared__ float s_p[QH_WARPS][4][2];
     __shared__ double s_hm[QH_WARPS][72];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -2638,8 +2640,9 @@ __global__ void __launch_bounds__(QH_WARPS * 32) k_quad_homography(const float *
 __global__ void __launch_bounds__(AT_DEC_THREADS) k_decode(const FrameDesc *frames, GpuParams prm,
                                                               const GpuFamily *fams, const uint8_t *img,
                                                               const uint8_t *qim, const GpuQuad *quads,
-                                                              int64_t nquads, const double *hs, const uint32_t *hok,
+                                                              const uint32_t *nq, const double *hs, const uint32_t *hok,
                                                               GpuDetection *dets, uint32_t *det_ok) {
+    const int64_t nquads = *nq;
     __shared__ double s_H[9];
     __shared__ double s_gx[8 * AT_MAX_TW], s_gy[8 * AT_MAX_TW], s_gv[8 * AT_MAX_TW];
     __shared__ int s_gk[8 * AT_MAX_TW];
@@ -2975,10 +2978,65 @@ __global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, c
     if (threadIdx.x == 0) out_n[f] = total;
 }
 
+// The quads in cluster order (so grouped by frame), and their count.
 __global__ void k_gather_quads(const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                               GpuQuad *out) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+                               GpuQuad *out, uint32_t *nq) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         if (ok[i]) out[scan[i]] = quads[i];
+        if (i == n - 1) *nq = scan[i] + ok[i];
+    }
+}
+
+// Per frame: its first quad and its first detection slot (nfam per quad).
+__global__ void k_frame_bounds(const GpuQuad *quads, const uint32_t *nq, int nframes, int nfam, int64_t *qstart,
+                               int64_t *out_off) {
+    const int64_t n = *nq;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f <= nframes; f += gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (quads[mid].frame < f)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        qstart[f] = lo;
+        out_off[f] = lo * nfam;
+    }
+}
+
+// Each frame's detections, packed frame after frame into host memory
+// (mapped pinned), with meta[3 f ..] = (first, count, quads) per frame and
+// meta[3 n], meta[3 n + 1] = the totals of detections and quads. One block;
+// first (device scratch, a slot per frame) keeps the offsets on the device.
+__global__ void __launch_bounds__(256) k_output(int nframes, const int64_t *qstart, const GpuDetection *out,
+                                                const int64_t *out_off, const int64_t *out_n, int64_t *first,
+                                                GpuDetection *host, int64_t *meta) {
+    __shared__ uint32_t sh[32];
+    int64_t base = 0;
+    for (int f0 = 0; f0 < nframes; f0 += blockDim.x) {
+        const int f = f0 + threadIdx.x;
+        const uint32_t cnt = f < nframes ? (uint32_t)out_n[f] : 0u;
+        uint32_t total;
+        const uint32_t off = block_excl_scan(cnt, &total, sh);
+        if (f < nframes) {
+            first[f] = base + off;
+            meta[3 * f] = base + off;
+            meta[3 * f + 1] = cnt;
+            meta[3 * f + 2] = qstart[f + 1] - qstart[f];
+        }
+        base += total;
+    }
+    __syncthreads();
+    for (int f = 0; f < nframes; f++) {
+        const int64_t at = first[f], cnt = out_n[f];
+        const GpuDetection *src = out + out_off[f];
+        for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) host[at + k] = src[k];
+    }
+    if (threadIdx.x == 0) {
+        meta[3 * nframes] = base;
+        meta[3 * nframes + 1] = qstart[nframes];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -3122,21 +3180,33 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
 }
 
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                         GpuQuad *out) {
+                         GpuQuad *out, uint32_t *nq) {
     if (n <= 0) return;
-    k_gather_quads<<<flat_blocks(n, 256), 256, 0, s>>>(quads, ok, scan, n, out);
+    k_gather_quads<<<flat_blocks(n, 256), 256, 0, s>>>(quads, ok, scan, n, out, nq);
+}
+
+void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *nq, int nframes, int nfam,
+                         int64_t *qstart, int64_t *out_off) {
+    k_frame_bounds<<<flat_blocks(nframes + 1, 256), 256, 0, s>>>(quads, nq, nframes, nfam, qstart, out_off);
+}
+
+void launch_output(cudaStream_t s, int nframes, const int64_t *qstart, const GpuDetection *out,
+                   const int64_t *out_off, const int64_t *out_n, int64_t *first, GpuDetection *host,
+                   int64_t *meta) {
+    k_output<<<1, 256, 0, s>>>(nframes, qstart, out, out_off, out_n, first, host, meta);
 }
 
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
-                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads,
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t max_quads,
                    const DecodeScratch &scr, GpuDetection *dets, uint32_t *det_ok) {
-    if (nquads <= 0) return;
-    const unsigned blocks = (unsigned)(nquads < 148 * 64 ? nquads : 148 * 64);
-    k_refine<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, img, qim, quads, nquads, scr.corners, det_ok);
-    const int64_t hb = (nquads + QH_WARPS - 1) / QH_WARPS;
-    k_quad_homography<<<(unsigned)(hb < 148 * 16 ? hb : 148 * 16), QH_WARPS * 32, 0, s>>>(scr.corners, nquads,
+    // grids for at most max_quads quads; the kernels read the count (scr.nq)
+    if (max_quads <= 0) return;
+    const unsigned blocks = (unsigned)(max_quads < 148 * 64 ? max_quads : 148 * 64);
+    k_refine<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, img, qim, quads, scr.nq, scr.corners, det_ok);
+    const int64_t hb = (max_quads + QH_WARPS - 1) / QH_WARPS;
+    k_quad_homography<<<(unsigned)(hb < 148 * 16 ? hb : 148 * 16), QH_WARPS * 32, 0, s>>>(scr.corners, scr.nq,
                                                                                         scr.h, scr.hok);
-    k_decode<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, fams, img, qim, quads, nquads, scr.h, scr.hok, dets,
+    k_decode<<<blocks, AT_DEC_THREADS, 0, s>>>(frames, prm, fams, img, qim, quads, scr.nq, scr.h, scr.hok, dets,
                                                det_ok);
 }
 

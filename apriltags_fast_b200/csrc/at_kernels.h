@@ -67,16 +67,22 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                         GpuQuad *out);
+                         GpuQuad *out, uint32_t *nq);
+void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *nq, int nframes, int nfam,
+                         int64_t *qstart, int64_t *out_off);
+void launch_output(cudaStream_t s, int nframes, const int64_t *qstart, const GpuDetection *out,
+                   const int64_t *out_off, const int64_t *out_n, int64_t *first, GpuDetection *host,
+                   int64_t *meta);
 // per quad: refined corners (8 floats), homography (9 doubles), and whether
 // the homography was found and is invertible
 struct DecodeScratch {
     float *corners;
     double *h;
     uint32_t *hok;
+    const uint32_t *nq;  // the number of quads, on the device
 };
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
-                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t nquads,
+                   const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t max_quads,
                    const DecodeScratch &scr, GpuDetection *dets, uint32_t *det_ok);
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
