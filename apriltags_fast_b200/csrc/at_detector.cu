@@ -45,7 +45,7 @@ struct DBuf {
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        size_t want = bytes + bytes / 4 + 4096;
+        size_t want = bytes + bytes / 2 + 4096;  // grow with headroom: growth synchronises the device
         cudaError_t e = cudaMalloc(&p, want);
         if (e == cudaSuccess) cap = want;
         return e;
@@ -67,7 +67,7 @@ struct HBuf {
         if (p) cudaFreeHost(p);
         p = nullptr;
         cap = 0;
-        size_t want = bytes + bytes / 4 + 4096;
+        size_t want = bytes + bytes / 2 + 4096;  // grow with headroom: growth synchronises the device
         cudaError_t e = cudaMallocHost(&p, want);
         if (e == cudaSuccess) cap = want;
         return e;
@@ -599,8 +599,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(in->h_small.ensure((3 * n + 4) * 8));
         launch_output(st, (int)n, B[B_QSTART].as<int64_t>(), B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(),
                       B[B_OUTN].as<int64_t>(), B[B_FIRST].as<int64_t>(), in->h_out.as<GpuDetection>(),
-                      in->h_small.as<int64_t>());
-        in->launches += 3;
+                      in->h_small.as<int64_t>(), nd);
+        in->launches += 4;
         CK(cudaGetLastError());
         CK(cudaEventRecord(in->ev[8], st));
         uint32_t derr = 0;

@@ -1784,6 +1784,7 @@ __device__ __forceinline__ void leaf_of32(int n, int p, int &lo, int &len) {
     len = sz;
 }
 
+
 // Bitonic sort, ascending, of a warp's keys k[0, np) in shared memory (np
 // a power of two): log2(np) (log2(np) + 1) / 2 steps of np / 2 exchanges.
 __device__ void warp_bitonic(uint64_t *k, int np, int lane) {
@@ -1799,6 +1800,61 @@ __device__ void warp_bitonic(uint64_t *k, int np, int lane) {
             }
             __syncwarp();
         }
+    }
+}
+
+// Stable sort of a warp's n (32-bit key, 16-bit value) pairs by key: four
+// passes of 8 bits; equal digits keep their order (ranked by lane among 32
+// consecutive pairs, match_any). ka/va hold the input and get the result,
+// kb/vb are the second buffers, hist 256 counters.
+__device__ void warp_radix_sort32(uint32_t *ka, uint16_t *va, uint32_t *kb, uint16_t *vb, int n, uint32_t *hist,
+                                  int lane) {
+    for (int shift = 0; shift < 32; shift += 8) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) hist[lane * 8 + j] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) atomicAdd(hist + (ka[i] >> shift & 255u), 1u);
+        __syncwarp();
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            c[j] = hist[lane * 8 + j];
+            sum += c[j];
+        }
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        uint32_t run = incl - sum;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            hist[lane * 8 + j] = run;
+            run += c[j];
+        }
+        __syncwarp();
+        for (int i0 = 0; i0 < n; i0 += 32) {
+            const int i = i0 + lane;
+            const bool valid = i < n;
+            const uint32_t k = valid ? ka[i] : 0;
+            const int d = valid ? (int)(k >> shift & 255u) : 256 + lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t base = valid ? hist[d] : 0;
+            if (valid) {
+                const uint32_t at = base + __popc(peers & ((1u << lane) - 1u));
+                kb[at] = k;
+                vb[at] = va[i];
+            }
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) hist[d] = base + __popc(peers);
+            __syncwarp();
+        }
+        uint32_t *tk = ka;
+        ka = kb;
+        kb = tk;
+        uint16_t *tv = va;
+        va = vb;
+        vb = tv;
     }
 }
 
@@ -1899,41 +1955,98 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         const int rev = okrev >> 1;
         FITW_PROF(3)
 
-        // The angle sort (see k_fit_quads): position i of leaf (lo, len)
-        // takes place t = i - lo of the leaf's network order; its sort key
-        // packs the slope bits of its block head, 0xffff - the head's index,
-        // t, and (below the order, since the rest is distinct) the index of
-        // its point. The keys live in the last prefix array until the moments.
-        uint64_t *s_skey = reinterpret_cast<uint64_t *>(pm + 5 * CAP);
-        int np = 32;
-        while (np < n) np <<= 1;
-        for (int i = lane; i < np; i += 32) {
-            uint64_t key = ~0ull;
-            if (i < n) {
+        // The angle sort (see k_fit_quads). Up to 256 points: a bitonic
+        // sort of packed keys; above: the points laid out in (head index,
+        // place) order and a stable radix sort by the head's slope bits.
+        const uint16_t *s_order;  // point index of each sorted position
+        if constexpr (R <= 8) {
+            // The angle sort (see k_fit_quads): position i of leaf (lo, len)
+            // takes place t = i - lo of the leaf's network order; its sort key
+            // packs the slope bits of its block head, 0xffff - the head's index,
+            // t, and (below the order, since the rest is distinct) the index of
+            // its point. The keys live in the last prefix array until the moments.
+            uint64_t *s_skey = reinterpret_cast<uint64_t *>(pm + 5 * CAP);
+            int np = 32;
+            while (np < n) np <<= 1;
+            for (int i = lane; i < np; i += 32) {
+                uint64_t key = ~0ull;
+                if (i < n) {
+                    int lo, len;
+                    leaf_of32(n, i, lo, len);
+                    uint64_t a[5];
+    #pragma unroll
+                    for (int t = 0; t < 5; t++) a[t] = t < len ? s_akey[lo + t] : ~0ull;
+                    leaf_network(a, len);
+                    const int tp = i - lo;
+                    uint64_t head = a[0], e = a[0];
+    #pragma unroll
+                    for (int t = 1; t < 5; t++) {
+                        if (t <= tp) {
+                            if (a[t] > head) head = a[t];
+                            e = a[t];
+                        }
+                    }
+                    const uint32_t hidx = ~(uint32_t)head;
+                    key = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 16 | (uint64_t)tp << 13 |
+                          (uint64_t)(~(uint32_t)e & 0x1fffu);
+                }
+                s_skey[i] = key;
+            }
+            __syncwarp();
+            FITW_PROF(4)
+            warp_bitonic(s_skey, np, lane);
+            s_order = nullptr;
+        } else {
+            // The angle sort (see k_fit_quads): the points laid out in (head
+            // index descending, place) order, a lane per leaf, then a stable
+            // radix sort by the head's slope bits. The sort keys and indices
+            // live in region x1, their second buffers and the histogram in the
+            // prefix arrays (free until the moments).
+            uint32_t *s_ka = reinterpret_cast<uint32_t *>(x1);
+            uint16_t *s_va = reinterpret_cast<uint16_t *>(x1 + 4 * CAP);
+            uint32_t *s_kb = reinterpret_cast<uint32_t *>(pm);
+            uint16_t *s_vb = reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(pm) + 4 * CAP);
+            uint32_t *s_hist = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(pm) + 8 * CAP);
+            for (int p = lane; p < n; p += 32) {
                 int lo, len;
-                leaf_of32(n, i, lo, len);
+                leaf_of32(n, p, lo, len);
+                if (p != lo) continue;
                 uint64_t a[5];
-#pragma unroll
+    #pragma unroll
                 for (int t = 0; t < 5; t++) a[t] = t < len ? s_akey[lo + t] : ~0ull;
                 leaf_network(a, len);
-                const int tp = i - lo;
-                uint64_t head = a[0], e = a[0];
-#pragma unroll
-                for (int t = 1; t < 5; t++) {
-                    if (t <= tp) {
-                        if (a[t] > head) head = a[t];
-                        e = a[t];
+                uint32_t hid[5], hkey[5];
+                int bs[5];
+                uint64_t head = a[0];
+                int start = 0;
+    #pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    if (t > 0 && a[t] > head) {
+                        head = a[t];
+                        start = t;
                     }
+                    hid[t] = ~(uint32_t)head;
+                    hkey[t] = (uint32_t)(head >> 32);
+                    bs[t] = start;
                 }
-                const uint32_t hidx = ~(uint32_t)head;
-                key = (head & 0xffffffff00000000ull) | (uint64_t)(0xffffu - hidx) << 16 | (uint64_t)tp << 13 |
-                      (uint64_t)(~(uint32_t)e & 0x1fffu);
+                const int base = n - lo - len;
+    #pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    if (t >= len) continue;
+                    int before = 0;
+    #pragma unroll
+                    for (int t2 = 0; t2 < 5; t2++) before += t2 < len && hid[t2] > hid[t];
+                    const int pos = base + before + (t - bs[t]);
+                    s_ka[pos] = hkey[t];
+                    s_va[pos] = (uint16_t)~(uint32_t)a[t];
+                }
             }
-            s_skey[i] = key;
+            __syncwarp();
+            FITW_PROF(4)
+            warp_radix_sort32(s_ka, s_va, s_kb, s_vb, n, s_hist, lane);
+            __syncwarp();
+            s_order = s_va;
         }
-        __syncwarp();
-        FITW_PROF(4)
-        warp_bitonic(s_skey, np, lane);
         FITW_PROF(5)
 
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
@@ -1941,7 +2054,12 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         // turns array q into its prefix sums in place
         const uint8_t *im = qim + f.q_off;
         for (int k = lane; k < n; k += 32) {
-            const uint64_t p = P[s_skey[k] & 0x1fffu];
+            uint32_t src;
+            if constexpr (R <= 8)
+                src = (uint32_t)(reinterpret_cast<const uint64_t *>(pm + 5 * CAP)[k] & 0x1fffu);
+            else
+                src = s_order[k];
+            const uint64_t p = P[src];
             const int32_t px = (int32_t)(p & 0xffff), py = (int32_t)(p >> 16 & 0xffff);
             const int32_t ix = (px >> 1) + (px & 1), iy = (py >> 1) + (py & 1);
             int32_t g2 = 0;
@@ -3006,12 +3124,12 @@ __global__ void k_frame_bounds(const GpuQuad *quads, const uint32_t *nq, int nfr
 }
 
 // Each frame's detections, packed frame after frame into host memory
-// (mapped pinned), with meta[3 f ..] = (first, count, quads) per frame and
-// meta[3 n], meta[3 n + 1] = the totals of detections and quads. One block;
-// first (device scratch, a slot per frame) keeps the offsets on the device.
-__global__ void __launch_bounds__(256) k_output(int nframes, const int64_t *qstart, const GpuDetection *out,
-                                                const int64_t *out_off, const int64_t *out_n, int64_t *first,
-                                                GpuDetection *host, int64_t *meta) {
+// (mapped pinned). k_output_meta (one block): meta[3 f ..] = (first, count,
+// quads) per frame, meta[3 n], meta[3 n + 1] = the totals of detections and
+// quads, and the offsets again on the device (first, with the total last).
+// k_output_copy: a warp per detection, its 21 words in one coalesced write.
+__global__ void __launch_bounds__(256) k_output_meta(int nframes, const int64_t *qstart, const int64_t *out_n,
+                                                     int64_t *first, int64_t *meta) {
     __shared__ uint32_t sh[32];
     int64_t base = 0;
     for (int f0 = 0; f0 < nframes; f0 += blockDim.x) {
@@ -3027,15 +3145,31 @@ __global__ void __launch_bounds__(256) k_output(int nframes, const int64_t *qsta
         }
         base += total;
     }
-    __syncthreads();
-    for (int f = 0; f < nframes; f++) {
-        const int64_t at = first[f], cnt = out_n[f];
-        const GpuDetection *src = out + out_off[f];
-        for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x) host[at + k] = src[k];
-    }
     if (threadIdx.x == 0) {
+        first[nframes] = base;
         meta[3 * nframes] = base;
         meta[3 * nframes + 1] = qstart[nframes];
+    }
+}
+
+__global__ void k_output_copy(int nframes, const GpuDetection *out, const int64_t *out_off, const int64_t *first,
+                              GpuDetection *host) {
+    constexpr int W = (int)(sizeof(GpuDetection) / 8);
+    const int lane = threadIdx.x & 31;
+    const int64_t total = first[nframes];
+    for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < total;
+         j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int lo = 0, hi = nframes - 1;  // the frame holding detection j
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= j)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint64_t *src = reinterpret_cast<const uint64_t *>(out + out_off[lo] + (j - first[lo]));
+        uint64_t *dst = reinterpret_cast<uint64_t *>(host + j);
+        if (lane < W) dst[lane] = src[lane];
     }
 }
 
@@ -3192,8 +3326,11 @@ void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *n
 
 void launch_output(cudaStream_t s, int nframes, const int64_t *qstart, const GpuDetection *out,
                    const int64_t *out_off, const int64_t *out_n, int64_t *first, GpuDetection *host,
-                   int64_t *meta) {
-    k_output<<<1, 256, 0, s>>>(nframes, qstart, out, out_off, out_n, first, host, meta);
+                   int64_t *meta, int64_t max_dets) {
+    k_output_meta<<<1, 256, 0, s>>>(nframes, qstart, out_n, first, meta);
+    const int64_t blocks = (max_dets + 7) / 8;
+    k_output_copy<<<(unsigned)(blocks < 1 ? 1 : blocks < 148 * 4 ? blocks : 148 * 4), 256, 0, s>>>(nframes, out, out_off,
+                                                                                                first, host);
 }
 
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,

@@ -72,7 +72,7 @@ void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *n
                          int64_t *qstart, int64_t *out_off);
 void launch_output(cudaStream_t s, int nframes, const int64_t *qstart, const GpuDetection *out,
                    const int64_t *out_off, const int64_t *out_n, int64_t *first, GpuDetection *host,
-                   int64_t *meta);
+                   int64_t *meta, int64_t max_dets);
 // per quad: refined corners (8 floats), homography (9 doubles), and whether
 // the homography was found and is invertible
 struct DecodeScratch {
