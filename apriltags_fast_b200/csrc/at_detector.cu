@@ -101,9 +101,9 @@ struct at_internal {
     bool fam_dirty = true;
 
     int device = 0;
-    cudaStream_t stream = nullptr, side = nullptr, side2 = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr, side2 = nullptr, side3 = nullptr;
     cudaEvent_t ev[12];
-    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;  // ordering only, no timing
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr, join3 = nullptr;  // ordering only, no timing
     DBuf buf[B_NBUF];
     HBuf h_frames, h_small, h_out;
     std::vector<at_detection> dets;
@@ -357,7 +357,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         return false;
     }
     const int nb = bits_for((uint64_t)nodes);
-    Launch L{st, (int)n, 0};
+    Launch L{st, (int)n, 0, 0};
+    for (auto &f : fd) L.max_qh = f.qh > L.max_qh ? f.qh : L.max_qh;
     int64_t maxq = 0;
     for (auto &f : fd) maxq = f.qw * (int64_t)f.qh > maxq ? f.qw * (int64_t)f.qh : maxq;
     L.blocks_per_frame = (int)((maxq + 255) / 256 < 148 * 4 ? (maxq + 255) / 256 : 148 * 4);
@@ -548,7 +549,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                        B[B_SERRS].as<double>(),   B[B_SFILT].as<double>(),  B[B_SMXE].as<double>(),
                        B[B_SMXI].as<int32_t>(),   B[B_FLIST].as<uint32_t>(), B[B_FCNT].as<uint32_t>()};
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
-        launch_fit_quads(st, in->side, in->side2, in->fork, in->join, in->join2, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
+        launch_fit_quads(st, in->side, in->side2, in->side3, in->fork, in->join, in->join2, in->join3, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
         in->launches += 7;
         CK(cudaGetLastError());
@@ -686,9 +687,11 @@ at_detector *at_detector_create(void) {
     for (int k = 0; k < 12; k++) cudaEventCreate(&in->ev[k]);
     cudaStreamCreateWithFlags(&in->side, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&in->side2, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&in->side3, cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&in->fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&in->join, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&in->join2, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&in->join3, cudaEventDisableTiming);
     return td;
 }
 
@@ -717,8 +720,10 @@ void at_detector_destroy(at_detector *td) {
     cudaEventDestroy(in->fork);
     cudaEventDestroy(in->join);
     cudaEventDestroy(in->join2);
+    cudaEventDestroy(in->join3);
     cudaStreamDestroy(in->side);
     cudaStreamDestroy(in->side2);
+    cudaStreamDestroy(in->side3);
     cudaStreamDestroy(in->stream);
     delete in;
     free(td);

@@ -323,62 +323,56 @@ __device__ __forceinline__ bool runs_touch(int64_t a0, int64_t a1, int64_t b0, i
 
 __global__ void __launch_bounds__(256) k_row_runs(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                                                   uint32_t *row_nruns) {
-    __shared__ __align__(16) uint8_t s_row[ROW_STAGE + 16];
+    // a warp per row: runs of equal value over columns [0, qw - 2], 32
+    // columns at a time (ballots of run starts), 127 runs not stored
     const FrameDesc f = frames[blockIdx.y];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    for (int64_t y = blockIdx.x; y < f.qh; y += gridDim.x) {
-        const uint8_t *t = thr + f.q_off + y * f.qw;
+    const int64_t wpb = blockDim.x >> 5;
+    for (int64_t y = blockIdx.x * wpb + (threadIdx.x >> 5); y < f.qh; y += gridDim.x * wpb) {
+        const uint8_t *row = thr + f.q_off + y * f.qw;
         const int64_t base = f.node_off + y * f.qw;
         const int64_t xmax = f.qw - 2;
-        const bool staged = f.qw <= ROW_STAGE;
-        __syncthreads();
-        if (staged)
-            for (int64_t x = threadIdx.x; x < f.qw; x += blockDim.x) s_row[x] = t[x];
-        __syncthreads();
-        const uint8_t *row = staged ? s_row : t;
-        if (warp == 0) {
-            int64_t count = 0, open = -1;
-            for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
-                int64_t x = x0 + lane;
-                bool valid = x <= xmax;
-                uint8_t v = valid ? row[x] : 0;
-                bool start = valid && (x == 0 || row[x - 1] != v);
-                uint32_t S = __ballot_sync(0xffffffffu, start);
-                uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
-                if (start) {
-                    uint32_t below = S & lt;
-                    int64_t prev_slot;
-                    if (below) {
-                        int pl = 31 - __clz(below);
-                        prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
-                    } else {
-                        prev_slot = open;
-                    }
-                    if (prev_slot >= 0) runs.end[base + prev_slot] = (uint16_t)(x - 1);
-                    if (v != 127) {
-                        int64_t sl = base + count + __popc(N & lt);
-                        runs.start[sl] = (uint16_t)x;
-                        runs.v[sl] = v;
-                        runs.parent[sl] = (uint32_t)sl;
-                        runs.px[sl] = 0;
-                        runs.minid[sl] = 0xffffffffu;
-                    }
+        int64_t count = 0, open = -1;
+        for (int64_t x0 = 0; x0 <= xmax; x0 += 32) {
+            int64_t x = x0 + lane;
+            bool valid = x <= xmax;
+            uint8_t v = valid ? row[x] : 0;
+            bool start = valid && (x == 0 || row[x - 1] != v);
+            uint32_t S = __ballot_sync(0xffffffffu, start);
+            uint32_t N = __ballot_sync(0xffffffffu, start && v != 127);
+            if (start) {
+                uint32_t below = S & lt;
+                int64_t prev_slot;
+                if (below) {
+                    int pl = 31 - __clz(below);
+                    prev_slot = (N >> pl & 1u) ? count + __popc(N & ((1u << pl) - 1u)) : -1;
+                } else {
+                    prev_slot = open;
                 }
-                if (S) {
-                    int ls = 31 - __clz(S);
-                    open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
+                if (prev_slot >= 0) runs.end[base + prev_slot] = (uint16_t)(x - 1);
+                if (v != 127) {
+                    int64_t sl = base + count + __popc(N & lt);
+                    runs.start[sl] = (uint16_t)x;
+                    runs.v[sl] = v;
+                    runs.parent[sl] = (uint32_t)sl;
+                    runs.px[sl] = 0;
+                    runs.minid[sl] = 0xffffffffu;
                 }
-                count += __popc(N);
             }
-            if (lane == 0) {
-                if (open >= 0) runs.end[base + open] = (uint16_t)xmax;
-                row_nruns[f.row0 + y] = (uint32_t)count;
-                int64_t vn = f.node_off + (int64_t)f.qw * f.qh + y;
-                runs.parent[vn] = (uint32_t)vn;
-                runs.px[vn] = 0;
-                runs.minid[vn] = 0xffffffffu;
+            if (S) {
+                int ls = 31 - __clz(S);
+                open = (N >> ls & 1u) ? count + __popc(N & ((1u << ls) - 1u)) : -1;
             }
+            count += __popc(N);
+        }
+        if (lane == 0) {
+            if (open >= 0) runs.end[base + open] = (uint16_t)xmax;
+            row_nruns[f.row0 + y] = (uint32_t)count;
+            int64_t vn = f.node_off + (int64_t)f.qw * f.qh + y;
+            runs.parent[vn] = (uint32_t)vn;
+            runs.px[vn] = 0;
+            runs.minid[vn] = 0xffffffffu;
         }
     }
 }
@@ -578,7 +572,9 @@ __device__ __forceinline__ uint32_t point_mask(const uint8_t *a, const uint8_t *
 }
 
 
-__global__ void k_point_count(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, uint64_t *row_npts) {
+// Block-per-row forms of the point passes (a block scan per 256 columns),
+// for batches too small to fill the GPU with a warp per row.
+__global__ void k_point_count_block(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, uint64_t *row_npts) {
     __shared__ uint32_t sh[32];
     const FrameDesc f = frames[blockIdx.y];
     for (int64_t y = blockIdx.x; y < f.qh; y += gridDim.x) {
@@ -594,9 +590,7 @@ __global__ void k_point_count(const FrameDesc *frames, const uint8_t *thr, const
     }
 }
 
-// The cluster key of a point: (larger label, smaller label) packed as
-// larger << nb | smaller, nb = bits of the largest node id.
-__global__ void k_point_emit(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+__global__ void k_point_emit_block(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                              const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb) {
     __shared__ uint32_t sh[32];
     const FrameDesc f = frames[blockIdx.y];
@@ -628,6 +622,76 @@ __global__ void k_point_emit(const FrameDesc *frames, const uint8_t *thr, const 
     }
 }
 
+// A warp per row for both passes: the row's points counted, then emitted
+// in (x, neighbour) order at the row's offset (warp scans, no block
+// barriers).
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t *total) {
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    *total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - v;
+}
+
+__global__ void __launch_bounds__(256) k_point_count(const FrameDesc *frames, const uint8_t *thr,
+                                                     const uint32_t *lab, uint64_t *row_npts) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int64_t wpb = blockDim.x >> 5;
+    for (int64_t y = blockIdx.x * wpb + (threadIdx.x >> 5); y < f.qh; y += gridDim.x * wpb) {
+        uint32_t cnt = 0;
+        if (y >= 1 && y + 1 < f.qh) {
+            const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;
+            const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+            for (int64_t x = lane; x < f.qw; x += 32) cnt += __popc(point_mask(a, b, la, lb, x, f.qw));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0) row_npts[f.row0 + y] = cnt;
+    }
+}
+
+// The cluster key of a point: (larger label, smaller label) packed as
+// larger << nb | smaller, nb = bits of the largest node id.
+__global__ void __launch_bounds__(256) k_point_emit(const FrameDesc *frames, const uint8_t *thr,
+                                                    const uint32_t *lab, const uint64_t *row_pt_off,
+                                                    uint64_t *pt_key, uint64_t *pt_val, int nb) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int64_t wpb = blockDim.x >> 5;
+    for (int64_t y = 1 + blockIdx.x * wpb + (threadIdx.x >> 5); y + 1 < f.qh; y += gridDim.x * wpb) {
+        const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;
+        const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+        uint64_t out = row_pt_off[f.row0 + y];
+        for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
+            const int64_t x = x0 + lane;
+            const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
+            uint32_t total;
+            const uint32_t off = warp_excl_scan(__popc(m), &total);
+            uint64_t o = out + off;
+            const int g = a[x < f.qw ? x : 0] == 0 ? 255 : -255;
+            for (int j = 0; j < 4; j++) {
+                if (!(m >> j & 1u)) continue;
+                const int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0;
+                const int dy = j == 0 ? 0 : 1;
+                const uint32_t l0 = la[x], l1 = dy ? lb[x + dx] : la[x + dx];
+                const uint64_t hi = l0 > l1 ? l0 : l1, lo = l0 > l1 ? l1 : l0;
+                const uint64_t px = (uint64_t)(2 * x + dx), py = (uint64_t)(2 * y + dy);
+                const uint64_t gx = (uint16_t)(int16_t)(dx * g), gy = (uint16_t)(int16_t)(dy * g);
+                pt_key[o] = hi << nb | lo;
+                pt_val[o] = px | py << 16 | gx << 32 | gy << 48;
+                o++;
+            }
+            out += total;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // 7. Clusters, by hashing (fast/clusters.c:318-382 groups points by their
 // label pair in a hash table too). The distinct pairs go into an
 // open-addressing table (each warp inserts each distinct pair of its 32
@@ -1748,8 +1812,10 @@ __host__ __device__ constexpr int binom4(int n) { return n < 4 ? 0 : n * (n - 1)
 __host__ __device__ constexpr size_t fit_warp_x1(int cap, int mm) {
     return (size_t)8 * cap > (size_t)32 * mm * mm ? (size_t)8 * cap : (size_t)32 * mm * mm;
 }
-__host__ __device__ constexpr size_t fit_warp_smem(int cap, int mm) {
-    return (size_t)56 * cap + fit_warp_x1(cap, mm);
+// gp: the prefix arrays in global scratch (the largest warp class, where
+// 48 B per point of shared memory would leave few warps per SM)
+__host__ __device__ constexpr size_t fit_warp_smem(int cap, int mm, bool gp = false) {
+    return (size_t)(gp ? 8 : 56) * cap + fit_warp_x1(cap, mm);
 }
 
 // The leaf of position p of n (see leaf_of), in 32-bit arithmetic.
@@ -1863,14 +1929,15 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
                                                           const uint64_t *pts, const uint32_t *cstart,
                                                           const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                           const uint32_t *list, const uint32_t *count,
-                                                          GpuQuad *quads, uint32_t *quad_ok, int mm) {
+                                                          GpuQuad *quads, uint32_t *quad_ok, int mm, FitScratch scr) {
     constexpr int CAP = 32 * R;
+    constexpr bool GP = R >= 16;  // prefix arrays in global scratch
     extern __shared__ __align__(16) unsigned char fw_smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
-    unsigned char *base = fw_smem + fit_warp_smem(CAP, mm) * wid;
-    double *pm = reinterpret_cast<double *>(base);  // prefix array q at pm + q * CAP
-    unsigned char *x0 = base + 48 * CAP, *x1 = x0 + 8 * CAP;
+    unsigned char *base = fw_smem + fit_warp_smem(CAP, mm, GP) * wid;
+    double *pm = reinterpret_cast<double *>(base);  // prefix array q at pm + q * CAP (not GP)
+    unsigned char *x0 = base + (GP ? 0 : 48 * CAP), *x1 = x0 + 8 * CAP;
     uint64_t *s_akey = reinterpret_cast<uint64_t *>(x0);
     double *s_err = reinterpret_cast<double *>(x0);
     double *s_mxe = reinterpret_cast<double *>(x0);
@@ -2004,9 +2071,13 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             // prefix arrays (free until the moments).
             uint32_t *s_ka = reinterpret_cast<uint32_t *>(x1);
             uint16_t *s_va = reinterpret_cast<uint16_t *>(x1 + 4 * CAP);
-            uint32_t *s_kb = reinterpret_cast<uint32_t *>(pm);
-            uint16_t *s_vb = reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(pm) + 4 * CAP);
-            uint32_t *s_hist = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(pm) + 8 * CAP);
+            // second buffers: in x0 once the angle keys are read (GP: x0
+            // holds 8 B per point of capacity, 4 + 2 for the buffers and
+            // 1 KB for the histogram)
+            unsigned char *sb = GP ? x0 : reinterpret_cast<unsigned char *>(pm);
+            uint32_t *s_kb = reinterpret_cast<uint32_t *>(sb);
+            uint16_t *s_vb = reinterpret_cast<uint16_t *>(sb + 4 * CAP);
+            uint32_t *s_hist = reinterpret_cast<uint32_t *>(sb + (GP ? 6 : 8) * CAP);
             for (int p = lane; p < n; p += 32) {
                 int lo, len;
                 leaf_of32(n, p, lo, len);
@@ -2052,6 +2123,9 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         // cumulative weighted moments in angle order (fast/quads.c:968-1035):
         // every lane stages the six terms of its positions, then lane q < 6
         // turns array q into its prefix sums in place
+        double *M0 = GP ? scr.mx + s0 : pm, *M1 = GP ? scr.my + s0 : pm + CAP, *M2 = GP ? scr.mxx + s0 : pm + 2 * CAP,
+               *M3 = GP ? scr.mxy + s0 : pm + 3 * CAP, *M4 = GP ? scr.myy + s0 : pm + 4 * CAP,
+               *M5 = GP ? scr.mw + s0 : pm + 5 * CAP;
         const uint8_t *im = qim + f.q_off;
         for (int k = lane; k < n; k += 32) {
             uint32_t src;
@@ -2073,16 +2147,16 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             const double fx = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
             const double fy = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
             const double wx = __dmul_rn(w, fx), wy = __dmul_rn(w, fy);
-            pm[0 * CAP + k] = wx;
-            pm[1 * CAP + k] = wy;
-            pm[2 * CAP + k] = __dmul_rn(wx, fx);
-            pm[3 * CAP + k] = __dmul_rn(wx, fy);
-            pm[4 * CAP + k] = __dmul_rn(wy, fy);
-            pm[5 * CAP + k] = w;
+            M0[k] = wx;
+            M1[k] = wy;
+            M2[k] = __dmul_rn(wx, fx);
+            M3[k] = __dmul_rn(wx, fy);
+            M4[k] = __dmul_rn(wy, fy);
+            M5[k] = w;
         }
         __syncwarp();
         if (lane < 6) {
-            double *o = pm + lane * CAP;
+            double *o = lane == 0 ? M0 : lane == 1 ? M1 : lane == 2 ? M2 : lane == 3 ? M3 : lane == 4 ? M4 : M5;
             double run = 0.0;
             int t = 0;
             for (; t + 16 <= n; t += 16) {
@@ -2104,7 +2178,7 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         }
         __syncwarp();
         FITW_PROF(6)
-        const Moments mo = {pm, pm + CAP, pm + 2 * CAP, pm + 3 * CAP, pm + 4 * CAP, pm + 5 * CAP};
+        const Moments mo = {M0, M1, M2, M3, M4, M5};
 
         // corner search (fast/quads.c:788-959)
         const int ksz = min(20, n / 12);
@@ -3177,6 +3251,14 @@ __global__ void k_output_copy(int nframes, const GpuDetection *out, const int64_
 // Launchers.
 
 static inline dim3 frame_grid(const Launch &L) { return dim3((unsigned)L.blocks_per_frame, (unsigned)L.nframes); }
+// a warp per row when the batch has rows enough to fill the GPU with warps
+// (16 per SM), else a block per row (lower latency for a few frames)
+static inline bool warp_rows(const Launch &L) { return (int64_t)L.nframes * L.max_qh >= 148 * 16; }
+// a warp per row, 8 rows a block
+static inline dim3 row_warp_grid(const Launch &L) {
+    const int64_t b = (L.max_qh + 7) / 8;
+    return dim3((unsigned)(b < 1 ? 1 : b < 148 * 8 ? b : 148 * 8), (unsigned)L.nframes);
+}
 static inline unsigned flat_blocks(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -3209,7 +3291,9 @@ void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uin
 int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
                    uint32_t *lab, int32_t min_px, int64_t max_qh) {
     dim3 rg((unsigned)(max_qh < 148 * 16 ? max_qh : 148 * 16), (unsigned)L.nframes);
-    k_row_runs<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    const int64_t rb = (max_qh + 7) / 8;
+    k_row_runs<<<dim3((unsigned)(rb < 148 * 8 ? rb : 148 * 8), (unsigned)L.nframes), 256, 0, L.stream>>>(frames, thr,
+                                                                                                        runs, row_nruns);
     k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
     k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
     k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
@@ -3218,12 +3302,18 @@ int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr,
 
 void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                         uint64_t *row_npts) {
-    k_point_count<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_npts);
+    if (warp_rows(L))
+        k_point_count<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_npts);
+    else
+        k_point_count_block<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_npts);
 }
 
 void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                        const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb) {
-    k_point_emit<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
+    if (warp_rows(L))
+        k_point_emit<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
+    else
+        k_point_emit_block<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
 }
 
 void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount,
@@ -3263,18 +3353,18 @@ template <int R>
 static void launch_fit_warp(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                             const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                             int64_t npoints, const FitScratch &scr, int q, GpuQuad *quads, uint32_t *quad_ok, int mm) {
-    const size_t wsm = fit_warp_smem(32 * R, mm) * FIT_WPB;
+    const size_t wsm = fit_warp_smem(32 * R, mm, R >= 16) * FIT_WPB;
     cudaFuncSetAttribute(k_fit_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
     const int64_t per_sm = (int64_t)(225 * 1024 / (wsm + 1024));
     const int64_t full = 148 * (per_sm < 1 ? 1 : per_sm > 32 ? 32 : per_sm);
     const int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
     k_fit_warp<R><<<(unsigned)(wb < full ? wb : full), FIT_WPB * 32, wsm, s>>>(
         frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr.lists + (int64_t)q * nclusters,
-        scr.counts + q, quads, quad_ok, mm);
+        scr.counts + q, quads, quad_ok, mm, scr);
 }
 
-void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
-                      cudaEvent_t join2, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaStream_t side3, cudaEvent_t fork,
+                      cudaEvent_t join, cudaEvent_t join2, cudaEvent_t join3, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
     if (nclusters <= 0) return;
@@ -3290,27 +3380,30 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
                                                                 prm.min_cluster_pixels, quad_ok, scr.lists,
                                                                 scr.counts);
     k_fit_order<<<2, 1024, FIT_ORDER_CAP * 8, s>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 3);
-    // three streams: the large clusters (a block of 512 each); the middle
-    // ones (a warp each up to 512 points, then a block of 128); the many
-    // small ones (a warp each)
+    // four streams, one per group of classes: the large clusters (a block
+    // of 512 each); 513-1024 points (a block of 128); 257-512 (a warp each);
+    // up to 256 (a warp each)
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     cudaStreamWaitEvent(side2, fork, 0);
+    cudaStreamWaitEvent(side3, fork, 0);
     const unsigned nbig = (unsigned)(nclusters < 148 ? nclusters : 148);
     k_fit_quads<512><<<nbig, 512, large, side>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
                                                  quads, quad_ok, err, scr.lists + 4 * nclusters, scr.counts + 4,
                                                  scr.counts + FIT_NCLASS + 4, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaEventRecord(join, side);
-    launch_fit_warp<16>(side2, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 2, quads, quad_ok, mm);
     const unsigned mid = (unsigned)(nclusters < 148 * 4 ? nclusters : 148 * 4);
     k_fit_quads<128><<<mid, 128, small, side2>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
                                                  quads, quad_ok, err, scr.lists + 3 * nclusters, scr.counts + 3,
                                                  scr.counts + FIT_NCLASS + 3, FIT_SMALL, FIT_CHUNK_SMALL);
     cudaEventRecord(join2, side2);
+    launch_fit_warp<16>(side3, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 2, quads, quad_ok, mm);
+    cudaEventRecord(join3, side3);
     launch_fit_warp<4>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 0, quads, quad_ok, mm);
     launch_fit_warp<8>(s, frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr, 1, quads, quad_ok, mm);
     cudaStreamWaitEvent(s, join, 0);
     cudaStreamWaitEvent(s, join2, 0);
+    cudaStreamWaitEvent(s, join3, 0);
 }
 
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,

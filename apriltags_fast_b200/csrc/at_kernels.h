@@ -36,6 +36,7 @@ struct Launch {
     cudaStream_t stream;
     int nframes;
     int blocks_per_frame;
+    int64_t max_qh;  // the tallest quad image of the batch
 };
 
 void launch_decimate(const Launch &L, const FrameDesc *frames, const uint8_t *img, uint8_t *qim, float factor);
@@ -62,8 +63,8 @@ void launch_cluster_assign(cudaStream_t s, const uint64_t *key, int64_t n, const
                            const uint32_t *rank_of_slot, uint32_t *cidx);
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
                            int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe);
-void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaEvent_t fork, cudaEvent_t join,
-                      cudaEvent_t join2, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
+void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaStream_t side3, cudaEvent_t fork,
+                      cudaEvent_t join, cudaEvent_t join2, cudaEvent_t join3, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
