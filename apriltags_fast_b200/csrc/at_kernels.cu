@@ -2468,6 +2468,62 @@ __device__ bool refine_sample(const DView &v, double x0, double y0, double nx, d
     return true;
 }
 
+// Lane u's share of one sample's first vsteps steps (a multiple of 4): the
+// steps k = u, u + 4, ..., summed in that order into (ln, lc), which is
+// partial sum u of refine_sample, so four lanes give its four sums.
+__device__ __forceinline__ void refine_part(const DView &v, double x0, double y0, double nx, double ny, int64_t range,
+                                            int64_t vsteps, int u, double *ln, double *lc) {
+    const double wl = (double)(v.w - 1), hl = (double)(v.h - 1);
+    const bool tiny = v.w < 2 || v.h < 2;
+    double sn = 0.0, sc = 0.0;
+#pragma unroll 3
+    for (int64_t k = u; k < vsteps; k += 4) {
+        const double n = (double)-range + 0.25 * (double)k;
+        const double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
+        const double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
+        const bool in = x1 > -1.0 && x1 < wl && y1 > -1.0 && y1 < hl && x2 > -1.0 && x2 < wl && y2 > -1.0 && y2 < hl;
+        const double tx1 = trunc(x1), ty1 = trunc(y1), tx2 = trunc(x2), ty2 = trunc(y2);
+        double wgt = 0.0;
+        if (in || !tiny) {
+            const uint8_t *p1 = v.im + (in ? (int64_t)ty1 * v.s + (int64_t)tx1 : 0);
+            const uint8_t *p2 = v.im + (in ? (int64_t)ty2 * v.s + (int64_t)tx2 : 0);
+            const int a0 = p1[0], a1 = p1[1], a2 = p1[v.s], a3 = p1[v.s + 1];
+            const int b0 = p2[0], b1 = p2[1], b2 = p2[v.s], b3 = p2[v.s + 1];
+            if (in) {
+                const double g1 = bil_vals(x1 - tx1, y1 - ty1, a0, a1, a2, a3);
+                const double g2 = bil_vals(x2 - tx2, y2 - ty2, b0, b1, b2, b3);
+                const double d = g2 - g1;
+                wgt = !(g1 < g2) ? d * d : 0.0;
+            }
+        }
+        sn = sn + wgt * n;
+        sc = sc + wgt;
+    }
+    *ln = sn;
+    *lc = sc;
+}
+
+// The steps after the first vsteps of one sample, in order, added to the
+// sums (mn, mc) (the tail of refine_sample).
+__device__ __forceinline__ void refine_tail(const DView &v, double x0, double y0, double nx, double ny, int64_t range,
+                                            int64_t vsteps, int64_t nsteps, double *mn, double *mc) {
+    for (int64_t k = vsteps; k < nsteps; k++) {
+        double n = (double)-range + 0.25 * (double)k;
+        double x1 = x0 + (n + 1.0) * nx - 0.5, y1 = y0 + (n + 1.0) * ny - 0.5;
+        int64_t x1i = c_int(x1), y1i = c_int(y1);
+        if (x1i < 0 || x1i + 1 >= v.w || y1i < 0 || y1i + 1 >= v.h) continue;
+        double x2 = x0 + (n - 1.0) * nx - 0.5, y2 = y0 + (n - 1.0) * ny - 0.5;
+        int64_t x2i = c_int(x2), y2i = c_int(y2);
+        if (x2i < 0 || x2i + 1 >= v.w || y2i < 0 || y2i + 1 >= v.h) continue;
+        double g1 = bil_seq(x1 - (double)x1i, y1 - (double)y1i, v.im + y1i * v.s + x1i, v.s);
+        double g2 = bil_seq(x2 - (double)x2i, y2 - (double)y2i, v.im + y2i * v.s + x2i, v.s);
+        if (g1 < g2) continue;
+        double wgt = (g2 - g1) * (g2 - g1);
+        *mn = *mn + wgt * n;
+        *mc = *mc + wgt;
+    }
+}
+
 // Correctly rounded f32 trig as the golden vectors need: the double
 // function, then one rounding (fast/decode.c:740-744).
 __device__ __forceinline__ float cr_atan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
@@ -2737,22 +2793,39 @@ __global__ void __launch_bounds__(AT_DEC_THREADS) k_refine(const FrameDesc *fram
             const int64_t o1 = s_ens[0], o2 = o1 + s_ens[1], o3 = o2 + s_ens[2], total = o3 + s_ens[3];
             double mx = 0.0, my = 0.0, mxx = 0.0, mxy = 0.0, myy = 0.0, cnt = 0.0;
             for (int64_t c0 = 0; c0 < total; c0 += REF_CHUNK) {
-                for (int w = tid; w < REF_CHUNK; w += blockDim.x) {
+                // four lanes per sample, lane u summing partial sum u
+                const int u = tid & 3;
+                for (int w0 = 0; w0 < REF_CHUNK; w0 += (int)(blockDim.x >> 2)) {
+                    const int w = w0 + (tid >> 2);
                     const int64_t gi = c0 + w;
-                    if (gi >= total) continue;
-                    const int e = gi < o1 ? 0 : gi < o2 ? 1 : gi < o3 ? 2 : 3;
-                    const int64_t si = gi - (e == 0 ? 0 : e == 1 ? o1 : e == 2 ? o2 : o3), ns = s_ens[e];
-                    const int a = e, b = (e + 1) & 3;
-                    const double nx = s_enx[e], ny = s_eny[e];
-                    double alpha = (1.0 + (double)si) / (double)(ns + 1);
-                    double x0 = alpha * (double)s_p[a][0] + (1.0 - alpha) * (double)s_p[b][0];
-                    double y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
-                    double n0;
-                    bool ok = refine_sample(v, x0, y0, nx, ny, range, vsteps, nsteps, &n0);
-                    s_bok[w] = ok;
-                    if (ok) {
-                        s_bx[w] = x0 + n0 * nx;
-                        s_by[w] = y0 + n0 * ny;
+                    const bool valid = w < REF_CHUNK && gi < total;
+                    double ln = 0.0, lc = 0.0, x0 = 0.0, y0 = 0.0, nx = 0.0, ny = 0.0;
+                    if (valid) {
+                        const int e = gi < o1 ? 0 : gi < o2 ? 1 : gi < o3 ? 2 : 3;
+                        const int64_t si = gi - (e == 0 ? 0 : e == 1 ? o1 : e == 2 ? o2 : o3), ns = s_ens[e];
+                        const int a = e, b = (e + 1) & 3;
+                        nx = s_enx[e];
+                        ny = s_eny[e];
+                        double alpha = (1.0 + (double)si) / (double)(ns + 1);
+                        x0 = alpha * (double)s_p[a][0] + (1.0 - alpha) * (double)s_p[b][0];
+                        y0 = alpha * (double)s_p[a][1] + (1.0 - alpha) * (double)s_p[b][1];
+                        refine_part(v, x0, y0, nx, ny, range, vsteps, u, &ln, &lc);
+                    }
+                    const double ln0 = __shfl_sync(0xffffffffu, ln, 0, 4), ln1 = __shfl_sync(0xffffffffu, ln, 1, 4),
+                                 ln2 = __shfl_sync(0xffffffffu, ln, 2, 4), ln3 = __shfl_sync(0xffffffffu, ln, 3, 4);
+                    const double lc0 = __shfl_sync(0xffffffffu, lc, 0, 4), lc1 = __shfl_sync(0xffffffffu, lc, 1, 4),
+                                 lc2 = __shfl_sync(0xffffffffu, lc, 2, 4), lc3 = __shfl_sync(0xffffffffu, lc, 3, 4);
+                    if (valid && u == 0) {
+                        double mn = 0.0 + ((ln0 + ln2) + (ln1 + ln3));
+                        double mc = 0.0 + ((lc0 + lc2) + (lc1 + lc3));
+                        refine_tail(v, x0, y0, nx, ny, range, vsteps, nsteps, &mn, &mc);
+                        const bool ok = mc != 0.0;
+                        s_bok[w] = ok;
+                        if (ok) {
+                            const double n0 = mn / mc;
+                            s_bx[w] = x0 + n0 * nx;
+                            s_by[w] = y0 + n0 * ny;
+                        }
                     }
                 }
                 __syncthreads();
