@@ -1038,6 +1038,72 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
 }
 
 
+// A double as a 64-bit integer in the same order (negative values
+// reversed below the positive ones); no NaN reaches it.
+__device__ __forceinline__ uint64_t dorder_key(double d) {
+    const uint64_t b = (uint64_t)__double_as_longlong(d);
+    return (b >> 63) ? ~b : b | 0x8000000000000000ull;
+}
+__device__ __forceinline__ double dorder_val(uint64_t k) {
+    return __longlong_as_double((long long)((k >> 63) ? k & 0x7fffffffffffffffull : ~k));
+}
+
+// The (r+1)-th largest of e[0, n) (r < n), by the whole block: a radix
+// select over dorder_key, 8 bits a pass from the top. hist holds 256
+// counters; *selp and *selr are the prefix found and the rank left.
+// Warp 0 finds each pass's digit: lane l counts digits 255-8l .. 248-8l.
+__device__ double block_select_desc(const double *e, int64_t n, uint32_t r, uint32_t *hist, uint64_t *selp,
+                                    uint32_t *selr) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    if (tid == 0) {
+        *selp = 0;
+        *selr = r;
+    }
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int b = tid; b < 256; b += nt) hist[b] = 0;
+        __syncthreads();
+        const uint64_t prefix = *selp, mask = shift == 56 ? 0ull : ~0ull << (shift + 8);
+        for (int64_t i = tid; i < n; i += nt) {
+            const uint64_t key = dorder_key(e[i]);
+            if ((key & mask) == prefix) atomicAdd(hist + ((key >> shift) & 255u), 1u);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            const uint32_t rr = *selr;
+            uint32_t c[8], sum = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                c[j] = hist[255 - 8 * lane - j];
+                sum += c[j];
+            }
+            uint32_t inc = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            const uint32_t excl = inc - sum;
+            if (excl <= rr && rr < inc) {
+                uint32_t acc = excl;
+                int bin = 255 - 8 * lane;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (rr >= acc + c[j]) {
+                        acc += c[j];
+                        continue;
+                    }
+                    bin = 255 - 8 * lane - j;
+                    break;
+                }
+                *selr = rr - acc;
+                *selp = prefix | (uint64_t)bin << shift;
+            }
+        }
+        __syncthreads();
+    }
+    return dorder_val(*selp);
+}
+
 // Two size classes of clusters, one kernel template: 128 threads for
 // clusters of at most FIT_SMALL points (everything staged in shared
 // memory), 512 threads for the larger ones (dynamic shared memory; sorts
@@ -1052,9 +1118,10 @@ __device__ __forceinline__ void line_of(MSum s, double lp[4], double *mse) {
 // points: region X (the angle keys; then the radix sort's second buffers;
 // then the staged moment terms of a chunk of points), the sort keys (4 B)
 // and point indices (2 B), and the radix histograms (256 per warp). The
-// moment terms take two chunks of six doubles per point.
+// moment terms take two chunks of six rows of chunk + 2 doubles (the pad
+// puts the six rows that one warp walks in step on distinct banks).
 __host__ __device__ constexpr size_t fit_x_bytes(int sort_cap, int chunk) {
-    return (size_t)sort_cap * 8 > (size_t)chunk * 96 ? (size_t)sort_cap * 8 : (size_t)chunk * 96;
+    return (size_t)sort_cap * 8 > (size_t)(chunk + 2) * 96 ? (size_t)sort_cap * 8 : (size_t)(chunk + 2) * 96;
 }
 __host__ __device__ constexpr size_t fit_smem_bytes(int sort_cap, int chunk, int nwarps) {
     return fit_x_bytes(sort_cap, chunk) + (size_t)sort_cap * 6 + (size_t)256 * nwarps * 4;
@@ -1186,6 +1253,8 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
     __shared__ double s_be[NT / 32], s_lines[4][4], s_lmse[4], s_best;
     __shared__ int64_t s_bo[NT / 32];
     __shared__ uint32_t s_next;
+    __shared__ uint64_t s_selp;
+    __shared__ uint32_t s_selr;
     const int tid = threadIdx.x;
     const uint32_t ncl = *count;
 
@@ -1317,10 +1386,11 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             // leaves in reverse order, and in each leaf its blocks by head
             // index descending, each block in network order. A stable sort
             // by the head's slope bits then gives the (head, place) order.
-            for (int64_t p = tid; p < sz; p += NT) {
-                uint32_t lf = leaf_of(sz, p);
+            // Each warp finds the leaves that start in its 32 points at a
+            // time, queues them in its slice of the (still unused) radix
+            // histograms, and arranges them 32 leaves at a time.
+            auto arrange = [&](uint32_t lf) {
                 const int lo = (int)(lf >> 8), len = (int)(lf & 255);
-                if (p != lo) continue;
                 // everything indexed by constants: registers only
                 uint64_t k5[5];
 #pragma unroll
@@ -1351,6 +1421,26 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
                     s_ka[pos] = hkey[t];
                     s_val[pos] = (uint16_t)~(uint32_t)k5[t];
                 }
+            };
+            {
+                const int lane = tid & 31;
+                uint32_t *lq = s_hist + (tid >> 5) * 256;
+                int qn = 0;
+                for (int64_t p0 = (int64_t)(tid >> 5) * 32; p0 < sz; p0 += NT) {
+                    const int64_t p = p0 + lane;
+                    const uint32_t lf = p < sz ? leaf_of(sz, p) : 0u;
+                    const bool lead = p < sz && (int64_t)(lf >> 8) == p;
+                    const uint32_t bal = __ballot_sync(0xffffffffu, lead);
+                    if (lead) lq[qn + __popc(bal & ((1u << lane) - 1u))] = lf;
+                    qn += __popc(bal);
+                    __syncwarp();
+                    if (qn >= 32) {
+                        qn -= 32;
+                        arrange(lq[qn + lane]);
+                        __syncwarp();
+                    }
+                }
+                if (lane < qn) arrange(lq[lane]);
             }
             __syncthreads();
             FIT_PROF(4)
@@ -1390,6 +1480,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
         const uint8_t *im = qim + f.q_off;
         double *M[6] = {scr.mx + s0, scr.my + s0, scr.mxx + s0, scr.mxy + s0, scr.myy + s0, scr.mw + s0};
         double run = 0.0;
+        const int cs = chunk + 2;  // row stride of the staged terms
         auto stage = [&](int64_t k0, double *buf, int first, int stride) {
             const int64_t kn = dmin((int64_t)chunk, sz - k0);
             for (int64_t t = first; t < kn; t += stride) {
@@ -1408,12 +1499,12 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
                 const double fx = __dadd_rn(__dmul_rn((double)px, 0.5), 0.5);
                 const double fy = __dadd_rn(__dmul_rn((double)py, 0.5), 0.5);
                 const double wx = __dmul_rn(w, fx), wy = __dmul_rn(w, fy);
-                buf[0 * chunk + t] = wx;
-                buf[1 * chunk + t] = wy;
-                buf[2 * chunk + t] = __dmul_rn(wx, fx);
-                buf[3 * chunk + t] = __dmul_rn(wx, fy);
-                buf[4 * chunk + t] = __dmul_rn(wy, fy);
-                buf[5 * chunk + t] = w;
+                buf[0 * cs + t] = wx;
+                buf[1 * cs + t] = wy;
+                buf[2 * cs + t] = __dmul_rn(wx, fx);
+                buf[3 * cs + t] = __dmul_rn(wx, fy);
+                buf[4 * cs + t] = __dmul_rn(wy, fy);
+                buf[5 * cs + t] = w;
             }
         };
         // the prefix sums are taken in place in shared memory; the other
@@ -1422,18 +1513,18 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             const int64_t kn = dmin((int64_t)chunk, sz - k0);
             for (int64_t t = first; t < 6 * kn; t += stride) {
                 const int64_t q = t / kn, i = t - q * kn;
-                M[q][k0 + i] = buf[q * chunk + i];
+                M[q][k0 + i] = buf[q * cs + i];
             }
         };
         stage(0, s_w, tid, NT);
         __syncthreads();
         int64_t ch = 0;
         for (int64_t k0 = 0; k0 < sz; k0 += chunk, ch++) {
-            double *cur = s_w + (ch & 1) * 6 * chunk, *oth = s_w + ((ch + 1) & 1) * 6 * chunk;
+            double *cur = s_w + (ch & 1) * 6 * cs, *oth = s_w + ((ch + 1) & 1) * 6 * cs;
             if (tid < 32) {
                 if (tid < 6) {
                     const int64_t kn = dmin((int64_t)chunk, sz - k0);
-                    double *src = cur + tid * chunk;
+                    double *src = cur + tid * cs;
                     int64_t t = 0;
                     // 16 loads, the 16 dependent additions, then 16 stores:
                     // stores between the additions would lengthen the chain
@@ -1461,7 +1552,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             }
             __syncthreads();
         }
-        if (ch > 0) copy_out((ch - 1) * chunk, s_w + ((ch - 1) & 1) * 6 * chunk, tid, NT);
+        if (ch > 0) copy_out((ch - 1) * chunk, s_w + ((ch - 1) & 1) * 6 * cs, tid, NT);
         __syncthreads();
         const Moments mo = {M[0], M[1], M[2], M[3], M[4], M[5]};
         FIT_PROF(6)
@@ -1531,20 +1622,18 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             // e_i exceeds that order statistic exactly when at most
             // max_nmaxima errors are >= e_i: a parallel count, then an
             // order-keeping compaction.
+            // The order statistic by a radix select over the errors'
+            // order-preserving 64-bit images, 8 bits a pass: e_i is kept
+            // exactly when e_i > T, T the (max_nmaxima+1)-th largest.
             const int64_t k = prm.max_nmaxima;
             double *e = in_smem && nm <= sort_cap ? reinterpret_cast<double *>(s_key) : filt;
             for (int64_t i = tid; i < nm; i += NT) e[i] = mxe[i];
-            __syncthreads();
+            const double T = block_select_desc(e, nm, (uint32_t)k, s_hist, &s_selp, &s_selr);
             int64_t kept_run = 0;
             for (int64_t i0 = 0; i0 < nm; i0 += NT) {
                 int64_t i = i0 + tid;
                 uint32_t keep = 0;
-                if (i < nm) {
-                    double ei = e[i];
-                    int64_t ge = 0;
-                    for (int64_t j = 0; j < nm && ge <= k; j++) ge += e[j] >= ei;
-                    keep = ge <= k;
-                }
+                if (i < nm) keep = e[i] > T;
                 uint32_t total;
                 uint32_t off = block_excl_scan(keep, &total, s_scan);
                 int32_t mi = i < nm ? mxi[i] : 0;
