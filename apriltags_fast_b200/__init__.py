@@ -152,6 +152,8 @@ def lib():
         L.at_detector_last_error.restype = C.c_int
         L.at_detector_diag.argtypes = [C.POINTER(CDetector), C.c_int, C.c_void_p, C.c_int64]
         L.at_detector_diag.restype = C.c_int64
+        L.at_detector_set_batch_split.argtypes = [C.POINTER(CDetector), C.c_int]
+        L.at_detector_set_batch_split.restype = C.c_int
         L.at_server_create.argtypes = [C.POINTER(CDetector), C.POINTER(ServerConfig)]
         L.at_server_create.restype = C.c_void_p
         L.at_server_submit.argtypes = [C.c_void_p, C.POINTER(Frame), C.c_uint64]
@@ -286,6 +288,13 @@ class Detector:
     def timing(self) -> dict:
         t = self._td.contents.timing
         return {n: getattr(t, n) for n, _ in Timing._fields_}
+
+    def set_batch_split(self, pipelines: int) -> None:
+        """Spread large batches over this many pipelines (1-4, default 3),
+        each with its own streams, arenas and host thread; the results do
+        not depend on it."""
+        if self._L.at_detector_set_batch_split(self._td, int(pipelines)) != 0:
+            raise ValueError("pipelines must be 1 to 4")
 
     def diag(self, what: str) -> np.ndarray:
         """An intermediate array of the last detection (frame 0), for

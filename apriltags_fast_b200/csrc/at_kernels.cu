@@ -881,6 +881,38 @@ __device__ __forceinline__ uint32_t leaf_of(int64_t n, int64_t p) {
     return (uint32_t)(lo << 8 | sz);
 }
 
+// The leaf of position p of n (see leaf_of), in 32-bit arithmetic.
+__device__ __forceinline__ void leaf_of32(int n, int p, int &lo, int &len) {
+    int l = 0, sz = n;
+    while (sz / 2 > 5) {
+        const int half = sz / 2, q1 = half / 2, q3 = half + (sz - half) / 2;
+        const int r = p - l;
+        if (r < q1) {
+            sz = q1;
+        } else if (r < half) {
+            l += q1;
+            sz = half - q1;
+        } else if (r < q3) {
+            l += half;
+            sz = q3 - half;
+        } else {
+            l += q3;
+            sz = sz - q3;
+        }
+    }
+    while (sz > 5) {
+        const int half = sz / 2;
+        if (p - l >= half) {
+            l += half;
+            sz -= half;
+        } else {
+            sz = half;
+        }
+    }
+    lo = l;
+    len = sz;
+}
+
 // The leaf networks of the reference (fast/quads.c:56-85): compare-exchange
 // on the upper 32 bits only.
 __device__ __forceinline__ void leaf_network(uint64_t *k, int n) {
@@ -1428,8 +1460,10 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
                 int qn = 0;
                 for (int64_t p0 = (int64_t)(tid >> 5) * 32; p0 < sz; p0 += NT) {
                     const int64_t p = p0 + lane;
-                    const uint32_t lf = p < sz ? leaf_of(sz, p) : 0u;
-                    const bool lead = p < sz && (int64_t)(lf >> 8) == p;
+                    int llo = -1, llen = 0;
+                    if (p < sz) leaf_of32((int)sz, (int)p, llo, llen);
+                    const bool lead = llo == (int)p;
+                    const uint32_t lf = (uint32_t)llo << 8 | (uint32_t)llen;
                     const uint32_t bal = __ballot_sync(0xffffffffu, lead);
                     if (lead) lq[qn + __popc(bal & ((1u << lane) - 1u))] = lf;
                     qn += __popc(bal);
@@ -1907,37 +1941,6 @@ __host__ __device__ constexpr size_t fit_warp_smem(int cap, int mm, bool gp = fa
     return (size_t)(gp ? 8 : 56) * cap + fit_warp_x1(cap, mm);
 }
 
-// The leaf of position p of n (see leaf_of), in 32-bit arithmetic.
-__device__ __forceinline__ void leaf_of32(int n, int p, int &lo, int &len) {
-    int l = 0, sz = n;
-    while (sz / 2 > 5) {
-        const int half = sz / 2, q1 = half / 2, q3 = half + (sz - half) / 2;
-        const int r = p - l;
-        if (r < q1) {
-            sz = q1;
-        } else if (r < half) {
-            l += q1;
-            sz = half - q1;
-        } else if (r < q3) {
-            l += half;
-            sz = q3 - half;
-        } else {
-            l += q3;
-            sz = sz - q3;
-        }
-    }
-    while (sz > 5) {
-        const int half = sz / 2;
-        if (p - l >= half) {
-            l += half;
-            sz -= half;
-        } else {
-            sz = half;
-        }
-    }
-    lo = l;
-    len = sz;
-}
 
 
 // Bitonic sort, ascending, of a warp's keys k[0, np) in shared memory (np

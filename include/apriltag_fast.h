@@ -161,6 +161,16 @@ typedef struct at_frame_result {
    detections, frame by frame; td->ndetections their total. */
 void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *results);
 
+/* How many pipelines at_detect_batch spreads a large batch over (1 to 4;
+   3 by default). Each pipeline takes a run of consecutive frames (at least
+   10, with about equal pixel counts): the first runs on this detector, the
+   others on helper detectors made like it (their own streams and device
+   arenas, created at first use), each driven by its own host thread, so
+   that their host synchronisations and latency-bound kernels overlap on the
+   GPU. Results do not depend on the setting; at_timing and the diagnostics
+   describe the first pipeline's part. Returns -1 for a value out of range. */
+int at_detector_set_batch_split(at_detector *td, int pipelines);
+
 /* Serving (no counterpart in the reference, which detects one frame per
    call). A server owns `workers` detectors made from `params` (its
    parameters and families at creation), each with its own stream and

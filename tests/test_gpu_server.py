@@ -102,3 +102,22 @@ def test_uneven_batch_with_family_sets_equals_single():
         assert one.tobytes() == batch[i].tobytes()
         assert det.last_batch_nquads[0] == nq[i]
         assert all(int(x["family"]) == (0 if masks[i] == 1 else 1) for x in one)
+
+
+def test_batch_split_equals_one_pipeline():
+    """A batch spread over 2-4 pipelines (helper detectors on their own
+    threads) gives the same detections and quad counts, frame by frame, as
+    one pipeline."""
+    frames, fams = synth.uneven_batch(40, 9)
+    det = AT.Detector(["tag36h11", "tag25h9"], 2)
+    masks = [1 if f == "tag36h11" else 2 for f in fams]
+    det.set_batch_split(1)
+    ref = [d.tobytes() for d in det.detect_batch(frames, family_masks=masks, as_arrays=True)]
+    ref_nq = list(det.last_batch_nquads)
+    for p in (2, 3, 4, 2):
+        det.set_batch_split(p)
+        got = det.detect_batch(frames, family_masks=masks, as_arrays=True)
+        assert [d.tobytes() for d in got] == ref
+        assert list(det.last_batch_nquads) == ref_nq
+    with pytest.raises(ValueError):
+        det.set_batch_split(5)
