@@ -498,10 +498,15 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
             CK(B[B_HCCOUNT].ensure(ncl * 4 + 4));
             uint64_t *sk = B[B_HSKEYS].as<uint64_t>();
             uint32_t *ss = B[B_HSSLOTS].as<uint32_t>(), *cc = B[B_HCCOUNT].as<uint32_t>();
-            if (!cub_call(in, [&](void *t, size_t &b) {
-                    return cub::DeviceRadixSort::SortPairs(t, b, B[B_HOKEYS].as<uint64_t>(), sk,
-                                                           B[B_HOSLOTS].as<uint32_t>(), ss, ncl, 0, 2 * nb, st);
-                }))
+            // the distinct keys in order: by rank when there are few (the
+            // device-wide radix sort takes six latency-bound passes for
+            // them), else the device-wide sort
+            if (launch_sort_distinct(st, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), ncl, sk, ss))
+                in->launches += 1;
+            else if (!cub_call(in, [&](void *t, size_t &b) {
+                         return cub::DeviceRadixSort::SortPairs(t, b, B[B_HOKEYS].as<uint64_t>(), sk,
+                                                                B[B_HOSLOTS].as<uint32_t>(), ss, ncl, 0, 2 * nb, st);
+                     }))
                 return false;
             launch_cluster_rank(st, sk, ss, ncl, tcount, B[B_HRANK].as<uint32_t>(), cc, nb, dfr, (int)n,
                                 B[B_CFRAME].as<int32_t>());

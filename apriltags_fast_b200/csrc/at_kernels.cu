@@ -1028,6 +1028,35 @@ __device__ __forceinline__ MSum seg_moments(const Moments &a, int64_t sz, int64_
     return s;
 }
 
+// The moments of the window of 2 ksz + 1 points centred on i, wrapping
+// around the ends (fast/quads.c:797-808).
+__device__ __forceinline__ MSum window_moments(const Moments &a, int64_t sz, int64_t ksz, int64_t i) {
+    const int64_t i0 = i - ksz, i1 = i + ksz;
+    if (i0 < 0) return seg_moments(a, sz, i0 + sz, i1);
+    if (i1 < sz) return seg_moments(a, sz, i0, i1);
+    return seg_moments(a, sz, i0, i1 - sz);
+}
+
+// The smoothed error at i (fast/quads.c:809-826): the 7-tap filter over
+// errs, wrapping around the ends; the sum in tap order.
+template <typename I>
+__device__ __forceinline__ double smooth_at(const double *e, I n, I i, const double *q) {
+    double acc;
+    if (i >= 3 && i < n - 3) {
+        acc = e[i - 3] * q[0];
+        for (int t = 1; t < 7; t++) acc = acc + e[i - 3 + t] * q[t];
+    } else {
+        acc = 0.0;
+        for (int t = 0; t < 7; t++) {
+            I j = i - 3 + t;
+            if (j < 0) j += n;
+            if (j >= n) j -= n;
+            acc = acc + e[j] * q[t];
+        }
+    }
+    return acc;
+}
+
 // The error of a window of nn points (fast/quads.c:604-653).
 __device__ __forceinline__ double window_error(MSum s, double nn) {
     double ex = s.x / s.w, ey = s.y / s.w;
@@ -1596,33 +1625,21 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
         if (ksz < 2) continue;
         const double nn = (double)(2 * ksz + 1);
         double *errs = scr.errs + s0, *filt = scr.filt + s0;
-        for (int64_t i = tid; i < sz; i += NT) {
-            int64_t i0 = i - ksz, i1 = i + ksz;
-            MSum s;
-            if (i0 < 0)
-                s = seg_moments(mo, sz, i0 + sz, i1);
-            else if (i1 < sz)
-                s = seg_moments(mo, sz, i0, i1);
-            else
-                s = seg_moments(mo, sz, i0, i1 - sz);
-            errs[i] = window_error(s, nn);
+        // two points a thread at a time: both windows' loads before either
+        // store (a store could alias the next loads)
+        for (int64_t i = tid; i < sz; i += 2 * NT) {
+            const int64_t i2 = i + NT < sz ? i + NT : i;
+            const MSum sa = window_moments(mo, sz, ksz, i), sb = window_moments(mo, sz, ksz, i2);
+            const double ea = window_error(sa, nn), eb = window_error(sb, nn);
+            errs[i] = ea;
+            errs[i2] = eb;
         }
         __syncthreads();
-        for (int64_t i = tid; i < sz; i += NT) {
-            double acc;
-            if (i >= 3 && i < sz - 3) {
-                acc = errs[i - 3] * prm.qsm[0];
-                for (int t = 1; t < 7; t++) acc = acc + errs[i - 3 + t] * prm.qsm[t];
-            } else {
-                acc = 0.0;
-                for (int t = 0; t < 7; t++) {
-                    int64_t j = i - 3 + t;
-                    if (j < 0) j += sz;
-                    if (j >= sz) j -= sz;
-                    acc = acc + errs[j] * prm.qsm[t];
-                }
-            }
-            filt[i] = acc;
+        for (int64_t i = tid; i < sz; i += 2 * NT) {
+            const int64_t i2 = i + NT < sz ? i + NT : i;
+            const double fa = smooth_at(errs, sz, i, prm.qsm), fb = smooth_at(errs, sz, i2, prm.qsm);
+            filt[i] = fa;
+            filt[i2] = fb;
         }
         __syncthreads();
         FIT_PROF(7)
@@ -2276,33 +2293,19 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
         const int ksz = min(20, n / 12);
         if (ksz < 2) continue;
         const double nn = (double)(2 * ksz + 1);
-        for (int i = lane; i < n; i += 32) {
-            const int i0 = i - ksz, i1 = i + ksz;
-            MSum s;
-            if (i0 < 0)
-                s = seg_moments(mo, n, i0 + n, i1);
-            else if (i1 < n)
-                s = seg_moments(mo, n, i0, i1);
-            else
-                s = seg_moments(mo, n, i0, i1 - n);
-            s_err[i] = window_error(s, nn);
+        for (int i = lane; i < n; i += 64) {
+            const int i2 = i + 32 < n ? i + 32 : i;
+            const MSum sa = window_moments(mo, n, ksz, i), sb = window_moments(mo, n, ksz, i2);
+            const double ea = window_error(sa, nn), eb = window_error(sb, nn);
+            s_err[i] = ea;
+            s_err[i2] = eb;
         }
         __syncwarp();
-        for (int i = lane; i < n; i += 32) {
-            double a;
-            if (i >= 3 && i < n - 3) {
-                a = s_err[i - 3] * prm.qsm[0];
-                for (int t = 1; t < 7; t++) a = a + s_err[i - 3 + t] * prm.qsm[t];
-            } else {
-                a = 0.0;
-                for (int t = 0; t < 7; t++) {
-                    int j = i - 3 + t;
-                    if (j < 0) j += n;
-                    if (j >= n) j -= n;
-                    a = a + s_err[j] * prm.qsm[t];
-                }
-            }
-            s_filt[i] = a;
+        for (int i = lane; i < n; i += 64) {
+            const int i2 = i + 32 < n ? i + 32 : i;
+            const double fa = smooth_at(s_err, n, i, prm.qsm), fb = smooth_at(s_err, n, i2, prm.qsm);
+            s_filt[i] = fa;
+            s_filt[i2] = fb;
         }
         __syncwarp();
         FITW_PROF(7)
@@ -3489,6 +3492,42 @@ void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_
 void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
                             uint32_t *count) {
     k_cluster_collect<<<flat_blocks(size, 256), 256, 0, s>>>(tkeys, size, okeys, oslots, count);
+}
+
+// Distinct keys in key order by rank: a warp per key counts the keys
+// smaller than it (its place, the keys being distinct) and stores the key
+// and its value there. n^2 / 32 comparisons a warp-instruction each, spread
+// over the whole GPU: a few microseconds for the keys of a frame or two.
+__global__ void __launch_bounds__(256) k_rank_sort(const uint64_t *kin, const uint32_t *vin, int n, uint64_t *kout,
+                                                   uint32_t *vout) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= n) return;  // the whole warp
+    const uint64_t ki = kin[i];
+    uint32_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    int j = lane;
+    for (; j + 96 < n; j += 128) {
+        const uint64_t a = kin[j], b = kin[j + 32], c = kin[j + 64], d = kin[j + 96];
+        c0 += a < ki;
+        c1 += b < ki;
+        c2 += c < ki;
+        c3 += d < ki;
+    }
+    for (; j < n; j += 32) c0 += kin[j] < ki;
+    uint32_t cnt = c0 + c1 + c2 + c3;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) {
+        kout[cnt] = ki;
+        vout[cnt] = vin[i];
+    }
+}
+
+bool launch_sort_distinct(cudaStream_t s, const uint64_t *kin, const uint32_t *vin, int64_t n, uint64_t *kout,
+                          uint32_t *vout) {
+    if (n > RANK_SORT_CAP || n < 1) return false;
+    k_rank_sort<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(kin, vin, (int)n, kout, vout);
+    return true;
 }
 
 void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,

@@ -56,6 +56,11 @@ void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_
                          uint32_t mask, uint32_t *full);
 void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
                             uint32_t *count);
+// Distinct 64-bit keys with 32-bit values in key order (a rank per key);
+// false (nothing launched) above RANK_SORT_CAP keys.
+#define RANK_SORT_CAP 8192
+bool launch_sort_distinct(cudaStream_t s, const uint64_t *kin, const uint32_t *vin, int64_t n, uint64_t *kout,
+                          uint32_t *vout);
 void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
                          const uint32_t *tcount, uint32_t *rank_of_slot, uint32_t *ccount, int nb,
                          const FrameDesc *frames, int nframes, int32_t *cframe);
