@@ -58,7 +58,7 @@ void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size
                             uint32_t *count);
 // Distinct 64-bit keys with 32-bit values in key order (a rank per key);
 // false (nothing launched) above RANK_SORT_CAP keys.
-#define RANK_SORT_CAP 8192
+#define RANK_SORT_CAP 16384
 bool launch_sort_distinct(cudaStream_t s, const uint64_t *kin, const uint32_t *vin, int64_t n, uint64_t *kout,
                           uint32_t *vout);
 void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
