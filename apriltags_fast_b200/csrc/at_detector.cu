@@ -573,7 +573,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         uint32_t *qok = B[B_QOK].as<uint32_t>(), *qscan = B[B_QSCAN].as<uint32_t>();
         launch_fit_quads(st, in->side, in->side2, in->side3, in->fork, in->join, in->join2, in->join3, dfr, prm, qim, spts, B[B_CSTART].as<uint32_t>(), B[B_CFRAME].as<int32_t>(), ncl,
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
-        in->launches += 7;
+        in->launches += 8;
         CK(cudaGetLastError());
         if (!cub_call(in, [&](void *t, size_t &b) {
                 return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);

@@ -3584,14 +3584,16 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
     k_fit_classify<<<flat_blocks(nclusters, 256), 256, 0, s>>>(frames, cstart, cframe, nclusters, npoints,
                                                                 prm.min_cluster_pixels, quad_ok, scr.lists,
                                                                 scr.counts);
-    k_fit_order<<<2, 1024, FIT_ORDER_CAP * 8, s>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 3);
     // four streams, one per group of classes: the large clusters (a block
     // of 512 each); 513-1024 points (a block of 128); 257-512 (a warp each);
-    // up to 256 (a warp each)
+    // up to 256 (a warp each). Only the two block classes are put largest
+    // first, each on its own stream, so the warp classes start at once.
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     cudaStreamWaitEvent(side2, fork, 0);
     cudaStreamWaitEvent(side3, fork, 0);
+    k_fit_order<<<1, 1024, FIT_ORDER_CAP * 8, side>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 4);
+    k_fit_order<<<1, 1024, FIT_ORDER_CAP * 8, side2>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 3);
     const unsigned nbig = (unsigned)(nclusters < 148 ? nclusters : 148);
     k_fit_quads<512><<<nbig, 512, large, side>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
                                                  quads, quad_ok, err, scr.lists + 4 * nclusters, scr.counts + 4,
