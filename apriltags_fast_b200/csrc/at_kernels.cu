@@ -2038,7 +2038,8 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
                                                           const uint64_t *pts, const uint32_t *cstart,
                                                           const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                           const uint32_t *list, const uint32_t *count,
-                                                          GpuQuad *quads, uint32_t *quad_ok, int mm, FitScratch scr) {
+                                                          uint32_t *next, GpuQuad *quads, uint32_t *quad_ok, int mm,
+                                                          FitScratch scr) {
     constexpr int CAP = 32 * R;
     constexpr bool GP = R >= 16;  // prefix arrays in global scratch
     extern __shared__ __align__(16) unsigned char fw_smem[];
@@ -2057,8 +2058,14 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
            *s_pny = s_pnx + mm * mm;
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
 
+    // one resident wave of warps, each taking the class's next cluster
+    // from a shared counter as it finishes one (no static share to wait on)
     const uint32_t ncl = *count;
-    for (uint32_t li = blockIdx.x * FIT_WPB + wid; li < ncl; li += gridDim.x * FIT_WPB) {
+    for (;;) {
+        uint32_t li = 0;
+        if (lane == 0) li = atomicAdd(next, 1u);
+        li = __shfl_sync(FULL, li, 0);
+        if (li >= ncl) break;
         const int64_t c = list[li];
         const int64_t s0 = cstart[c];
         const int64_t sz = (c + 1 < nclusters ? (int64_t)cstart[c + 1] : npoints) - s0;
@@ -3560,12 +3567,16 @@ static void launch_fit_warp(cudaStream_t s, const FrameDesc *frames, const GpuPa
                             int64_t npoints, const FitScratch &scr, int q, GpuQuad *quads, uint32_t *quad_ok, int mm) {
     const size_t wsm = fit_warp_smem(32 * R, mm, R >= 16) * FIT_WPB;
     cudaFuncSetAttribute(k_fit_warp<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
-    const int64_t per_sm = (int64_t)(225 * 1024 / (wsm + 1024));
-    const int64_t full = 148 * (per_sm < 1 ? 1 : per_sm > 32 ? 32 : per_sm);
+    // as many blocks as fit on the SMs at once (registers and shared memory)
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fit_warp<R>, FIT_WPB * 32, wsm) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int64_t full = 148 * (int64_t)per_sm;
     const int64_t wb = (nclusters + FIT_WPB - 1) / FIT_WPB;
     k_fit_warp<R><<<(unsigned)(wb < full ? wb : full), FIT_WPB * 32, wsm, s>>>(
         frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr.lists + (int64_t)q * nclusters,
-        scr.counts + q, quads, quad_ok, mm, scr);
+        scr.counts + q, scr.counts + FIT_NCLASS + q, quads, quad_ok, mm, scr);
 }
 
 void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaStream_t side3, cudaEvent_t fork,
