@@ -550,6 +550,67 @@ __global__ void __launch_bounds__(LAB_THREADS) k_labels(const FrameDesc *frames,
     }
 }
 
+// The same labels with a warp per row (8 rows a block, for batches large
+// enough to fill the GPU that way): the run starting at each column staged
+// in the warp's slice of shared memory, a max-scan 32 columns at a time
+// (carried across chunks), and each pixel's label read through its run's
+// root (the L1 cache holds the few roots of a row). Rows wider than
+// LW_CAP columns search the runs per pixel instead.
+#define LW_CAP 2048
+__global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const RunArrays runs,
+                                                  const uint32_t *row_nruns, uint32_t *lab, int32_t min_px) {
+    __shared__ uint16_t s_run[8][LW_CAP];
+    const FrameDesc f = frames[blockIdx.y];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int qw = (int)f.qw, W = qw - 1;
+    uint16_t *sr = s_run[w];
+    for (int y = (int)blockIdx.x * 8 + w; y < (int)f.qh; y += (int)gridDim.x * 8) {
+        const int64_t base = f.node_off + (int64_t)y * qw;
+        const int nr = (int)row_nruns[f.row0 + y];
+        uint32_t *out = lab + f.q_off + (int64_t)y * qw;
+        auto label_of = [&](int i) -> uint32_t {
+            const uint32_t r = runs.parent[base + i];
+            return (int64_t)runs.px[r] >= min_px ? runs.minid[r] : AT_NOK;
+        };
+        if (lane == 0) {
+            const uint32_t r = runs.parent[f.node_off + (int64_t)qw * f.qh + y];
+            out[W] = (int64_t)runs.px[r] >= min_px ? runs.minid[r] : AT_NOK;
+        }
+        if (W > LW_CAP) {
+            for (int x = lane; x < W; x += 32) {
+                int lo = 0, hi = nr;
+                while (lo < hi) {  // the first run with start > x
+                    const int mid = (lo + hi) >> 1;
+                    if ((int)runs.start[base + mid] <= x)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                out[x] = lo > 0 && (int)runs.end[base + lo - 1] >= x ? label_of(lo - 1) : AT_NOK;
+            }
+            continue;
+        }
+        for (int x = lane; x < W; x += 32) sr[x] = 0;
+        __syncwarp();
+        for (int i = lane; i < nr; i += 32) sr[runs.start[base + i]] = (uint16_t)(i + 1);
+        __syncwarp();
+        uint32_t carry = 0;
+        for (int x0 = 0; x0 < W; x0 += 32) {
+            const int x = x0 + lane;
+            uint32_t v = x < W ? sr[x] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v = max(v, t);
+            }
+            v = max(v, carry);
+            carry = __shfl_sync(0xffffffffu, v, 31);
+            if (x < W) out[x] = v && x <= (int)runs.end[base + v - 1] ? label_of((int)v - 1) : AT_NOK;
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // 6. Boundary points (fast/clusters.c:144-252). Pixel (x, y), y in
 // 1..qh-2, against (1,0), (0,1), (-1,1), (1,1): a point where one pixel is
@@ -3471,7 +3532,10 @@ int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr,
                                                                                                         runs, row_nruns);
     k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
     k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
-    k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+    if (warp_rows(L))
+        k_labels_w<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+    else
+        k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
     return 4;
 }
 
