@@ -94,10 +94,30 @@ __global__ void k_decimate(const FrameDesc *frames, const uint8_t *img, uint8_t 
                 // (fast/image.c:26-46)
                 const uint8_t *r0 = src + (int64_t)(2 * y) * stride, *r1 = r0 + stride;
                 const int xv = qw - qw % 32;
-                for (int x = threadIdx.x; x < qw; x += blockDim.x) {
-                    const int a = r0[2 * x], b = r0[2 * x + 1], c = r1[2 * x], d = r1[2 * x + 1];
+                auto box = [&](int x, int a, int b, int c, int d) {
                     out[x] = x < xv ? (uint8_t)((((a + c + 1) >> 1) + ((b + d + 1) >> 1) + 1) >> 1)
                                     : (uint8_t)((a + b + c + d + 2) >> 2);
+                };
+                if ((((uintptr_t)r0 | (uintptr_t)r1) & 7) == 0) {
+                    // four outputs a thread from 8-byte loads of both rows
+                    for (int x4 = 4 * threadIdx.x; x4 < qw; x4 += 4 * blockDim.x) {
+                        if (x4 + 3 < qw) {
+                            const uint2 p = *reinterpret_cast<const uint2 *>(r0 + 2 * x4);
+                            const uint2 q = *reinterpret_cast<const uint2 *>(r1 + 2 * x4);
+#pragma unroll
+                            for (int u = 0; u < 4; u++) {
+                                const uint32_t pw = u < 2 ? p.x : p.y, qv = u < 2 ? q.x : q.y;
+                                const int sh = 16 * (u & 1);
+                                box(x4 + u, (pw >> sh) & 255, (pw >> (sh + 8)) & 255, (qv >> sh) & 255,
+                                    (qv >> (sh + 8)) & 255);
+                            }
+                        } else {
+                            for (int x = x4; x < qw; x++) box(x, r0[2 * x], r0[2 * x + 1], r1[2 * x], r1[2 * x + 1]);
+                        }
+                    }
+                } else {
+                    for (int x = threadIdx.x; x < qw; x += blockDim.x)
+                        box(x, r0[2 * x], r0[2 * x + 1], r1[2 * x], r1[2 * x + 1]);
                 }
             } else {
                 const uint8_t *r0 = src + (int64_t)y * k * stride;
