@@ -184,16 +184,29 @@ __global__ void k_blur_finish(const FrameDesc *frames, const uint8_t *blurred, u
 __global__ void k_tile_minmax(const FrameDesc *frames, const uint8_t *qim, uint8_t *tmax, uint8_t *tmin) {
     const FrameDesc f = frames[blockIdx.y];
     const int64_t tw = f.qw / 4, th = f.qh / 4, n = tw * th;
+    // 4-byte loads when every tile row is 4-byte aligned, else byte loads
+    const bool al = (((uintptr_t)(qim + f.q_off)) & 3) == 0 && (f.qw & 3) == 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int64_t ty = i / tw, tx = i - ty * tw;
         const uint8_t *p = qim + f.q_off + 4 * ty * f.qw + 4 * tx;
         uint32_t hi = 0, lo = 255;
+        if (al) {
+            uint32_t mx = 0, mn = 0xffffffffu;
 #pragma unroll
-        for (int dy = 0; dy < 4; dy++) {
-            // byte loads: rows of odd widths are not 4-byte aligned
-            const uint8_t *r = p + dy * f.qw;
-            hi = max(hi, (uint32_t)max(max(r[0], r[1]), max(r[2], r[3])));
-            lo = min(lo, (uint32_t)min(min(r[0], r[1]), min(r[2], r[3])));
+            for (int dy = 0; dy < 4; dy++) {
+                const uint32_t v = *reinterpret_cast<const uint32_t *>(p + dy * f.qw);
+                mx = __vmaxu4(mx, v);
+                mn = __vminu4(mn, v);
+            }
+            hi = max(max(mx & 255u, mx >> 8 & 255u), max(mx >> 16 & 255u, mx >> 24));
+            lo = min(min(mn & 255u, mn >> 8 & 255u), min(mn >> 16 & 255u, mn >> 24));
+        } else {
+#pragma unroll
+            for (int dy = 0; dy < 4; dy++) {
+                const uint8_t *r = p + dy * f.qw;
+                hi = max(hi, (uint32_t)max(max(r[0], r[1]), max(r[2], r[3])));
+                lo = min(lo, (uint32_t)min(min(r[0], r[1]), min(r[2], r[3])));
+            }
         }
         tmax[f.tile_off + i] = (uint8_t)hi;
         tmin[f.tile_off + i] = (uint8_t)lo;
@@ -212,6 +225,7 @@ __global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const u
     const int tw = qw / 4, th = qh / 4, cw = (qw + 3) / 4, ch = (qh + 3) / 4;
     const int n = cw * ch;
     const uint8_t *tx_max = tmax + f.tile_off, *tx_min = tmin + f.tile_off;
+    const bool al = ((((uintptr_t)(qim + f.q_off)) | ((uintptr_t)(thr + f.q_off))) & 3) == 0 && (qw & 3) == 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int cy = i / cw, cx = i - cy * cw;
         int ty = cy, tx = cx;
@@ -236,9 +250,19 @@ __global__ void k_threshold(const FrameDesc *frames, const uint8_t *qim, const u
         const bool flat = may_flat && (int32_t)(hi - lo) < diff;
         const int x0 = 4 * cx, y0 = 4 * cy;
         const int xe = x0 + 4 < qw ? x0 + 4 : qw, ye = y0 + 4 < qh ? y0 + 4 : qh;
-        for (int y = y0; y < ye; y++) {
-            const int64_t o = f.q_off + (int64_t)y * qw;
-            for (int x = x0; x < xe; x++) thr[o + x] = flat ? 127 : (qim[o + x] > t ? 255 : 0);
+        if (al && xe == x0 + 4) {
+            // a whole tile row at a time: per byte 255 above t, else 0
+            const uint32_t t4 = t * 0x01010101u;
+            for (int y = y0; y < ye; y++) {
+                const int64_t o = f.q_off + (int64_t)y * qw + x0;
+                const uint32_t v = *reinterpret_cast<const uint32_t *>(qim + o);
+                *reinterpret_cast<uint32_t *>(thr + o) = flat ? 0x7f7f7f7fu : __vcmpgtu4(v, t4);
+            }
+        } else {
+            for (int y = y0; y < ye; y++) {
+                const int64_t o = f.q_off + (int64_t)y * qw;
+                for (int x = x0; x < xe; x++) thr[o + x] = flat ? 127 : (qim[o + x] > t ? 255 : 0);
+            }
         }
     }
 }
