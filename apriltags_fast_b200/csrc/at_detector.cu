@@ -726,6 +726,7 @@ static void release_arenas(at_internal *in) {
 
 void at_shutdown(at_detector *td) {
     if (!td) return;
+    for (at_detector *h : td->in->helper) at_shutdown(h);  // the batch pipelines' arenas too
     cudaStreamSynchronize(td->in->stream);
     release_arenas(td->in);
 }

@@ -112,7 +112,8 @@ const char *at_family_name(const at_detector *td, const at_detection *d);
    (pageable or pinned) or device memory; it is never written. */
 void at_detect(at_detector *td, const uint8_t *pixels, int64_t width, int64_t height, int64_t stride);
 /* Replaces at_shutdown (fast/detector.c:33): releases the detector's
-   device arenas; the next at_detect allocates them again. */
+   device arenas (and those of its batch helper detectors); the next
+   at_detect allocates them again. */
 void at_shutdown(at_detector *td);
 
 /* The built-in families (fast/families.c:44-78). NULL when the library
