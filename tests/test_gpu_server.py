@@ -121,3 +121,14 @@ def test_batch_split_equals_one_pipeline():
         assert list(det.last_batch_nquads) == ref_nq
     with pytest.raises(ValueError):
         det.set_batch_split(5)
+
+
+def test_shutdown_with_batch_pipelines_then_detect_again():
+    """at_shutdown releases the arenas of the detector and of its batch
+    helpers; the next batch allocates them again and gives the same bytes."""
+    frames, _ = synth.uneven_batch(20, 4)
+    det = AT.Detector(["tag36h11"], 2)
+    first = [d.tobytes() for d in det.detect_batch(frames, as_arrays=True)]
+    det.shutdown()
+    again = [d.tobytes() for d in det.detect_batch(frames, as_arrays=True)]
+    assert again == first
