@@ -47,6 +47,25 @@ W, H = 1920, 1080
 POOL = 64
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The slowest rank's time in ms (the whole job's time): an all-reduce
+    MAX over the process group when there is one (`dist` is
+    torch.distributed or None)."""
+    if not dist:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_frames_per_s(world: int, steps: int, batch: int, t_max_ms: float) -> float:
+    """All ranks' frames over the slowest rank's time (weak scaling: each
+    rank detects its own `steps` batches of `batch` frames)."""
+    return world * steps * batch / (t_max_ms / 1e3)
+
+
 def make_pool(rank: int, n: int = POOL):
     from apriltags_fast_b200 import synth
 
@@ -349,12 +368,8 @@ def main():
         barrier()
     ms = ev0.elapsed_time(ev1)
     launches = int(det.diag("sizes")[5]) - launches0 if len(det.diag("sizes")) > 5 else None
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * args.steps * B / (t_max / 1e3)
+    t_max = max_over_ranks(ms, dist, "cuda")
+    value = job_frames_per_s(world, args.steps, B, t_max)
 
     # --- e2e: the same call on pinned host frames ---
     for s in range(args.warmup):
@@ -368,12 +383,8 @@ def main():
         ndet_e2e += sum(len(o) for o in out)
     e1.record()
     barrier()
-    ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = world * args.steps * B / (ms_e2e / 1e3)
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    e2e = job_frames_per_s(world, args.steps, B, ms_e2e)
 
     # --- stage times for the roofline: the batch on one pipeline, so that
     # each stage's event time covers all B frames (the timed runs above
