@@ -1,11 +1,9 @@
 """Build libapriltag_b200.so in-tree with nvcc for sm_100a.
 
-    python -m apriltags_fast_b200.build [--reference DIR]
+    python -m apriltags_fast_b200.build [--force]
 
-The tag family tables are extracted at build time from the AprilTag family
-files of the reference checkout (default: $APRILTAG_REFERENCE, else
-/root/reference) into _build/ (not committed). Without them the library
-still builds, and the at_tag*() accessors return NULL.
+The built-in tag families come from csrc/families.bin (committed data),
+turned into a C source under _build/ by csrc/gen_families.py.
 """
 from __future__ import annotations
 
@@ -43,21 +41,19 @@ def _newer(target, deps):
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(reference: str | None = None, force: bool = False) -> str:
+def build(force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    reference = reference or os.environ.get("APRILTAG_REFERENCE", "/root/reference")
     headers = [os.path.join(CSRC, h) for h in ("at_gpu.h", "at_kernels.h")] + [
         os.path.join(ROOT, "include", "apriltag_fast.h")]
     objs = []
     fam_c = os.path.join(BUILD, "at_families_data.c")
-    if os.path.isdir(reference) and os.path.exists(os.path.join(reference, "tag36h11.c")):
-        if force or not os.path.exists(fam_c):
-            _run([sys.executable, os.path.join(CSRC, "gen_families.py"), reference, fam_c])
-    if os.path.exists(fam_c):
-        fam_o = os.path.join(BUILD, "at_families_data.o")
-        if force or _newer(fam_o, [fam_c]):
-            _run(["gcc", "-O1", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c", fam_c, "-o", fam_o])
-        objs.append(fam_o)
+    fam_bin = os.path.join(CSRC, "families.bin")
+    if force or _newer(fam_c, [fam_bin, os.path.join(CSRC, "gen_families.py")]):
+        _run([sys.executable, os.path.join(CSRC, "gen_families.py"), "csource", fam_c])
+    fam_o = os.path.join(BUILD, "at_families_data.o")
+    if force or _newer(fam_o, [fam_c]):
+        _run(["gcc", "-O1", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c", fam_c, "-o", fam_o])
+    objs.append(fam_o)
     # the upstream API shim (plain C over the native API)
     for src in C_SOURCES:
         c = os.path.join(CSRC, src)
@@ -79,7 +75,6 @@ def build(reference: str | None = None, force: bool = False) -> str:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=None)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
-    print(build(a.reference, a.force))
+    print(build(a.force))

@@ -34,10 +34,10 @@ static_assert(sizeof(GpuDetection) == sizeof(at_detection), "detection layout");
 static_assert(sizeof(at_detector) == 160, "at_detector layout");
 static_assert(sizeof(at_family) == 584, "at_family layout");
 
-// Tables of the built-in families, generated at build time (gen_families.py);
-// a build without them links this empty list.
+// Tables of the built-in families, a C source that the build makes from
+// csrc/families.bin (gen_families.py); a null-terminated list.
 extern "C" {
-extern const at_family *const at_builtin_families[] __attribute__((weak));
+extern const at_family *const at_builtin_families[];
 }
 
 namespace {
@@ -941,7 +941,7 @@ int at_detector_last_error(const at_detector *td, const char **message) {
 
 // Built-in families (fast/families.c:44-78).
 static const at_family *builtin(const char *name) {
-    if (!at_builtin_families) return nullptr;
+    if (name == nullptr) return nullptr;
     for (int i = 0; at_builtin_families[i]; i++)
         if (!strcmp(at_builtin_families[i]->name, name)) return at_builtin_families[i];
     return nullptr;
@@ -957,65 +957,79 @@ const at_family *at_tagCustom48h12(void) { return builtin("tagCustom48h12"); }
 const at_family *at_tagStandard41h12(void) { return builtin("tagStandard41h12"); }
 const at_family *at_tagStandard52h13(void) { return builtin("tagStandard52h13"); }
 
-// PNM files, as the reference reads them (fast/image.c:204-266): binary PGM
-// or PPM with maxval 255; color becomes (r + 2g + b) / 4.
-static void pnm_skip(const uint8_t *d, int64_t n, int64_t *at) {
-    while (*at < n) {
-        uint8_t c = d[*at];
+// PNM files. Contract (fast/apriltag_fast.h:126-131 of the reference):
+// binary PGM (P5) or PPM (P6) with maxval 255 only; a PPM becomes gray as
+// (r + 2 g + b) / 4 with integer division; at_read_pnm_into reuses
+// *pixels when *cap holds width * height bytes and otherwise replaces it
+// with a new malloc'd buffer (freeing the old one); false on any error.
+
+// The next decimal number of a PNM header, after whitespace and '#'
+// comments. The character after the number is left unread.
+static bool pnm_number(FILE *fp, int64_t *value) {
+    int c;
+    for (;;) {
+        c = getc(fp);
         if (c == '#') {
-            while (*at < n && d[*at] != '\n') (*at)++;
-        } else if (c == ' ' || c == '\n' || c == '\r' || c == '\t') {
-            (*at)++;
-        } else {
-            return;
+            do c = getc(fp);
+            while (c != '\n' && c != EOF);
+        } else if (!(c == ' ' || c == '\t' || c == '\r' || c == '\n')) {
+            break;
         }
     }
-}
-static int64_t pnm_int(const uint8_t *d, int64_t n, int64_t *at) {
-    pnm_skip(d, n, at);
+    if (c < '0' || c > '9') return false;
     int64_t v = 0;
-    while (*at < n && d[*at] >= '0' && d[*at] <= '9') v = v * 10 + (d[(*at)++] - '0');
-    return v;
+    for (; c >= '0' && c <= '9'; c = getc(fp)) {
+        if (v > ((int64_t)1 << 40)) return false;  // no real image is this large
+        v = v * 10 + (c - '0');
+    }
+    if (c != EOF) ungetc(c, fp);
+    *value = v;
+    return true;
 }
 
-bool at_read_pnm_into(const char *path, int64_t *width, int64_t *height, uint8_t **pixels, int64_t *cap) {
-    FILE *fp = fopen(path, "rb");
-    if (!fp) return false;
-    std::vector<uint8_t> d;
-    bool ok = false;
-    if (fseek(fp, 0, SEEK_END) == 0) {
-        long len = ftell(fp);
-        if (len > 0 && fseek(fp, 0, SEEK_SET) == 0) {
-            d.resize(len);
-            ok = fread(d.data(), 1, len, fp) == (size_t)len;
-        }
-    }
-    fclose(fp);
-    if (!ok || d.size() < 2 || d[0] != 'P' || (d[1] != '5' && d[1] != '6')) return false;
-    int64_t n = (int64_t)d.size(), at = 2;
-    int64_t w = pnm_int(d.data(), n, &at), h = pnm_int(d.data(), n, &at), mv = pnm_int(d.data(), n, &at);
-    at++;
-    if (w <= 0 || h <= 0 || mv != 255) return false;
-    int64_t ch = d[1] == '5' ? 1 : 3;
-    if (n - at < w * h * ch) return false;
-    if (!*pixels || *cap < w * h) {
-        uint8_t *px = (uint8_t *)aligned_alloc(64, (size_t)(w * h + 63) / 64 * 64);
-        if (!px) return false;
-        free(*pixels);
-        *pixels = px;
-        *cap = w * h;
-    }
-    if (ch == 1) {
-        memcpy(*pixels, d.data() + at, w * h);
+static bool pnm_load(FILE *fp, int64_t *width, int64_t *height, uint8_t **pixels, int64_t *cap) {
+    char magic[2];
+    if (fread(magic, 1, 2, fp) != 2 || magic[0] != 'P' || (magic[1] != '5' && magic[1] != '6')) return false;
+    const int channels = magic[1] == '5' ? 1 : 3;
+    int64_t w = 0, h = 0, maxval = 0;
+    if (!pnm_number(fp, &w) || !pnm_number(fp, &h) || !pnm_number(fp, &maxval)) return false;
+    if (w <= 0 || h <= 0 || maxval != 255 || w > ((int64_t)1 << 20) || h > ((int64_t)1 << 20)) return false;
+    if (getc(fp) == EOF) return false;  // the one whitespace byte that ends the header
+    const size_t npx = (size_t)w * (size_t)h;
+    uint8_t *dst = *pixels;
+    const bool fresh = dst == nullptr || *cap < (int64_t)npx;
+    if (fresh && (dst = (uint8_t *)malloc(npx)) == nullptr) return false;
+    bool ok = true;
+    if (channels == 1) {
+        ok = fread(dst, 1, npx, fp) == npx;
     } else {
-        for (int64_t i = 0; i < w * h; i++) {
-            int r = d[at + 3 * i], g = d[at + 3 * i + 1], b = d[at + 3 * i + 2];
-            (*pixels)[i] = (uint8_t)((r + g + g + b) / 4);
+        std::vector<uint8_t> rgb((size_t)w * 3);
+        for (int64_t y = 0; ok && y < h; y++) {
+            ok = fread(rgb.data(), 1, rgb.size(), fp) == rgb.size();
+            for (int64_t x = 0; ok && x < w; x++)
+                dst[y * w + x] = (uint8_t)((rgb[3 * x] + 2 * rgb[3 * x + 1] + rgb[3 * x + 2]) / 4);
         }
+    }
+    if (!ok) {
+        if (fresh) free(dst);
+        return false;
+    }
+    if (fresh) {
+        free(*pixels);
+        *pixels = dst;
+        *cap = (int64_t)npx;
     }
     *width = w;
     *height = h;
     return true;
+}
+
+bool at_read_pnm_into(const char *path, int64_t *width, int64_t *height, uint8_t **pixels, int64_t *cap) {
+    FILE *fp = fopen(path, "rb");
+    if (fp == nullptr) return false;
+    const bool ok = pnm_load(fp, width, height, pixels, cap);
+    fclose(fp);
+    return ok;
 }
 
 bool at_read_pnm(const char *path, int64_t *width, int64_t *height, uint8_t **pixels) {
@@ -1025,11 +1039,14 @@ bool at_read_pnm(const char *path, int64_t *width, int64_t *height, uint8_t **pi
 }
 
 bool at_write_pgm(const char *path, const uint8_t *pixels, int64_t width, int64_t height) {
+    char header[64];
+    const int hl = snprintf(header, sizeof header, "P5\n%lld %lld\n255\n", (long long)width, (long long)height);
     FILE *fp = fopen(path, "wb");
-    if (!fp) return false;
-    fprintf(fp, "P5\n%lld %lld\n255\n", (long long)width, (long long)height);
-    bool ok = fwrite(pixels, 1, (size_t)(width * height), fp) == (size_t)(width * height);
-    return fclose(fp) == 0 && ok;
+    if (fp == nullptr) return false;
+    const size_t n = (size_t)width * (size_t)height;
+    bool ok = fwrite(header, 1, (size_t)hl, fp) == (size_t)hl && fwrite(pixels, 1, n, fp) == n;
+    ok = (fclose(fp) == 0) && ok;
+    return ok;
 }
 
 }  // extern "C"

@@ -75,7 +75,9 @@ __global__ void k_noalloc_threshold(const uint8_t *im, int64_t w, int64_t h, con
 }
 
 // The device address of the scratch on each device, found once per device
-// (in host code the array's name is only a stand-in for it).
+// (in host code the array's name is only a stand-in for it) and kept for the
+// life of the process: a cudaDeviceReset unloads the module, after which the
+// array may live elsewhere, so calls after a reset are not supported.
 static uint8_t *g_tiles_addr[128];
 static std::mutex g_tiles_mu;
 

@@ -7,6 +7,8 @@
    reference's common/ library that the API's callers use: matd_t, image_u8_t
    and the built-in families' create/destroy. */
 #include <math.h>
+#include <stddef.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -228,42 +230,70 @@ void apriltag_detector_clear_families(apriltag_detector_t *td) {
     td->families_changed = true;
 }
 
-/* Hand the families to the native detector again; one it refuses is
-   dropped from the list (with a message), so the family indices agree. */
+/* Contract of the family list: after any add/remove/clear, the next
+   detection hands the upstream list to the native detector in list order,
+   and a detection's `family` is the list entry at its native index. So an
+   entry that the native detector refuses (bits_corrected out of range, a
+   17th family, a table it cannot hold) must leave the upstream list too;
+   the caller learns of it on stderr. */
 static void sync_families(apriltag_detector_t *td) {
+    const int n = zarray_size(td->tag_families);
+    apriltag_family_t **fams = (apriltag_family_t **)malloc(sizeof(apriltag_family_t *) * (n > 0 ? n : 1));
+    int *bits = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    int kept = 0;
     at_clear_families(td->fast);
-    for (int i = 0; i < zarray_size(td->tag_families);) {
-        apriltag_family_t *fam;
-        int bits;
-        zarray_get(td->tag_families, i, &fam);
-        zarray_get(td->family_bits, i, &bits);
-        at_family f;
-        if (family_to_native(fam, &f) && at_add_family(td->fast, &f, bits)) {
-            i++;
-            continue;
+    for (int i = 0; i < n; i++) {
+        zarray_get(td->tag_families, i, &fams[kept]);
+        zarray_get(td->family_bits, i, &bits[kept]);
+        at_family native;
+        const bool taken = family_to_native(fams[kept], &native) && at_add_family(td->fast, &native, bits[kept]);
+        if (taken) {
+            kept++;
+        } else {
+            const char *nm = fams[kept] != NULL && fams[kept]->name != NULL ? fams[kept]->name : "(unnamed)";
+            fprintf(stderr, "apriltag_b200: the GPU detector refused family %s at %d corrected bits; it is no "
+                            "longer in the detector's list\n", nm, bits[kept]);
         }
-        fprintf(stderr, "apriltag: cannot add family %s (bits_corrected %d), removed\n",
-                fam && fam->name ? fam->name : "?", bits);
-        zarray_remove_index(td->tag_families, i, 0);
-        zarray_remove_index(td->family_bits, i, 0);
     }
+    zarray_clear(td->tag_families);
+    zarray_clear(td->family_bits);
+    for (int i = 0; i < kept; i++) {
+        zarray_add(td->tag_families, &fams[i]);
+        zarray_add(td->family_bits, &bits[i]);
+    }
+    free(fams);
+    free(bits);
     td->families_changed = false;
 }
 
-/* td->tp: one stamp per stage, from the stage times of the detection. */
-static void fill_timeprofile(timeprofile_t *tp, const at_timing *t) {
-    timeprofile_clear(tp);
-    const char *names[] = {"init", "decimate", "blur/sharp", "threshold", "unionfind",
-                           "make clusters", "fit quads to clusters", "decode+refinement", "reconcile"};
-    const double secs[] = {0.0, t->decimate, t->blur, t->threshold, t->unionfind,
-                           t->clusters, t->fit_quads, t->decode, t->reconcile};
-    int64_t u = tp->utime;
-    for (size_t i = 0; i < sizeof secs / sizeof secs[0]; i++) {
-        struct timeprofile_entry e;
-        memset(&e, 0, sizeof e);
-        u += (int64_t)(secs[i] * 1e6);
-        strncpy(e.name, names[i], sizeof e.name - 1);
-        e.utime = u;
+/* td->tp after a detection: a stamp at the end of each stage, at the
+   detection's start time plus the stage times so far (the GPU's event
+   times). The stage names are the ones upstream users see in
+   timeprofile_display. */
+static const struct {
+    const char *name;
+    size_t field; /* offset of the stage's seconds in at_timing; SIZE_MAX: none */
+} kStages[] = {
+    {"init", (size_t)-1},
+    {"decimate", offsetof(at_timing, decimate)},
+    {"blur/sharp", offsetof(at_timing, blur)},
+    {"threshold", offsetof(at_timing, threshold)},
+    {"unionfind", offsetof(at_timing, unionfind)},
+    {"make clusters", offsetof(at_timing, clusters)},
+    {"fit quads to clusters", offsetof(at_timing, fit_quads)},
+    {"decode+refinement", offsetof(at_timing, decode)},
+    {"reconcile", offsetof(at_timing, reconcile)},
+};
+
+static void stamp_stages(timeprofile_t *tp, const at_timing *t) {
+    const int64_t t0 = tp->utime;
+    double elapsed = 0.0;
+    zarray_clear(tp->stamps);
+    tp->utime = t0;
+    for (size_t k = 0; k < sizeof kStages / sizeof kStages[0]; k++) {
+        if (kStages[k].field != (size_t)-1) elapsed += *(const double *)((const char *)t + kStages[k].field);
+        struct timeprofile_entry e = {{0}, t0 + (int64_t)(elapsed * 1e6)};
+        snprintf(e.name, sizeof e.name, "%s", kStages[k].name);
         zarray_add(tp->stamps, &e);
     }
 }
@@ -291,7 +321,7 @@ zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig)
 
     td->tp->utime = utime_now();
     at_detect(fd, im_orig->buf, im_orig->width, im_orig->height, im_orig->stride);
-    fill_timeprofile(td->tp, &fd->timing);
+    stamp_stages(td->tp, &fd->timing);
     td->nquads = (uint32_t)fd->nquads;
     td->nedges = 0;
     td->nsegments = 0;
@@ -328,47 +358,53 @@ void apriltag_detections_destroy(zarray_t *detections) {
     zarray_destroy(detections);
 }
 
+/* Deep copies: the copy owns its own H (a new matd_t); the family pointer
+   is shared, as families are owned by the caller. */
 void apriltag_detection_copy(apriltag_detection_t *src, apriltag_detection_t *dst) {
-    if (dst->H) matd_destroy(dst->H);
+    matd_t *old = dst->H;
+    *dst = *src;
     dst->H = matd_copy(src->H);
-    dst->c[0] = src->c[0];
-    dst->c[1] = src->c[1];
-    memcpy(dst->p, src->p, sizeof dst->p);
-    dst->id = src->id;
-    dst->family = src->family;
-    dst->hamming = src->hamming;
-    dst->decision_margin = src->decision_margin;
+    matd_destroy(old);
 }
 
 zarray_t *apriltag_detections_copy(zarray_t *detections) {
+    const int n = zarray_size(detections);
     zarray_t *out = zarray_create(sizeof(apriltag_detection_t *));
-    for (int i = 0; i < zarray_size(detections); i++) {
-        apriltag_detection_t *det, *c;
-        zarray_get(detections, i, &det);
-        c = (apriltag_detection_t *)calloc(1, sizeof(apriltag_detection_t));
-        apriltag_detection_copy(det, c);
-        zarray_add(out, &c);
+    zarray_ensure_capacity(out, n);
+    for (int i = 0; i < n; i++) {
+        apriltag_detection_t *src = NULL;
+        zarray_get(detections, i, &src);
+        apriltag_detection_t *dup = (apriltag_detection_t *)malloc(sizeof *dup);
+        *dup = *src;
+        dup->H = matd_copy(src->H);
+        zarray_add(out, &dup);
     }
     return out;
 }
 
-/* The tag's image, one pixel per module: the white ring inside the black
-   border, then the code's bits (apriltag.c:269-297). */
+/* One pixel per module of a tag of `fam` with code index idx: 0 (black)
+   everywhere except a white square ring of side w centred in the
+   total_width grid (w = width_at_border + 2 for a normal border, the
+   border width itself for a reversed one: the white module ring just
+   inside a reversed border, just outside the black border of a normal
+   one), and the code's bits, most significant first, at (bit_x, bit_y)
+   relative to the border's corner. NULL for a bad index. */
 image_u8_t *apriltag_to_image(apriltag_family_t *fam, uint32_t idx) {
     if (fam == NULL || idx >= fam->ncodes) return NULL;
-    const uint64_t code = fam->codes[idx];
-    image_u8_t *im = image_u8_create((unsigned)fam->total_width, (unsigned)fam->total_width);
-    const int wbw = fam->width_at_border + (fam->reversed_border ? 0 : 2);
-    const int wbs = (fam->total_width - wbw) / 2;
-    for (int i = 0; i < wbw - 1; i++) {
-        im->buf[wbs * im->stride + wbs + i] = 255;
-        im->buf[(wbs + i) * im->stride + fam->total_width - 1 - wbs] = 255;
-        im->buf[(fam->total_width - 1 - wbs) * im->stride + wbs + i + 1] = 255;
-        im->buf[(wbs + 1 + i) * im->stride + wbs] = 255;
+    const int tw = fam->total_width;
+    const int w = fam->width_at_border + (fam->reversed_border ? 0 : 2);
+    const int lo = (tw - w) / 2, hi = tw - 1 - lo;  /* ring rows/columns */
+    const int bs = (tw - fam->width_at_border) / 2; /* border corner */
+    image_u8_t *im = image_u8_create((unsigned)tw, (unsigned)tw);
+    for (int y = 0; y < tw; y++)
+        for (int x = 0; x < tw; x++) {
+            const bool inside = x >= lo && x <= hi && y >= lo && y <= hi;
+            const bool edge = x == lo || x == hi || y == lo || y == hi;
+            if (inside && edge) im->buf[y * im->stride + x] = 255;
+        }
+    for (uint32_t b = 0; b < fam->nbits; b++) {
+        const uint32_t bit = fam->nbits - 1 - b; /* bit b of the code, counted from the top */
+        if ((fam->codes[idx] >> bit) & 1u) im->buf[(fam->bit_y[b] + bs) * im->stride + fam->bit_x[b] + bs] = 255;
     }
-    const int bs = (fam->total_width - fam->width_at_border) / 2;
-    for (uint32_t i = 0; i < fam->nbits; i++)
-        if (code & ((uint64_t)1 << (fam->nbits - i - 1)))
-            im->buf[(fam->bit_y[i] + bs) * im->stride + fam->bit_x[i] + bs] = 255;
     return im;
 }

@@ -5,10 +5,15 @@ a linear-gradient background with Gaussian noise, tags rendered from the
 family code tables (a 1-module white border, as apriltag_to_image draws
 them), placed by random homographies without overlap, optional filled
 rectangle/ellipse distractors and an illumination ramp, a Gaussian blur,
-rounded and clamped to u8. Tag codes are drawn without replacement, so
-every detection id in a frame is distinct.
+rounded and clamped to u8. Tag codes are drawn uniformly from the
+family's code table, with replacement (Config.replacement; without it
+every id in a frame is distinct).
 
     img, truth = make_frame(CONFIGS["1080p"], seed=2)
+
+The family tables come from the GPU library by default; `tables_from`
+builds them from any at_family source (e.g. the reference's own library),
+so that a frame can be made without loading the GPU library.
 """
 from __future__ import annotations
 
@@ -31,6 +36,7 @@ class Config:
     distractors: int = 0
     ramp: tuple | None = None        # illumination ramp (lo, hi)
     gradient: tuple = (60.0, 190.0)
+    replacement: bool = False        # draw tag codes with replacement (ids may repeat)
 
 
 CONFIGS = {
@@ -197,13 +203,16 @@ def make_frame(cfg: Config, seed: int, family_tables=None):
             continue
         fname = cfg.families[int(rng.integers(len(cfg.families)))]
         codes, nbits, bx, by, wab, tw, rev = family_tables[fname]
-        if len(used[fname]) >= len(codes):
-            continue
-        while True:
+        if cfg.replacement:
             tid = int(rng.integers(len(codes)))
-            if tid not in used[fname]:
-                break
-        used[fname].add(tid)
+        else:
+            if len(used[fname]) >= len(codes):
+                continue
+            while True:
+                tid = int(rng.integers(len(codes)))
+                if tid not in used[fname]:
+                    break
+            used[fname].add(tid)
         pat = tag_pattern(int(codes[tid]), nbits, bx, by, wab, tw, rev)
         corners = _tag_corners(rng, cx, cy, side, cfg.tilt_deg)
         # the tag's outer edge maps to the corners: module grid [0, tw]
@@ -234,11 +243,22 @@ def make_frame(cfg: Config, seed: int, family_tables=None):
     return np.clip(np.rint(img), 0, 255).astype(np.uint8), truths
 
 
-def builtin_table(name: str):
-    """(codes, nbits, bit_x, bit_y, wab, tw, reversed) of a built-in family."""
-    from . import family
-
-    f = family(name)
+def table_of(f):
+    """(codes, nbits, bit_x, bit_y, wab, tw, reversed) of an at_family
+    struct (any ctypes struct with the at_family fields)."""
     codes = np.ctypeslib.as_array(f.codes, shape=(f.ncodes,)).copy()
     return (codes, f.nbits, list(f.bit_x[:f.nbits]), list(f.bit_y[:f.nbits]), f.width_at_border, f.total_width,
             bool(f.reversed_border))
+
+
+def builtin_table(name: str):
+    """The table of a built-in family of the GPU library."""
+    from . import family
+
+    return table_of(family(name))
+
+
+def tables_from(lookup, names):
+    """name -> table for `names`, with lookup(name) giving an at_family
+    struct (for example the reference library's at_family_by_name)."""
+    return {n: table_of(lookup(n)) for n in names}

@@ -41,6 +41,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "1080p frames/s (batched GPU detector, bit-exact detections)"
+WORKLOAD = "1080p tag36h11 decimate 2, 24 tags + 200 distractors, bits 2"
 # pipelines a batched call spreads its frames over (the library's default)
 PIPELINES = 3
 W, H = 1920, 1080
@@ -66,13 +67,23 @@ def job_frames_per_s(world: int, steps: int, batch: int, t_max_ms: float) -> flo
     return world * steps * batch / (t_max_ms / 1e3)
 
 
-def make_pool(rank: int, n: int = POOL):
+def make_pool(rank: int, n: int = POOL, tables=None):
+    """The frame pool of a rank. `tables` (family name -> table) lets the
+    reference arm make the same frames from the reference's own family
+    tables, without loading the GPU library."""
     from apriltags_fast_b200 import synth
 
     cfg = synth.CONFIGS["1080p"]
-    base = [synth.make_frame(cfg, 1000 * rank + s)[0] for s in range((n + 1) // 2)]
+    base = [synth.make_frame(cfg, 1000 * rank + s, tables)[0] for s in range((n + 1) // 2)]
     pool = base + [np.ascontiguousarray(f[::-1, ::-1]) for f in base]  # 180 deg: still valid tags
     return pool[:n]
+
+
+def workload_config(batch: int, world: int) -> dict:
+    """The `config` of both arms' lines (the same workload, the same keys)."""
+    return {"workload": WORKLOAD, "batch": batch, "frame": [W, H], "pool_frames": POOL,
+            "l2": f"inputs larger than L2 ({POOL} frames, {POOL * W * H / 1e6:.0f} MB)",
+            "parallelism": f"replicas x{world}"}
 
 
 class Clocks:
@@ -149,20 +160,26 @@ def cpu_reference_fps(pool, nthreads: int, seconds: float):
 
 
 def run_reference(args):
+    """The reference's own CPU detector (oracle/_ref, compiled from its
+    sources) on the same frame pool as the GPU arm, all host threads. The
+    frames are made from the reference library's family tables, so this
+    arm loads nothing of the GPU library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pool = make_pool(0, 16)
     cores = os.cpu_count() or 1
     from oracle import oracle as O
 
     if O.ref_lib() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
         return
-    # each step: B frames through the reference's at_detect, all threads
     import ctypes as C
 
+    from apriltags_fast_b200 import synth
+
     R = O.ref_lib()
+    tables = synth.tables_from(lambda n: R.at_family_by_name(n.encode()).contents, ["tag36h11"])
+    pool = make_pool(0, POOL, tables)
     R.at_detector_create.restype = C.POINTER(O._RefDetector)
     R.at_add_family.argtypes = [C.POINTER(O._RefDetector), C.POINTER(O.Family), C.c_int]
     R.at_detect.argtypes = [C.POINTER(O._RefDetector), C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
@@ -186,10 +203,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "1080p tag36h11 decimate 2, 24 tags + 200 distractors", "batch": B,
-                   "frame": [W, H], "threads": cores},
+        "config": workload_config(B, 1),
+        "threads": cores,
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "reference",
-                         "sample": f"{args.steps} steps x {B} frames of 16 distinct 1080p frames"},
+                         "sample": f"{args.steps} steps x {B} frames of the {POOL}-frame 1080p pool, "
+                                   f"{cores} threads"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -468,9 +486,8 @@ def main():
         "vs_baseline": None,
         "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": "1080p tag36h11 decimate 2, 24 tags + 200 distractors, bits 2", "batch": B,
-                   "frame": [W, H], "pool_frames": len(pool), "l2": "inputs larger than L2 (64 frames, 132 MB)",
-                   "parallelism": f"replicas x{world}", "pipelines_per_batch": PIPELINES},
+        "config": workload_config(B, world),
+        "pipelines_per_batch": PIPELINES,
         "detections_per_frame": ndet / (steps * B),
         "single_frame": {"fps": 1e3 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
                          "p99_ms": float(np.percentile(lat, 99)), "p999_ms": float(np.percentile(lat, 99.9)),

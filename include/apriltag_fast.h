@@ -116,8 +116,8 @@ void at_detect(at_detector *td, const uint8_t *pixels, int64_t width, int64_t he
    at_detect allocates them again. */
 void at_shutdown(at_detector *td);
 
-/* The built-in families (fast/families.c:44-78). NULL when the library
-   was built without the family tables. */
+/* The built-in families (fast/families.c:44-78): the AprilTag code
+   tables, built into the library. */
 const at_family *at_tag16h5(void);
 const at_family *at_tag25h9(void);
 const at_family *at_tag36h10(void);
@@ -253,7 +253,9 @@ int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap
    holds from the first call until the process exits: images above 1 Mi
    4x4 tiles (e.g. 4096 x 4096) are refused, as are images below one tile.
    The first call on a device finds that array's device address (once per
-   device): make that first call before any stream capture. Every call
+   device) and keeps it for the life of the process: make that first call
+   before any stream capture, and do not call it again on a device after
+   cudaDeviceReset there (the array may then live at another address). Every call
    shares the array: calls that overlap on the GPU race. Returns 0, 1 for
    a refused size, 2 for a CUDA error (message on stderr). */
 int at_threshold_noalloc(const uint8_t *image, int64_t width, int64_t height, int32_t min_white_black_diff,

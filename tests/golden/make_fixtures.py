@@ -6,7 +6,7 @@ configurations (test/cases.txt) on two synthetic 640x480 images
 byte with test/golden/*.hex. Those files are copied here unchanged so the
 tests can run where the reference checkout is absent.
 
-    python tests/golden/make_fixtures.py [reference dir]
+    python tests/golden/make_fixtures.py <reference dir>
 """
 import os
 import shutil
@@ -25,4 +25,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "test", "golden")):
+        sys.exit("usage: make_fixtures.py <reference checkout> (a directory with test/golden)")
+    main(sys.argv[1])
