@@ -127,8 +127,11 @@ class ServerResult(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("admitted", C.c_int64), ("rejected", C.c_int64), ("completed", C.c_int64), ("batches", C.c_int64),
-                ("in_flight", C.c_int64), ("pending", C.c_int64), ("peak_arena_bytes", C.c_int64),
-                ("bytes_per_pixel", C.c_double)]
+                ("in_flight", C.c_int64), ("pending", C.c_int64), ("cancelled", C.c_int64),
+                ("peak_arena_bytes", C.c_int64), ("bytes_per_pixel", C.c_double)]
+
+
+SERVER_CANCELLED = -1  # at_server_result.status of a cancelled request
 
 
 def lib():
@@ -158,6 +161,8 @@ def lib():
         L.at_server_create.restype = C.c_void_p
         L.at_server_submit.argtypes = [C.c_void_p, C.POINTER(Frame), C.c_uint64]
         L.at_server_submit.restype = C.c_uint64
+        L.at_server_cancel.argtypes = [C.c_void_p, C.c_uint64]
+        L.at_server_cancel.restype = C.c_int
         L.at_server_poll.argtypes = [C.c_void_p, C.POINTER(ServerResult), C.c_int64, C.c_int32]
         L.at_server_poll.restype = C.c_int64
         L.at_server_free_result.argtypes = [C.POINTER(ServerResult)]
@@ -360,6 +365,11 @@ class Server:
         if t:
             self._keep[t] = img
         return t
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancel a request still in the queue (its result comes back with
+        status SERVER_CANCELLED); False when it already runs or is done."""
+        return bool(self._L.at_server_cancel(self._s, int(ticket)))
 
     def poll(self, max_results: int = 256, wait_ms: int = 0) -> list:
         buf = (ServerResult * max_results)()

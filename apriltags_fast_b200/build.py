@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 CUFLAGS = ARCH + FP + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                        "-I", os.path.join(ROOT, "include"), "-I", CSRC]
-SOURCES = ["at_kernels.cu", "at_detector.cu", "at_noalloc.cu", "at_server.cu"]
+SOURCES = ["at_kernels.cu", "at_cluster.cu", "at_order.cu", "at_detector.cu", "at_noalloc.cu", "at_server.cu"]
 C_SOURCES = ["at_upstream.c"]
 
 
@@ -43,7 +43,7 @@ def _newer(target, deps):
 
 def build(force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, h) for h in ("at_gpu.h", "at_kernels.h")] + [
+    headers = [os.path.join(CSRC, h) for h in ("at_gpu.h", "at_kernels.h", "at_device.cuh")] + [
         os.path.join(ROOT, "include", "apriltag_fast.h")]
     objs = []
     fam_c = os.path.join(BUILD, "at_families_data.c")

@@ -1,0 +1,438 @@
+// Clusters of boundary points without sorting the points
+// (fast/clusters.c:16-66, 123-252, 318-382).
+//
+// The reference groups the boundary points by the pair of components they
+// lie between, each cluster's points in emission order (y, x, neighbour),
+// and orders the clusters. Here the points are never stored in emission
+// order; each is made from the threshold image and the labels where it is
+// needed, and written once, to its place in its cluster:
+//
+//   k_pair_hash      a warp per row: the points' label pairs into an
+//                    open-addressing table, with each pair's point count and
+//                    the first and last row holding its points; the total.
+//   k_cluster_collect (at_kernels.cu): the distinct pairs.
+//   -- the host reads the pair and point counts (its only wait here) --
+//   k_pair_frame, k_pair_scatter, k_pair_rank: the distinct pairs in order.
+//                    A frame's pairs sort before the next frame's (the
+//                    larger label is a node of the frame), so each frame's
+//                    pairs are ranked among themselves.
+//   k_cluster_span   per cluster: count, frame, first row, rows spanned.
+//   scans            each cluster's first point; its row table's offset.
+//   k_seg_count      a warp per row: points per (cluster, row).
+//   k_seg_scan       a warp per cluster: the counts of its rows become the
+//                    places of each row's first point of the cluster.
+//   k_point_place    a warp per row: every point to its place; points of a
+//                    row go in emission order, so a cluster's points keep
+//                    the reference's order.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "at_device.cuh"
+#include "at_gpu.h"
+#include "at_kernels.h"
+
+// The cluster key and the packed value of point j (neighbour (1,0), (0,1),
+// (-1,1), (1,1)) of pixel x of row y (la, lb: labels of rows y, y + 1).
+__device__ __forceinline__ uint64_t point_key(const uint32_t *la, const uint32_t *lb, int64_t x, int j, int nb) {
+    const int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0;
+    const uint32_t l0 = la[x], l1 = j == 0 ? la[x + dx] : lb[x + dx];
+    const uint64_t hi = l0 > l1 ? l0 : l1, lo = l0 > l1 ? l1 : l0;
+    return hi << nb | lo;
+}
+
+__device__ __forceinline__ uint64_t point_value(const uint8_t *a, int64_t x, int64_t y, int j) {
+    const int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0;
+    const int dy = j == 0 ? 0 : 1;
+    const int g = a[x] == 0 ? 255 : -255;
+    const uint64_t px = (uint64_t)(2 * x + dx), py = (uint64_t)(2 * y + dy);
+    const uint64_t gx = (uint16_t)(int16_t)(dx * g), gy = (uint16_t)(int16_t)(dy * g);
+    return px | py << 16 | gx << 32 | gy << 48;
+}
+
+// The table slot of a key that is in the table.
+__device__ __forceinline__ uint32_t pair_slot(const PairTable &T, uint64_t k) {
+    uint32_t slot = ch_hash(k) & T.mask;
+    for (int p = 0; p < CH_PROBES && T.keys[slot] != k; p++) slot = (slot + 1) & T.mask;
+    return slot;
+}
+
+// Rows 1 .. qh-2 of each frame, a warp per row.
+#define ROW_WARPS_BEGIN                                                                              \
+    const FrameDesc f = frames[blockIdx.y];                                                          \
+    const int lane = threadIdx.x & 31;                                                               \
+    const int64_t wpb = blockDim.x >> 5;                                                             \
+    for (int64_t y = 1 + blockIdx.x * wpb + (threadIdx.x >> 5); y + 1 < f.qh; y += gridDim.x * wpb) { \
+        const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;                                   \
+        const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+#define ROW_WARPS_END }
+
+__global__ void __launch_bounds__(256) k_pair_hash(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                                                   int nb, PairTable T, uint32_t *full,
+                                                   unsigned long long *npoints) {
+    ROW_WARPS_BEGIN
+    uint32_t cnt = 0;
+    for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
+        const int64_t x = x0 + lane;
+        const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
+        if (!__any_sync(0xffffffffu, m != 0)) continue;
+        cnt += __popc(m);
+        for (int j = 0; j < 4; j++) {
+            const uint64_t k = (m >> j & 1u) ? point_key(la, lb, x, j, nb) : CH_EMPTY;
+            const uint32_t peers = __match_any_sync(0xffffffffu, k);
+            if (k == CH_EMPTY || lane != __ffs(peers) - 1) continue;
+            uint32_t slot = ch_hash(k) & T.mask;
+            int p = 0;
+            for (; p < CH_PROBES; p++) {
+                uint64_t cur = *(volatile uint64_t *)(T.keys + slot);
+                if (cur == CH_EMPTY) {
+                    const unsigned long long old =
+                        atomicCAS(reinterpret_cast<unsigned long long *>(T.keys + slot), CH_EMPTY, k);
+                    cur = old == CH_EMPTY ? k : old;
+                }
+                if (cur == k) break;
+                slot = (slot + 1) & T.mask;
+            }
+            if (p == CH_PROBES) {
+                atomicOr(full, 1u);
+                continue;
+            }
+            atomicAdd(T.count + slot, (uint32_t)__popc(peers));
+            atomicMin(T.ymin + slot, (uint32_t)y);
+            atomicMax(T.ymax + slot, (uint32_t)y);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(npoints, (unsigned long long)cnt);
+    ROW_WARPS_END
+}
+
+__device__ __forceinline__ int frame_of_node(const FrameDesc *frames, int nframes, int64_t node) {
+    int lo = 0, hi = nframes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (frames[mid].node_off <= node)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Each distinct pair's frame; pairs per frame.
+__global__ void k_pair_frame(const uint64_t *okeys, int64_t ncl, int nb, const FrameDesc *frames, int nframes,
+                             uint32_t *kframe, uint32_t *fcount) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < ncl; r += (int64_t)gridDim.x * blockDim.x) {
+        const int fr = frame_of_node(frames, nframes, (int64_t)(okeys[r] >> nb));
+        kframe[r] = (uint32_t)fr;
+        atomicAdd(fcount + fr, 1u);
+    }
+}
+
+// One block: each frame's first pair (foff, nframes + 1 entries).
+__global__ void __launch_bounds__(1024) k_pair_frame_offsets(const uint32_t *fcount, int nframes, uint32_t *foff,
+                                                             uint32_t *fcur) {
+    __shared__ uint32_t sh[32];
+    uint32_t base = 0;
+    for (int f0 = 0; f0 < nframes; f0 += blockDim.x) {
+        const int f = f0 + threadIdx.x;
+        const uint32_t c = f < nframes ? fcount[f] : 0u;
+        uint32_t total;
+        const uint32_t off = block_excl_scan(c, &total, sh);
+        if (f < nframes) {
+            foff[f] = base + off;
+            fcur[f] = 0;
+        }
+        base += total;
+    }
+    if (threadIdx.x == 0) foff[nframes] = base;
+}
+
+__global__ void k_pair_scatter(const uint64_t *okeys, const uint32_t *oslots, int64_t ncl, const uint32_t *kframe,
+                               const uint32_t *foff, uint32_t *fcur, uint64_t *gkeys, uint32_t *gslots) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < ncl; r += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t fr = kframe[r];
+        const uint32_t p = foff[fr] + atomicAdd(fcur + fr, 1u);
+        gkeys[p] = okeys[r];
+        gslots[p] = oslots[r];
+    }
+}
+
+// A warp per pair: its place = its frame's first place + the number of
+// smaller pairs of the frame (the pairs are distinct).
+__global__ void __launch_bounds__(256) k_pair_rank(const uint64_t *gkeys, const uint32_t *gslots, int64_t ncl,
+                                                   const uint32_t *foff, int nframes, uint64_t *skeys,
+                                                   uint32_t *sslots) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < ncl;
+         p += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int lo = 0, hi = nframes - 1;  // the frame whose segment holds p
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (foff[mid] <= (uint32_t)p)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint64_t k = gkeys[p];
+        uint32_t below = 0;
+        for (uint32_t q = foff[lo] + lane; q < foff[lo + 1]; q += 32) below += gkeys[q] < k;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) below += __shfl_xor_sync(0xffffffffu, below, o);
+        if (lane == 0) {
+            skeys[foff[lo] + below] = k;
+            sslots[foff[lo] + below] = gslots[p];
+        }
+    }
+}
+
+// Cluster c (in pair order): its slot's rank; its point count, frame,
+// first row and rows spanned.
+__global__ void k_cluster_span(const uint64_t *skeys, const uint32_t *sslots, int64_t ncl, PairTable T, int nb,
+                               const FrameDesc *frames, int nframes, uint32_t *rank_of_slot, uint32_t *ccount,
+                               uint32_t *cspan, uint32_t *cy0, int32_t *cframe) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncl; c += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = sslots[c];
+        rank_of_slot[s] = (uint32_t)c;
+        ccount[c] = T.count[s];
+        cy0[c] = T.ymin[s];
+        cspan[c] = T.ymax[s] - T.ymin[s] + 1;
+        cframe[c] = frame_of_node(frames, nframes, (int64_t)(skeys[c] >> nb));
+    }
+}
+
+// Exclusive scans of two arrays of n values at once (a pass per block of
+// SCAN_ITEMS, one block over the block sums, a pass that adds them):
+// out_a, out_b get n + 1 entries (the totals last).
+#define SCAN_THREADS 256
+#define SCAN_ITEMS (4 * SCAN_THREADS)
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan2_sums(const uint32_t *a, const uint32_t *b, int64_t n,
+                                                             uint32_t *sa, uint32_t *sb) {
+    __shared__ uint32_t sh[32];
+    const int64_t i0 = (int64_t)blockIdx.x * SCAN_ITEMS + 4 * threadIdx.x;
+    uint32_t va = 0, vb = 0;
+    for (int k = 0; k < 4; k++)
+        if (i0 + k < n) {
+            va += a[i0 + k];
+            vb += b[i0 + k];
+        }
+    uint32_t ta, tb;
+    block_excl_scan(va, &ta, sh);
+    block_excl_scan(vb, &tb, sh);
+    if (threadIdx.x == 0) {
+        sa[blockIdx.x] = ta;
+        sb[blockIdx.x] = tb;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_scan2_top(uint32_t *sa, uint32_t *sb, int64_t nblocks) {
+    __shared__ uint32_t sh[32];
+    uint32_t ba = 0, bb = 0;
+    for (int64_t i0 = 0; i0 < nblocks; i0 += blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        const uint32_t va = i < nblocks ? sa[i] : 0u, vb = i < nblocks ? sb[i] : 0u;
+        uint32_t ta, tb;
+        const uint32_t oa = block_excl_scan(va, &ta, sh), ob = block_excl_scan(vb, &tb, sh);
+        if (i < nblocks) {
+            sa[i] = ba + oa;
+            sb[i] = bb + ob;
+        }
+        ba += ta;
+        bb += tb;
+    }
+    if (threadIdx.x == 0) {
+        sa[nblocks] = ba;
+        sb[nblocks] = bb;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan2_apply(const uint32_t *a, const uint32_t *b, int64_t n,
+                                                              const uint32_t *sa, const uint32_t *sb,
+                                                              int64_t nblocks, uint32_t *out_a, uint32_t *out_b) {
+    __shared__ uint32_t sh[32];
+    const int64_t i0 = (int64_t)blockIdx.x * SCAN_ITEMS + 4 * threadIdx.x;
+    uint32_t xa[4], xb[4], va = 0, vb = 0;
+    for (int k = 0; k < 4; k++) {
+        xa[k] = i0 + k < n ? a[i0 + k] : 0u;
+        xb[k] = i0 + k < n ? b[i0 + k] : 0u;
+        va += xa[k];
+        vb += xb[k];
+    }
+    uint32_t ta, tb;
+    uint32_t oa = block_excl_scan(va, &ta, sh) + sa[blockIdx.x], ob = block_excl_scan(vb, &tb, sh) + sb[blockIdx.x];
+    for (int k = 0; k < 4; k++)
+        if (i0 + k < n) {
+            out_a[i0 + k] = oa;
+            out_b[i0 + k] = ob;
+            oa += xa[k];
+            ob += xb[k];
+        }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        out_a[n] = sa[nblocks];
+        out_b[n] = sb[nblocks];
+    }
+}
+
+// The row tables: zeroed up to their total (checked against the capacity:
+// a shortfall sets AT_ERR_SEGCAP and the host runs the batch again with
+// room enough; the point kernels then skip their work).
+__global__ void k_seg_zero(const uint32_t *spanoff, int64_t ncl, uint32_t *seg, int64_t cap, uint32_t *err) {
+    const int64_t total = spanoff[ncl];
+    if (total > cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, AT_ERR_SEGCAP);
+        return;
+    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+        seg[i] = 0;
+}
+
+__global__ void __launch_bounds__(256) k_seg_count(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                                                   int nb, PairTable T, const uint32_t *rank_of_slot,
+                                                   const uint32_t *spanoff, const uint32_t *cy0, int64_t ncl,
+                                                   uint32_t *seg, int64_t cap) {
+    if (spanoff[ncl] > cap) return;
+    ROW_WARPS_BEGIN
+    for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
+        const int64_t x = x0 + lane;
+        const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
+        if (!__any_sync(0xffffffffu, m != 0)) continue;
+        for (int j = 0; j < 4; j++) {
+            uint32_t c = 0xffffffffu;
+            if (m >> j & 1u) c = rank_of_slot[pair_slot(T, point_key(la, lb, x, j, nb))];
+            const uint32_t peers = __match_any_sync(0xffffffffu, c);
+            if (c == 0xffffffffu || lane != __ffs(peers) - 1) continue;
+            atomicAdd(seg + spanoff[c] + ((uint32_t)y - cy0[c]), (uint32_t)__popc(peers));
+        }
+    }
+    ROW_WARPS_END
+}
+
+// A warp per cluster: seg[spanoff[c] + r] = the place of the cluster's
+// first point in row cy0[c] + r.
+__global__ void __launch_bounds__(256) k_seg_scan(const uint32_t *cstart, const uint32_t *spanoff,
+                                                  const uint32_t *cspan, int64_t ncl, uint32_t *seg, int64_t cap) {
+    if (spanoff[ncl] > cap) return;
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncl;
+         c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        uint32_t *row = seg + spanoff[c];
+        const uint32_t n = cspan[c];
+        uint32_t carry = cstart[c];
+        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const uint32_t v = i < n ? row[i] : 0u;
+            uint32_t total;
+            const uint32_t o = warp_excl_scan(v, &total);
+            if (i < n) row[i] = carry + o;
+            carry += total;
+        }
+    }
+}
+
+#define PLACE_STAGE 128  // points of 32 pixels, at most
+
+__global__ void __launch_bounds__(256) k_point_place(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                                                     int nb, PairTable T, const uint32_t *rank_of_slot,
+                                                     const uint32_t *spanoff, const uint32_t *cy0, int64_t ncl,
+                                                     uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts,
+                                                     uint32_t *err) {
+    __shared__ uint32_t s_c[8][PLACE_STAGE];
+    __shared__ uint64_t s_v[8][PLACE_STAGE];
+    if (spanoff[ncl] > cap) return;
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
+    uint32_t *sc = s_c[threadIdx.x >> 5];
+    uint64_t *sv = s_v[threadIdx.x >> 5];
+    ROW_WARPS_BEGIN
+    for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
+        const int64_t x = x0 + lane;
+        const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
+        if (!__any_sync(0xffffffffu, m != 0)) continue;
+        // this chunk's points in emission order (x, then neighbour)
+        uint32_t total;
+        uint32_t o = warp_excl_scan(__popc(m), &total);
+        for (int j = 0; j < 4; j++)
+            if (m >> j & 1u) {
+                sc[o] = rank_of_slot[pair_slot(T, point_key(la, lb, x, j, nb))];
+                sv[o] = point_value(a, x, y, j);
+                o++;
+            }
+        __syncwarp();
+        // 32 at a time, in order: a point's place is its cluster's cursor
+        // for this row plus the cluster's points before it in the batch
+        for (uint32_t s0 = 0; s0 < total; s0 += 32) {
+            const uint32_t i = s0 + lane;
+            const bool valid = i < total;
+            const uint32_t c = valid ? sc[i] : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, c);
+            const int leader = __ffs(peers) - 1;
+            uint32_t *cursor = valid ? seg + spanoff[c] + ((uint32_t)y - cy0[c]) : nullptr;
+            uint32_t base = 0;
+            if (valid && lane == leader) base = *cursor;
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (valid) {
+                const uint32_t at = base + __popc(peers & lt);
+                if (at < npts)  // always, unless the counts disagree: then an error, not a stray write
+                    out[at] = sv[i];
+                else
+                    atomicOr(err, AT_ERR_CAPACITY);
+                if (lane == leader) *cursor = base + __popc(peers);
+            }
+            __syncwarp();
+        }
+    }
+    ROW_WARPS_END
+}
+
+// ---------------------------------------------------------------------------
+// Launchers.
+
+static inline unsigned flat_grid(int64_t n, int threads) {
+    const int64_t b = (n + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : b < 148 * 16 ? b : 148 * 16);
+}
+
+static inline dim3 row_warps(const Launch &L) {
+    const int64_t b = (L.max_qh + 7) / 8;
+    return dim3((unsigned)(b < 1 ? 1 : b < 148 * 8 ? b : 148 * 8), (unsigned)L.nframes);
+}
+
+void launch_pair_hash(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                      const PairTable &T, uint32_t *full, unsigned long long *npoints) {
+    k_pair_hash<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, full, npoints);
+}
+
+void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *oslots, int64_t ncl, int nb,
+                       const FrameDesc *frames, int nframes, const PairTable &T, const PairScratch &P,
+                       uint64_t *skeys, uint32_t *sslots, uint32_t *rank_of_slot, uint32_t *ccount, uint32_t *cspan,
+                       uint32_t *cy0, int32_t *cframe, uint32_t *cstart, uint32_t *spanoff) {
+    if (ncl <= 0) return;
+    cudaMemsetAsync(P.fcount, 0, (size_t)nframes * 4, s);
+    k_pair_frame<<<flat_grid(ncl, 256), 256, 0, s>>>(okeys, ncl, nb, frames, nframes, P.kframe, P.fcount);
+    k_pair_frame_offsets<<<1, 1024, 0, s>>>(P.fcount, nframes, P.foff, P.fcur);
+    k_pair_scatter<<<flat_grid(ncl, 256), 256, 0, s>>>(okeys, oslots, ncl, P.kframe, P.foff, P.fcur, P.gkeys,
+                                                       P.gslots);
+    k_pair_rank<<<flat_grid(ncl * 32, 256), 256, 0, s>>>(P.gkeys, P.gslots, ncl, P.foff, nframes, skeys, sslots);
+    k_cluster_span<<<flat_grid(ncl, 256), 256, 0, s>>>(skeys, sslots, ncl, T, nb, frames, nframes, rank_of_slot,
+                                                       ccount, cspan, cy0, cframe);
+    const int64_t nblk = (ncl + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    k_scan2_sums<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(ccount, cspan, ncl, P.bsum_a, P.bsum_b);
+    k_scan2_top<<<1, 1024, 0, s>>>(P.bsum_a, P.bsum_b, nblk);
+    k_scan2_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(ccount, cspan, ncl, P.bsum_a, P.bsum_b, nblk, cstart,
+                                                          spanoff);
+}
+
+int64_t pair_scan_blocks(int64_t ncl) { return (ncl + SCAN_ITEMS - 1) / SCAN_ITEMS + 1; }
+
+void launch_point_place(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                        const PairTable &T, const uint32_t *rank_of_slot, const uint32_t *cstart,
+                        const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0, int64_t ncl,
+                        uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err) {
+    if (ncl <= 0) return;
+    k_seg_zero<<<flat_grid(cap, 256), 256, 0, L.stream>>>(spanoff, ncl, seg, cap, err);
+    k_seg_count<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, rank_of_slot, spanoff, cy0, ncl, seg,
+                                                    cap);
+    k_seg_scan<<<flat_grid(ncl * 32, 256), 256, 0, L.stream>>>(cstart, spanoff, cspan, ncl, seg, cap);
+    k_point_place<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, rank_of_slot, spanoff, cy0, ncl, seg,
+                                                      cap, out, npts, err);
+}

@@ -95,8 +95,14 @@ enum {
     B_KEY, B_VAL, B_KEY2, B_VAL2, B_HEAD, B_HSCAN, B_CSTART, B_CFRAME,
     B_SKEYS, B_SSKEY, B_SSVAL, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW, B_SERRS, B_SFILT,
     B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_QNUM, B_FIRST, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
+    B_HYMIN, B_HYMAX, B_CSPAN, B_CY0, B_SPANOFF, B_PKFRAME, B_PGKEYS, B_PGSLOTS, B_PFRAMES, B_PBSUM, B_SEG,
+    B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
     B_CUB, B_ERR, B_NBUF
 };
+
+// the replay of the reference's union order keeps its arrays in shared
+// memory up to this size, else in a global scratch region per frame
+#define AT_REF_SMEM_MAX (200 * 1024)
 
 }  // namespace
 
@@ -122,6 +128,8 @@ struct at_internal {
     // sizes of the last run (frame 0), for at_detector_diag
     int64_t last_qw = 0, last_qh = 0, last_npts = 0, last_ncl = 0, last_nq = 0;
     int64_t launches = 0;  // kernels of this library launched so far
+    size_t ref_smem = 0;   // the shared memory the replay kernel is allowed (set per device)
+    int64_t seg_slack = 64;  // row-table entries per cluster beyond its points (grows on a shortfall)
 
     // A large batch is spread over up to `split` pipelines: this detector
     // and split - 1 helpers (each with its own streams and arenas), each
@@ -246,25 +254,30 @@ static int blur_taps(float qsigma, BlurTaps *t) {
     return (int)n;
 }
 
-static void gpu_params(const at_detector *td, const at_internal *in, bool decode_blurred, GpuParams *p) {
-    memset(p, 0, sizeof *p);
-    p->quad_decimate = td->quad_decimate;
-    p->min_cluster_pixels = td->qtp.min_cluster_pixels;
-    p->max_nmaxima = td->qtp.max_nmaxima;
-    p->min_white_black_diff = td->qtp.min_white_black_diff;
-    // min_tag_width (fast/detector.c:67-81)
+// min_tag_width (fast/detector.c:67-81) and the border kinds of the
+// families in `mask`.
+static void frame_families(const at_detector *td, const at_internal *in, uint32_t mask, FrameDesc *f) {
     int32_t mtw = 1000000;
     bool normal = false, reversed = false;
     for (int i = 0; i < in->nfam; i++) {
+        if (!(mask >> i & 1u)) continue;
         if (in->families[i].width_at_border < mtw) mtw = in->families[i].width_at_border;
         normal = normal || !in->families[i].reversed_border;
         reversed = reversed || in->families[i].reversed_border;
     }
     if (td->quad_decimate > 1.0f) mtw = (int32_t)((float)mtw / td->quad_decimate);
     if (mtw < 3) mtw = 3;
-    p->tag_width = mtw;
-    p->normal_border = normal;
-    p->reversed_border = reversed;
+    f->tag_width = mtw;
+    f->normal_border = normal;
+    f->reversed_border = reversed;
+}
+
+static void gpu_params(const at_detector *td, const at_internal *in, bool decode_blurred, GpuParams *p) {
+    memset(p, 0, sizeof *p);
+    p->quad_decimate = td->quad_decimate;
+    p->min_cluster_pixels = td->qtp.min_cluster_pixels;
+    p->max_nmaxima = td->qtp.max_nmaxima;
+    p->min_white_black_diff = td->qtp.min_white_black_diff;
     p->refine_edges = td->refine_edges ? 1 : 0;
     p->decode_blurred = decode_blurred ? 1 : 0;
     p->nfam = in->nfam;
@@ -324,7 +337,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         FrameDesc &f = fd[i];
         memset(&f, 0, sizeof f);
         const at_frame &fr = frames[i];
-        bool live = in->nfam > 0 && fr.width >= 8 && fr.height >= 8;
+        // a frame whose family set is empty is detected as with no families
+        bool live = in->nfam > 0 && fr.width >= 8 && fr.height >= 8 && (!fr.family_mask || (fr.family_mask & all));
         int64_t qw = 0, qh = 0;
         if (live) quad_size(fr.width, fr.height, td->quad_decimate, &qw, &qh);
         if (qw < 4 || qh < 4) live = false;
@@ -357,6 +371,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         f.row0 = rows;
         f.tile_off = tiles;
         f.fam_mask = fr.family_mask ? (fr.family_mask & all) : all;
+        frame_families(td, in, f.fam_mask, &f);
         f.max_px = (int32_t)(2 * (2 * f.qw + 2 * f.qh));
         qpx += (int64_t)f.qw * f.qh;
         nodes += (int64_t)f.qw * f.qh + f.qh;
@@ -419,16 +434,32 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                              fd[i].h, cudaMemcpyDefault, st));
     }
     uint8_t *qim = B[B_QIM].as<uint8_t>(), *thr = B[B_THR].as<uint8_t>();
-    launch_decimate(L, dfr, B[B_IMG].as<uint8_t>(), qim, td->quad_decimate);
-    in->launches += 1;
-    CK(cudaEventRecord(in->ev[1], st));
-    if (ntaps > 1) {
-        launch_blur(L, dfr, qim, B[B_TMPA].as<uint8_t>(), B[B_TMPB].as<uint8_t>(), taps, td->quad_sigma < 0);
-        in->launches += 3;
+    // decimate 2 without blur: decimation and threshold in one pass (its
+    // time is the threshold stage's, as when the reference fuses them)
+    const bool fused = (int)td->quad_decimate == 2 && ntaps <= 1;
+    if (fused) {
+        int64_t blocks = 1;
+        for (auto &f : fd) {
+            const int64_t b = f.qw > 0 ? decimate_threshold_blocks(f.qw, f.qh) : 0;
+            blocks = b > blocks ? b : blocks;
+        }
+        CK(cudaEventRecord(in->ev[1], st));
+        CK(cudaEventRecord(in->ev[2], st));
+        launch_decimate_threshold(L, dfr, blocks, qim, thr, td->qtp.min_white_black_diff);
+        in->launches += 1;
+    } else {
+        launch_decimate(L, dfr, B[B_IMG].as<uint8_t>(), qim, td->quad_decimate);
+        in->launches += 1;
+        CK(cudaEventRecord(in->ev[1], st));
+        if (ntaps > 1) {
+            launch_blur(L, dfr, qim, B[B_TMPA].as<uint8_t>(), B[B_TMPB].as<uint8_t>(), taps, td->quad_sigma < 0);
+            in->launches += 3;
+        }
+        CK(cudaEventRecord(in->ev[2], st));
+        launch_threshold(L, dfr, qim, B[B_TMAX].as<uint8_t>(), B[B_TMIN].as<uint8_t>(), thr,
+                         td->qtp.min_white_black_diff);
+        in->launches += 2;
     }
-    CK(cudaEventRecord(in->ev[2], st));
-    launch_threshold(L, dfr, qim, B[B_TMAX].as<uint8_t>(), B[B_TMIN].as<uint8_t>(), thr, td->qtp.min_white_black_diff);
-    in->launches += 2;
     if (td->qtp.deglitch) {
         launch_deglitch(L, dfr, thr, B[B_TMPA].as<uint8_t>());
         in->launches += 2;
@@ -445,113 +476,119 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(cudaEventRecord(in->ev[4], st));
     CK(cudaGetLastError());
 
-    // boundary points
-    uint64_t *row_npts = B[B_ROWPTS].as<uint64_t>(), *row_off = B[B_ROWOFF].as<uint64_t>();
-    CK(cudaMemsetAsync(row_npts + rows, 0, 8, st));
-    launch_point_count(L, dfr, thr, lab, row_npts);
-    in->launches += 1;
-    if (!cub_call(in, [&](void *t, size_t &b) {
-            return cub::DeviceScan::ExclusiveSum(t, b, row_npts, row_off, rows + 1, st);
-        }))
-        return false;
-    uint64_t npts = 0;
-    CK(cudaMemcpyAsync(&npts, row_off + rows, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    // boundary points and clusters: the label pairs hashed straight from
+    // the threshold image (at_cluster.cu); the only wait of this stage reads
+    // the pair and point counts. If the pair table overflows, the points are
+    // emitted in order and sorted by pair instead (at_kernels.cu, CUB).
     int64_t ncl = 0, nq = 0;
-    if (npts > 0) {
+    uint64_t npts = 0;
+    uint32_t hsize = 1u << 16;
+    while ((int64_t)hsize < qpx / 8 && hsize < (1u << 30)) hsize <<= 1;
+    CK(B[B_HKEYS].ensure((size_t)hsize * 8));
+    CK(B[B_HCOUNT].ensure((size_t)hsize * 4));
+    CK(B[B_HYMIN].ensure((size_t)hsize * 4));
+    CK(B[B_HYMAX].ensure((size_t)hsize * 4));
+    CK(B[B_HRANK].ensure((size_t)hsize * 4));
+    CK(B[B_HMISC].ensure(32));
+    const PairTable pt{B[B_HKEYS].as<uint64_t>(), B[B_HCOUNT].as<uint32_t>(), B[B_HYMIN].as<uint32_t>(),
+                       B[B_HYMAX].as<uint32_t>(), hsize - 1};
+    uint32_t *misc = B[B_HMISC].as<uint32_t>();  // [0] overflow, [1] pairs, [2..3] points (u64)
+    CK(cudaMemsetAsync(pt.keys, 0xff, (size_t)hsize * 8, st));
+    CK(cudaMemsetAsync(pt.count, 0, (size_t)hsize * 4, st));
+    CK(cudaMemsetAsync(pt.ymin, 0xff, (size_t)hsize * 4, st));
+    CK(cudaMemsetAsync(pt.ymax, 0, (size_t)hsize * 4, st));
+    CK(cudaMemsetAsync(misc, 0, 32, st));
+    launch_pair_hash(L, dfr, thr, lab, nb, pt, misc, reinterpret_cast<unsigned long long *>(misc + 2));
+    CK(B[B_HOKEYS].ensure((size_t)hsize * 8));
+    CK(B[B_HOSLOTS].ensure((size_t)hsize * 4));
+    launch_cluster_collect(st, pt.keys, hsize, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), misc + 1);
+    in->launches += 2;
+    uint32_t hm[4];
+    CK(cudaMemcpyAsync(hm, misc, 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const bool hashed = hm[0] == 0;
+    npts = (uint64_t)hm[2] | (uint64_t)hm[3] << 32;
+    CK(B[B_CKEY].ensure(8));
+    if (npts > 0 && hashed) {
+        ncl = hm[1];
+        CK(B[B_VAL2].ensure(npts * 8));
+        CK(B[B_CSTART].ensure(ncl * 4 + 4));
+        CK(B[B_CFRAME].ensure(ncl * 4 + 4));
+        CK(B[B_HSKEYS].ensure(ncl * 8 + 8));
+        CK(B[B_HSSLOTS].ensure(ncl * 4 + 4));
+        CK(B[B_HCCOUNT].ensure(ncl * 4 + 4));
+        CK(B[B_CSPAN].ensure(ncl * 4 + 4));
+        CK(B[B_CY0].ensure(ncl * 4 + 4));
+        CK(B[B_SPANOFF].ensure(ncl * 4 + 4));
+        CK(B[B_PKFRAME].ensure(ncl * 4 + 4));
+        CK(B[B_PGKEYS].ensure(ncl * 8 + 8));
+        CK(B[B_PGSLOTS].ensure(ncl * 4 + 4));
+        CK(B[B_PFRAMES].ensure((3 * n + 1) * 4));
+        CK(B[B_PBSUM].ensure(2 * pair_scan_blocks(ncl) * 4));
+        const int64_t segcap = (int64_t)npts + in->seg_slack * ncl + 4096;
+        CK(B[B_SEG].ensure(segcap * 4));
+        uint32_t *pf = B[B_PFRAMES].as<uint32_t>();
+        uint32_t *bs = B[B_PBSUM].as<uint32_t>();
+        const PairScratch ps{B[B_PKFRAME].as<uint32_t>(), pf, pf + n, pf + 2 * n + 1, B[B_PGKEYS].as<uint64_t>(),
+                             B[B_PGSLOTS].as<uint32_t>(), bs, bs + pair_scan_blocks(ncl)};
+        launch_pair_order(st, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), ncl, nb, dfr, (int)n, pt, ps,
+                          B[B_HSKEYS].as<uint64_t>(), B[B_HSSLOTS].as<uint32_t>(), B[B_HRANK].as<uint32_t>(),
+                          B[B_HCCOUNT].as<uint32_t>(), B[B_CSPAN].as<uint32_t>(), B[B_CY0].as<uint32_t>(),
+                          B[B_CFRAME].as<int32_t>(), B[B_CSTART].as<uint32_t>(), B[B_SPANOFF].as<uint32_t>());
+        launch_point_place(L, dfr, thr, lab, nb, pt, B[B_HRANK].as<uint32_t>(), B[B_CSTART].as<uint32_t>(),
+                           B[B_SPANOFF].as<uint32_t>(), B[B_CSPAN].as<uint32_t>(), B[B_CY0].as<uint32_t>(), ncl,
+                           B[B_SEG].as<uint32_t>(), segcap, B[B_VAL2].as<uint64_t>(), (int64_t)npts,
+                           B[B_ERR].as<uint32_t>());
+        in->launches += 13;
+    } else if (npts > 0) {
+        // the pair table overflowed: points in emission order, sorted by pair
+        uint64_t *row_npts = B[B_ROWPTS].as<uint64_t>(), *row_off = B[B_ROWOFF].as<uint64_t>();
+        CK(cudaMemsetAsync(row_npts + rows, 0, 8, st));
+        launch_point_count(L, dfr, thr, lab, row_npts);
+        in->launches += 1;
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceScan::ExclusiveSum(t, b, row_npts, row_off, rows + 1, st);
+            }))
+            return false;
         CK(B[B_KEY].ensure(npts * 8));
         CK(B[B_VAL].ensure(npts * 8));
         CK(B[B_KEY2].ensure(npts * 8));
         CK(B[B_VAL2].ensure(npts * 8));
         CK(B[B_HEAD].ensure(npts * 4));
         CK(B[B_HSCAN].ensure(npts * 4));
+        CK(B[B_CKEY].ensure(npts * 8));
         launch_point_emit(L, dfr, thr, lab, row_off, B[B_KEY].as<uint64_t>(), B[B_VAL].as<uint64_t>(), nb);
         in->launches += 1;
-        const uint64_t *spts = B[B_VAL2].as<uint64_t>();
-        // group by hashing the label pairs (the full sort if the table overflows)
-        uint32_t hsize = 1u << 16;
-        while (hsize < (uint64_t)npts / 16 && hsize < (1u << 30)) hsize <<= 1;
-        CK(B[B_HKEYS].ensure((size_t)hsize * 8));
-        CK(B[B_HCOUNT].ensure((size_t)hsize * 4));
-        CK(B[B_HRANK].ensure((size_t)hsize * 4));
-        CK(B[B_HMISC].ensure(16));
-        uint64_t *tkeys = B[B_HKEYS].as<uint64_t>();
-        uint32_t *tcount = B[B_HCOUNT].as<uint32_t>(), *misc = B[B_HMISC].as<uint32_t>();
-        CK(cudaMemsetAsync(tkeys, 0xff, (size_t)hsize * 8, st));
-        CK(cudaMemsetAsync(tcount, 0, (size_t)hsize * 4, st));
-        CK(cudaMemsetAsync(misc, 0, 16, st));
-        launch_cluster_hash(st, B[B_KEY].as<uint64_t>(), (int64_t)npts, tkeys, tcount, hsize - 1, misc);
-        CK(B[B_HOKEYS].ensure((size_t)hsize * 8));
-        CK(B[B_HOSLOTS].ensure((size_t)hsize * 4));
-        launch_cluster_collect(st, tkeys, hsize, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), misc + 1);
-        in->launches += 2;
-        uint32_t hm[2];
-        CK(cudaMemcpyAsync(hm, misc, 8, cudaMemcpyDeviceToHost, st));
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
+                                                       B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
+                                                       (int64_t)npts, 0, 2 * nb, st);
+            }))
+            return false;
+        const uint64_t *skey = B[B_KEY2].as<uint64_t>();
+        uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
+        launch_cluster_heads(st, skey, npts, head);
+        in->launches += 1;
+        if (!cub_call(in, [&](void *t, size_t &b) {
+                return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
+            }))
+            return false;
+        uint32_t last[2];
+        CK(cudaMemcpyAsync(&last[0], hscan + npts - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&last[1], head + npts - 1, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        const bool hashed = hm[0] == 0;
-        if (hashed) {
-            ncl = hm[1];
-            CK(B[B_CSTART].ensure(ncl * 4 + 4));
-            CK(B[B_CFRAME].ensure(ncl * 4 + 4));
-            CK(B[B_HSKEYS].ensure(ncl * 8 + 8));
-            CK(B[B_HSSLOTS].ensure(ncl * 4 + 4));
-            CK(B[B_HCCOUNT].ensure(ncl * 4 + 4));
-            uint64_t *sk = B[B_HSKEYS].as<uint64_t>();
-            uint32_t *ss = B[B_HSSLOTS].as<uint32_t>(), *cc = B[B_HCCOUNT].as<uint32_t>();
-            // the distinct keys in order: by rank when there are few (the
-            // device-wide radix sort takes six latency-bound passes for
-            // them), else the device-wide sort
-            if (launch_sort_distinct(st, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), ncl, sk, ss))
-                in->launches += 1;
-            else if (!cub_call(in, [&](void *t, size_t &b) {
-                         return cub::DeviceRadixSort::SortPairs(t, b, B[B_HOKEYS].as<uint64_t>(), sk,
-                                                                B[B_HOSLOTS].as<uint32_t>(), ss, ncl, 0, 2 * nb, st);
-                     }))
-                return false;
-            launch_cluster_rank(st, sk, ss, ncl, tcount, B[B_HRANK].as<uint32_t>(), cc, nb, dfr, (int)n,
-                                B[B_CFRAME].as<int32_t>());
-            if (!cub_call(in, [&](void *t, size_t &b) {
-                    return cub::DeviceScan::ExclusiveSum(t, b, cc, B[B_CSTART].as<uint32_t>(), ncl, st);
-                }))
-                return false;
-            uint32_t *cidx = B[B_HEAD].as<uint32_t>(), *cidx2 = B[B_HSCAN].as<uint32_t>();
-            launch_cluster_assign(st, B[B_KEY].as<uint64_t>(), (int64_t)npts, tkeys, hsize - 1,
-                                  B[B_HRANK].as<uint32_t>(), cidx);
-            in->launches += 2;
-            const int cb = bits_for((uint64_t)ncl);
-            if (!cub_call(in, [&](void *t, size_t &b) {
-                    return cub::DeviceRadixSort::SortPairs(t, b, cidx, cidx2, B[B_VAL].as<uint64_t>(),
-                                                           B[B_VAL2].as<uint64_t>(), (int64_t)npts, 0,
-                                                           cb > 0 ? cb : 1, st);
-                }))
-                return false;
-        } else {
-            if (!cub_call(in, [&](void *t, size_t &b) {
-                    return cub::DeviceRadixSort::SortPairs(t, b, B[B_KEY].as<uint64_t>(), B[B_KEY2].as<uint64_t>(),
-                                                           B[B_VAL].as<uint64_t>(), B[B_VAL2].as<uint64_t>(),
-                                                           (int64_t)npts, 0, 2 * nb, st);
-                }))
-                return false;
-            const uint64_t *skey = B[B_KEY2].as<uint64_t>();
-            uint32_t *head = B[B_HEAD].as<uint32_t>(), *hscan = B[B_HSCAN].as<uint32_t>();
-            launch_cluster_heads(st, skey, npts, head);
-            in->launches += 1;
-            if (!cub_call(in, [&](void *t, size_t &b) {
-                    return cub::DeviceScan::ExclusiveSum(t, b, head, hscan, (int64_t)npts, st);
-                }))
-                return false;
-            uint32_t last[2];
-            CK(cudaMemcpyAsync(&last[0], hscan + npts - 1, 4, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(&last[1], head + npts - 1, 4, cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            ncl = (int64_t)last[0] + last[1];
-            CK(B[B_CSTART].ensure(ncl * 4));
-            CK(B[B_CFRAME].ensure(ncl * 4));
-            launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
-                                  B[B_CFRAME].as<int32_t>());
-            in->launches += 1;
-        }
+        ncl = (int64_t)last[0] + last[1];
+        CK(B[B_CSTART].ensure(ncl * 4 + 4));
+        CK(B[B_CFRAME].ensure(ncl * 4));
+        launch_cluster_starts(st, skey, head, hscan, npts, nb, dfr, (int)n, B[B_CSTART].as<uint32_t>(),
+                              B[B_CFRAME].as<int32_t>(), B[B_CKEY].as<uint64_t>());
+        in->launches += 1;
+    }
+    if (npts > 0) {
+        const uint64_t *spts = B[B_VAL2].as<uint64_t>();
         CK(cudaEventRecord(in->ev[5], st));
+        // each cluster's label pair (the reference order of shared ids needs it)
+        const uint64_t *ckey = hashed ? B[B_HSKEYS].as<uint64_t>() : B[B_CKEY].as<uint64_t>();
 
         // quads
         const int sc[] = {B_SKEYS, B_SSKEY, B_SW, B_SFX, B_SFY, B_SMX, B_SMY, B_SMXX, B_SMXY, B_SMYY, B_SMW,
@@ -583,9 +620,11 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         // frame's first quad stay on the device: decode is sized by ncl
         CK(B[B_QUADSC].ensure(ncl * sizeof(GpuQuad)));
         CK(B[B_QNUM].ensure(8));
+        CK(B[B_QCL].ensure(ncl * 4));
         uint32_t *nq_dev = B[B_QNUM].as<uint32_t>();
         CK(cudaMemsetAsync(nq_dev, 0, 4, st));
-        launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>(), nq_dev);
+        launch_gather_quads(st, B[B_QUADS].as<GpuQuad>(), qok, qscan, ncl, B[B_QUADSC].as<GpuQuad>(), nq_dev,
+                            B[B_QCL].as<uint32_t>());
         in->launches += 1;
         CK(cudaEventRecord(in->ev[6], st));
         // decode
@@ -614,9 +653,45 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                       ncl, dscr, B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>());
         CK(cudaEventRecord(in->ev[7], st));
         in->launches += 4;
+        // the reference's quad order for detections that share an id: the
+        // roots its union order picks for their components (at_order.cu)
+        CK(B[B_RNEED].ensure(n * 4));
+        CK(B[B_RNT].ensure(n * 4));
+        CK(B[B_RTLAB].ensure(n * AT_REF_MAXT * 4));
+        CK(B[B_RTPX].ensure(n * AT_REF_MAXT * 4));
+        CK(B[B_RTROOT].ensure(n * AT_REF_MAXT * 4));
+        CK(B[B_RTLIST].ensure(nodes * 8));
+        CK(B[B_RTROW].ensure(rows * 4));
+        CK(B[B_RPRE].ensure((rows + n) * 4));
+        CK(B[B_ROKEY].ensure(nd * 16));
+        CK(B[B_RIDX2].ensure(nd * 4));
+        CK(cudaMemsetAsync(B[B_RTROOT].p, 0xff, n * AT_REF_MAXT * 4, st));
+        const RefOrder ro{B[B_RNEED].as<uint32_t>(), B[B_RNT].as<uint32_t>(),  B[B_RTLAB].as<uint32_t>(),
+                          B[B_RTPX].as<uint32_t>(),  B[B_RTROOT].as<uint32_t>(), B[B_RTLIST].as<uint64_t>(),
+                          B[B_RTROW].as<uint32_t>(), B[B_RPRE].as<uint32_t>()};
+        int64_t capr = 1;
+        for (auto &f : fd) capr = f.qw - 1 > capr ? f.qw - 1 : capr;
+        const size_t rbytes = ref_replay_bytes(capr);
+        uint8_t *rscr = nullptr;
+        if (rbytes > AT_REF_SMEM_MAX) {
+            CK(B[B_RSCR].ensure(rbytes * n));
+            rscr = B[B_RSCR].as<uint8_t>();
+        } else if (rbytes > in->ref_smem) {
+            if (!ref_replay_set_smem(AT_REF_SMEM_MAX)) {
+                set_error(in, 1, "cudaFuncSetAttribute for the order replay failed");
+                return false;
+            }
+            in->ref_smem = AT_REF_SMEM_MAX;
+        }
+        launch_ref_order(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), in->nfam, B[B_QSTART].as<int64_t>(),
+                         B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>(), B[B_QCL].as<uint32_t>(), ckey, nb,
+                         capr, rscr, rbytes, ro, B[B_ERR].as<uint32_t>());
+        in->launches += 3;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
-                        B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(), B[B_OUTN].as<int64_t>());
+                        B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(), B[B_OUTN].as<int64_t>(), dfr, ro,
+                        B[B_QCL].as<uint32_t>(), ckey, nb, B[B_ROKEY].as<uint64_t>(), B[B_RIDX2].as<uint32_t>(),
+                        B[B_ERR].as<uint32_t>());
         // the frames' detections and counts straight into pinned host memory
         CK(in->h_out.ensure(nd * sizeof(GpuDetection) + 16));
         CK(in->h_small.ensure((3 * n + 4) * 8));
@@ -629,6 +704,12 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         uint32_t derr = 0;
         CK(cudaMemcpyAsync(&derr, B[B_ERR].p, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if ((derr & AT_ERR_SEGCAP) && in->seg_slack < ((int64_t)1 << 24)) {
+            // the clusters' row tables were short (rows without points inside
+            // a cluster's span): the batch again, with more room
+            in->seg_slack *= 8;
+            return run_batch(td, frames, n, res);
+        }
         if (derr) {
             set_error(in, 3, "device check failed (code " + std::to_string(derr) + ")");
             return false;

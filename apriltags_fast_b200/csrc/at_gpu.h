@@ -21,6 +21,8 @@
 // Error bits set by device-side checks (read back by the host).
 #define AT_ERR_CLUSTER_TOO_BIG 1u
 #define AT_ERR_CAPACITY 2u
+#define AT_ERR_ORDER 4u             // the reference's quad order could not be recovered
+#define AT_ERR_SEGCAP 8u            // the clusters' row tables needed more room: the batch runs again
 
 struct FrameDesc {
     int32_t w, h;          // input frame
@@ -33,6 +35,8 @@ struct FrameDesc {
     int64_t tile_off;      // into the tile arenas ((qw/4) * (qh/4))
     uint32_t fam_mask;     // families decoded for this frame
     int32_t max_px;        // 2 * (2 qw + 2 qh)
+    int32_t tag_width;     // min_tag_width of the frame's families (fast/detector.c:67-81)
+    int32_t normal_border, reversed_border;  // whether any of them has a normal / reversed border
 };
 
 // Detector parameters that the kernels need (host copies them per call).
@@ -41,8 +45,6 @@ struct GpuParams {
     int32_t min_cluster_pixels;
     int32_t max_nmaxima;
     int32_t min_white_black_diff;
-    int32_t tag_width;        // min_tag_width (fast/detector.c:67-81)
-    int32_t normal_border, reversed_border;
     int32_t refine_edges;
     int32_t decode_blurred;   // decode samples the blurred quad image
     int32_t nfam;

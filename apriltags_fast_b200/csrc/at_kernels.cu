@@ -10,46 +10,17 @@
 #include <stdint.h>
 
 #include "at_gpu.h"
+#include "at_device.cuh"
 #include "at_kernels.h"
 
 // ---------------------------------------------------------------------------
 // Small helpers.
-
-__device__ __forceinline__ int64_t dmin(int64_t a, int64_t b) { return a < b ? a : b; }
-__device__ __forceinline__ int64_t dmax(int64_t a, int64_t b) { return a > b ? a : b; }
 
 // C's (int) of a double on x86-64: truncation, INT_MIN out of range or NaN
 // (fast/decode.c:8-11).
 __device__ __forceinline__ int64_t c_int(double x) {
     if (x > -2147483649.0 && x < 2147483648.0) return (int64_t)x;
     return -2147483648LL;
-}
-
-// Block-wide exclusive scan of one value per thread (blockDim <= 1024).
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total, uint32_t *sh) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    uint32_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    __syncthreads();
-    if (lane == 31) sh[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t s = lane < nw ? sh[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += t;
-        }
-        if (lane < nw) sh[lane] = s;
-    }
-    __syncthreads();
-    uint32_t off = wid > 0 ? sh[wid - 1] : 0;
-    *total = sh[nw - 1];
-    return off + incl - v;
 }
 
 #define FRAME_LOOP_BEGIN(n_items)                                                               \
@@ -213,6 +184,159 @@ __global__ void k_tile_minmax(const FrameDesc *frames, const uint8_t *qim, uint8
     }
 }
 
+// The streaming stages fused for decimate 2 without blur (fast/image.c:26-46
+// and fast/threshold.c:15-161 in one pass): a block takes a region of
+// DT_ROWS x DT_COLS 4x4 cells of one frame. It reads the input rows of the
+// region's tiles and of a one-tile halo around them (16-byte loads), makes
+// each tile's 16 quad pixels in registers, keeps the region's own quad
+// pixels and every tile's max/min in shared memory, then per cell the 3x3
+// tile neighbourhood's max/min and per pixel the threshold, and writes the
+// quad image and the threshold image once (16-byte stores). Cells right of
+// the last whole tile column or below the last whole tile row (no tile of
+// their own) use the nearest tile's neighbourhood and are never flat.
+#define DT_ROWS 16
+#define DT_COLS 64
+#define DT_THREADS 256
+
+// 2x2 box of the reference's decimate2_row: columns below the largest
+// multiple of 32 round twice (its AVX2 path), the rest once.
+__device__ __forceinline__ uint32_t box2(int x, int xv, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    return x < xv ? ((((a + c + 1) >> 1) + ((b + d + 1) >> 1) + 1) >> 1) : ((a + b + c + d + 2) >> 2);
+}
+
+__global__ void __launch_bounds__(DT_THREADS) k_decimate_threshold(const FrameDesc *frames, uint8_t *qim, uint8_t *thr,
+                                                                   int32_t diff) {
+    __shared__ __align__(16) uint8_t s_q[4 * DT_ROWS][4 * DT_COLS];
+    __shared__ uint8_t s_tmax[DT_ROWS + 2][DT_COLS + 4], s_tmin[DT_ROWS + 2][DT_COLS + 4];
+    __shared__ uint16_t s_cell[DT_ROWS][DT_COLS];  // threshold | flat << 8
+    const FrameDesc f = frames[blockIdx.y];
+    const int qw = f.qw, qh = f.qh, tw = qw / 4, th = qh / 4;
+    const int cw = (qw + 3) / 4, ch = (qh + 3) / 4;
+    const int ncb = (cw + DT_COLS - 1) / DT_COLS;
+    const int rb = blockIdx.x / ncb, cb = blockIdx.x - rb * ncb;
+    const int cy0 = rb * DT_ROWS, cx0 = cb * DT_COLS;
+    if (cy0 >= ch) return;
+    const int cy1 = min(cy0 + DT_ROWS, ch), cx1 = min(cx0 + DT_COLS, cw);  // own cells
+    // tiles needed: the own cells' tiles (clamped to the grid) and one around
+    const int ty0 = max(min(cy0, th - 1) - 1, 0), ty1 = min(min(cy1 - 1, th - 1) + 1, th - 1);
+    const int tx0 = max(min(cx0, tw - 1) - 1, 0), tx1 = min(min(cx1 - 1, tw - 1) + 1, tw - 1);
+    const int px0 = tx0 & ~1;  // tiles go in pairs (16 input bytes) from an even tile
+    const int npair = (tx1 - px0) / 2 + 1, ntr = ty1 - ty0 + 1;
+    const int xv = qw - qw % 32;
+    const uint8_t *img = f.img;
+    const int64_t st = f.stride;
+    const bool al16 = ((((uintptr_t)img) | (uintptr_t)st) & 15) == 0;
+    // 1. tiles: max/min of each, and the own tiles' quad pixels
+    for (int i = threadIdx.x; i < npair * ntr; i += DT_THREADS) {
+        const int r = i / npair, tp = px0 + 2 * (i - r * npair);
+        const int ty = ty0 + r;
+        uint32_t q[2][4][4];  // [tile][row][col]
+#pragma unroll
+        for (int dy = 0; dy < 4; dy++) {
+            const uint8_t *r0 = img + (int64_t)(8 * ty + 2 * dy) * st + 8 * tp, *r1 = r0 + st;
+            uint32_t a[4], b[4];  // 16 input bytes of each row, as words
+            if (al16 && tp + 1 < tw) {
+                const uint4 u = *reinterpret_cast<const uint4 *>(r0), v = *reinterpret_cast<const uint4 *>(r1);
+                a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w;
+                b[0] = v.x, b[1] = v.y, b[2] = v.z, b[3] = v.w;
+            } else {
+                const int nb = tp + 1 < tw ? 16 : 8;
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    a[w] = b[w] = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (4 * w + k < nb) {
+                            a[w] |= (uint32_t)r0[4 * w + k] << (8 * k);
+                            b[w] |= (uint32_t)r1[4 * w + k] << (8 * k);
+                        }
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < 8; o++) {  // quad pixel 4 tp + o of row 4 ty + dy
+                const uint32_t w0 = a[o >> 1], w1 = b[o >> 1];
+                const int sh = 16 * (o & 1);
+                q[o >> 2][dy][o & 3] = box2(4 * tp + o, xv, (w0 >> sh) & 255, (w0 >> (sh + 8)) & 255,
+                                            (w1 >> sh) & 255, (w1 >> (sh + 8)) & 255);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int tx = tp + k;
+            if (tx < tx0 || tx > tx1) continue;
+            uint32_t hi = 0, lo = 255;
+#pragma unroll
+            for (int dy = 0; dy < 4; dy++)
+#pragma unroll
+                for (int dx = 0; dx < 4; dx++) {
+                    hi = max(hi, q[k][dy][dx]);
+                    lo = min(lo, q[k][dy][dx]);
+                }
+            s_tmax[ty - ty0][tx - tx0] = (uint8_t)hi;
+            s_tmin[ty - ty0][tx - tx0] = (uint8_t)lo;
+            if (ty >= cy0 && ty < cy1 && tx >= cx0 && tx < cx1) {
+#pragma unroll
+                for (int dy = 0; dy < 4; dy++)
+                    *reinterpret_cast<uint32_t *>(&s_q[4 * (ty - cy0) + dy][4 * (tx - cx0)]) =
+                        q[k][dy][0] | q[k][dy][1] << 8 | q[k][dy][2] << 16 | q[k][dy][3] << 24;
+            }
+        }
+    }
+    __syncthreads();
+    // 2. per own cell: its tile's 3x3 neighbourhood (clipped to the grid)
+    for (int i = threadIdx.x; i < (cy1 - cy0) * (cx1 - cx0); i += DT_THREADS) {
+        const int cy = cy0 + i / (cx1 - cx0), cx = cx0 + i % (cx1 - cx0);
+        const int ty = min(cy, th - 1), tx = min(cx, tw - 1);
+        const bool may_flat = cy < th && cx < tw;
+        uint32_t hi = 0, lo = 255;
+        for (int yy = max(ty - 1, 0); yy <= min(ty + 1, th - 1); yy++)
+            for (int xx = max(tx - 1, 0); xx <= min(tx + 1, tw - 1); xx++) {
+                hi = max(hi, (uint32_t)s_tmax[yy - ty0][xx - tx0]);
+                lo = min(lo, (uint32_t)s_tmin[yy - ty0][xx - tx0]);
+            }
+        const uint32_t t = lo + (hi - lo) / 2;
+        const bool flat = may_flat && (int32_t)(hi - lo) < diff;
+        s_cell[cy - cy0][cx - cx0] = (uint16_t)(t | (flat ? 256u : 0u));
+    }
+    __syncthreads();
+    // 3. the own pixels, 16 a thread: quad image and threshold image
+    const int y0 = 4 * cy0, y1 = min(4 * cy1, qh), x0 = 4 * cx0, x1 = min(4 * cx1, qw);
+    const int nseg = (x1 - x0 + 15) / 16;
+    const bool st16 = ((((uintptr_t)(qim + f.q_off)) | ((uintptr_t)(thr + f.q_off)) | (uintptr_t)qw) & 15) == 0;
+    for (int i = threadIdx.x; i < (y1 - y0) * nseg; i += DT_THREADS) {
+        const int y = y0 + i / nseg, xs = x0 + 16 * (i % nseg);
+        const int n = min(16, x1 - xs);
+        const bool whole_tiles = y < 4 * th;
+        uint32_t qv[4] = {0, 0, 0, 0}, tv[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int o = 0; o < 16; o++) {
+            if (o >= n) break;
+            const int x = xs + o;
+            uint32_t v;
+            if (whole_tiles && x < 4 * tw) {
+                v = s_q[y - y0][x - x0];
+            } else {  // a pixel of no tile: decimated here
+                const uint8_t *r0 = img + (int64_t)(2 * y) * st + 2 * x, *r1 = r0 + st;
+                v = box2(x, xv, r0[0], r0[1], r1[0], r1[1]);
+            }
+            const uint32_t c = s_cell[(y >> 2) - cy0][(x >> 2) - cx0];
+            const uint32_t tb = (c & 256u) ? 127u : (v > (c & 255u) ? 255u : 0u);
+            qv[o >> 2] |= v << (8 * (o & 3));
+            tv[o >> 2] |= tb << (8 * (o & 3));
+        }
+        const int64_t o = f.q_off + (int64_t)y * qw + xs;
+        if (st16 && n == 16) {
+            *reinterpret_cast<uint4 *>(qim + o) = make_uint4(qv[0], qv[1], qv[2], qv[3]);
+            *reinterpret_cast<uint4 *>(thr + o) = make_uint4(tv[0], tv[1], tv[2], tv[3]);
+        } else {
+            for (int k = 0; k < n; k++) {
+                qim[o + k] = (uint8_t)(qv[k >> 2] >> (8 * (k & 3)));
+                thr[o + k] = (uint8_t)(tv[k >> 2] >> (8 * (k & 3)));
+            }
+        }
+    }
+}
+
 // A thread per 4x4 tile: the max and min of its 3x3 tile neighbourhood
 // (cells outside the grid left out) once, then its 16 pixels. Pixels right
 // of the last whole tile column use that column and are never 127; rows
@@ -333,13 +457,6 @@ __device__ __forceinline__ void uf_unite(uint32_t *par, uint32_t a, uint32_t b) 
         }
         if (atomicCAS(par + a, a, b) == a) return;
     }
-}
-
-__device__ __forceinline__ bool runs_touch(int64_t a0, int64_t a1, int64_t b0, int64_t b1, uint8_t v) {
-    if (dmax(dmax(a0, b0), 1) <= dmin(a1, b1)) return true;
-    if (v != 255) return false;
-    if (dmax(dmax(a0, b0 + 1), 1) <= dmin(a1, b1 + 1)) return true;
-    return dmax(dmax(a0, b0 - 1), 1) <= dmin(a1, b1 - 1);
 }
 
 // The runs of row y of slots [base, base + n) that touch run (a0, a1, v),
@@ -465,6 +582,163 @@ __global__ void __launch_bounds__(256) k_row_union(const FrameDesc *frames, cons
             if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
                 uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
         }
+    }
+}
+
+// The same unions in bands: a block takes UB_ROWS rows of a frame and does
+// the unions between those rows in shared memory over band-local ids (the
+// larger id hooked under the smaller, lock-free, so a local root is its
+// set's smallest node of the band); every node then points at its local
+// root in global memory. k_band_join then joins the bands in global memory
+// (each band's first row with the row above, hash-ordered links between
+// roots as in uf_unite) and adds the last-column links of every row. The
+// same pairs are joined as by k_row_union, so the partition is the same. A
+// band with more than UB_CAP runs joins its rows in global memory instead.
+#define UB_ROWS 8
+#define UB_CAP 4608
+
+__device__ __forceinline__ uint32_t lu_find(volatile uint32_t *par, uint32_t x) {
+    uint32_t p = par[x];
+    while (p != x) {
+        const uint32_t pp = par[p];
+        if (pp != p) par[x] = pp;  // path halving: only ever an ancestor
+        x = p;
+        p = par[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void lu_unite(uint32_t *par, uint32_t a, uint32_t b) {
+    volatile uint32_t *vp = par;
+    for (;;) {
+        a = lu_find(vp, a);
+        b = lu_find(vp, b);
+        if (a == b) return;
+        if (a < b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(par + a, a, b) == a) return;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, RunArrays runs,
+                                                    const uint32_t *row_nruns) {
+    __shared__ uint32_t s_se[UB_CAP];
+    __shared__ uint32_t s_par[UB_CAP];
+    __shared__ uint8_t s_v[UB_CAP];
+    __shared__ uint32_t s_roff[UB_ROWS + 1];
+    const FrameDesc f = frames[blockIdx.y];
+    const int nband = (f.qh + UB_ROWS - 1) / UB_ROWS;
+    for (int b = blockIdx.x; b < nband; b += gridDim.x) {
+        const int y0 = b * UB_ROWS, nr = min(UB_ROWS, f.qh - y0);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int r = 0; r < nr; r++) {
+                s_roff[r] = acc;
+                acc += row_nruns[f.row0 + y0 + r];
+            }
+            s_roff[nr] = acc;
+        }
+        __syncthreads();
+        const uint32_t L = s_roff[nr];
+        if (L > UB_CAP) {
+            // too many runs to stage: the band's unions in global memory
+            for (int r = 1; r < nr; r++) {
+                const int64_t cur = f.node_off + (int64_t)(y0 + r) * f.qw, prev = cur - f.qw;
+                const int64_t ncur = s_roff[r + 1] - s_roff[r], nprev = s_roff[r] - s_roff[r - 1];
+                for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
+                    const int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
+                    const uint8_t v = runs.v[cur + i];
+                    int64_t lo = 0, hi = nprev;
+                    while (lo < hi) {
+                        const int64_t mid = (lo + hi) >> 1;
+                        if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    for (int64_t k = lo; k < nprev && (int64_t)runs.start[prev + k] <= a1 + 1; k++)
+                        if (runs.v[prev + k] == v && runs_touch(a0, a1, runs.start[prev + k], runs.end[prev + k], v))
+                            uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + k));
+                }
+            }
+            continue;
+        }
+        // stage the band's runs (local id = s_roff[row] + index)
+        for (int r = 0; r < nr; r++) {
+            const int64_t base = f.node_off + (int64_t)(y0 + r) * f.qw;
+            const uint32_t o = s_roff[r], n = s_roff[r + 1] - o;
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                s_se[o + i] = (uint32_t)runs.start[base + i] | (uint32_t)runs.end[base + i] << 16;
+                s_v[o + i] = runs.v[base + i];
+                s_par[o + i] = o + i;
+            }
+        }
+        __syncthreads();
+        // the unions of rows 1.. of the band with the row above, in shared memory
+        for (uint32_t l = s_roff[1] + threadIdx.x; l < L; l += blockDim.x) {
+            int r = 1;
+            while (s_roff[r + 1] <= l) r++;
+            const uint32_t pb = s_roff[r - 1], np = s_roff[r] - pb;
+            const int64_t a0 = s_se[l] & 0xffffu, a1 = s_se[l] >> 16;
+            const uint8_t v = s_v[l];
+            FOR_TOUCHING(s_se, s_v, pb, np, a0, a1, v, k, { lu_unite(s_par, l, (uint32_t)(pb + k)); })
+        }
+        __syncthreads();
+        // every node points at its local root (read-only walks)
+        for (uint32_t l = threadIdx.x; l < L; l += blockDim.x) {
+            uint32_t x = l;
+            while (s_par[x] != x) x = s_par[x];
+            int r = 0;
+            while (s_roff[r + 1] <= l) r++;
+            int rr = 0;
+            while (s_roff[rr + 1] <= x) rr++;
+            const int64_t node = f.node_off + (int64_t)(y0 + r) * f.qw + (l - s_roff[r]);
+            const int64_t root = f.node_off + (int64_t)(y0 + rr) * f.qw + (x - s_roff[rr]);
+            runs.parent[node] = (uint32_t)root;
+        }
+    }
+}
+
+// The joins between bands (each band's first row with the row above) and
+// the last-column links of every row (fast/unionfind.c:89-97), in global
+// memory: a block per band boundary row, then a thread per row for the
+// last column.
+__global__ void __launch_bounds__(256) k_band_join(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
+                                                   const uint32_t *row_nruns) {
+    const FrameDesc f = frames[blockIdx.y];
+    const int nband = (f.qh + UB_ROWS - 1) / UB_ROWS;
+    for (int b = 1 + blockIdx.x; b < nband; b += gridDim.x) {
+        const int64_t y = (int64_t)b * UB_ROWS;
+        const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
+        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
+        for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
+            const int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
+            const uint8_t v = runs.v[cur + i];
+            int64_t lo = 0, hi = nprev;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            for (int64_t k = lo; k < nprev && (int64_t)runs.start[prev + k] <= a1 + 1; k++)
+                if (runs.v[prev + k] == v && runs_touch(a0, a1, runs.start[prev + k], runs.end[prev + k], v))
+                    uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + k));
+        }
+    }
+    for (int64_t y = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < f.qh;
+         y += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ncur = row_nruns[f.row0 + y];
+        if (ncur == 0) continue;
+        const int64_t last = f.node_off + y * f.qw + ncur - 1;
+        const uint8_t *above = thr + f.q_off + (y - 1) * f.qw;
+        if (runs.end[last] == f.qw - 2 && runs.v[last] == 255 && above[f.qw - 1] == 255 && above[f.qw - 2] != 255)
+            uf_unite(runs.parent, (uint32_t)last, (uint32_t)(f.node_off + (int64_t)f.qw * f.qh + y - 1));
     }
 }
 
@@ -660,22 +934,8 @@ __global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const
 // 1..qh-2, against (1,0), (0,1), (-1,1), (1,1): a point where one pixel is
 // 0 and the other 255 and both labels are not AT_NOK. The (-1,1) point is
 // left out when the pixel to the left gave its (1,1) point, except at x=1;
-// x = 0 gives only (1,0). Points are emitted in (y, x, neighbour) order.
-
-__device__ __forceinline__ uint32_t point_mask(const uint8_t *a, const uint8_t *b, const uint32_t *la,
-                                               const uint32_t *lb, int64_t x, int64_t qw) {
-    if (x >= qw - 1) return 0;
-    if (x == 0) return ((a[0] ^ a[1]) == 255 && la[0] != AT_NOK && la[1] != AT_NOK) ? 1u : 0u;
-    if (la[x] == AT_NOK) return 0;
-    uint8_t v = a[x];
-    uint32_t c10 = (v ^ a[x + 1]) == 255 && la[x + 1] != AT_NOK;
-    uint32_t c01 = (v ^ b[x]) == 255 && lb[x] != AT_NOK;
-    uint32_t cm1 = (v ^ b[x - 1]) == 255 && lb[x - 1] != AT_NOK;
-    uint32_t c11 = (v ^ b[x + 1]) == 255 && lb[x + 1] != AT_NOK;
-    uint32_t left11 = x > 1 && (a[x - 1] ^ b[x]) == 255 && la[x - 1] != AT_NOK && lb[x] != AT_NOK;
-    return c10 | c01 << 1 | (cm1 & (left11 ^ 1u)) << 2 | c11 << 3;
-}
-
+// x = 0 gives only (1,0) (point_mask). Points are emitted in (y, x,
+// neighbour) order.
 
 // Block-per-row forms of the point passes (a block scan per 256 columns),
 // for batches too small to fill the GPU with a warp per row.
@@ -730,17 +990,6 @@ __global__ void k_point_emit_block(const FrameDesc *frames, const uint8_t *thr, 
 // A warp per row for both passes: the row's points counted, then emitted
 // in (x, neighbour) order at the row's offset (warp scans, no block
 // barriers).
-__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t *total) {
-    const int lane = threadIdx.x & 31;
-    uint32_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    *total = __shfl_sync(0xffffffffu, incl, 31);
-    return incl - v;
-}
 
 __global__ void __launch_bounds__(256) k_point_count(const FrameDesc *frames, const uint8_t *thr,
                                                      const uint32_t *lab, uint64_t *row_npts) {
@@ -797,55 +1046,9 @@ __global__ void __launch_bounds__(256) k_point_emit(const FrameDesc *frames, con
 }
 
 // ---------------------------------------------------------------------------
-// 7. Clusters, by hashing (fast/clusters.c:318-382 groups points by their
-// label pair in a hash table too). The distinct pairs go into an
-// open-addressing table (each warp inserts each distinct pair of its 32
-// points once and adds its count); the few distinct pairs are sorted, which
-// gives every cluster its index in (larger, smaller) label order; each point
-// then carries its cluster index, and a stable radix sort on that index of
-// only log2(clusters) bits groups the points in emission order. A probe
-// that runs past CH_PROBES slots sets *full: the caller then groups by the
-// full sort instead.
-#define CH_EMPTY 0xffffffffffffffffull
-#define CH_PROBES 64
-
-__device__ __forceinline__ uint32_t ch_hash(uint64_t k) {
-    k ^= k >> 33;
-    k *= 0xff51afd7ed558ccdull;
-    k ^= k >> 33;
-    return (uint32_t)k;
-}
-
-__global__ void k_cluster_hash(const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount, uint32_t mask,
-                               uint32_t *full) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = i0 + threadIdx.x;
-        const bool valid = i < n;
-        const uint64_t k = valid ? key[i] : CH_EMPTY;
-        const uint32_t peers = __match_any_sync(0xffffffffu, k);
-        if (!valid || lane != __ffs(peers) - 1) continue;
-        uint32_t slot = ch_hash(k) & mask;
-        bool found = false;
-        for (int p = 0; p < CH_PROBES; p++) {
-            uint64_t cur = *(volatile uint64_t *)(tkeys + slot);
-            if (cur == CH_EMPTY) {
-                const unsigned long long old =
-                    atomicCAS(reinterpret_cast<unsigned long long *>(tkeys + slot), CH_EMPTY, k);
-                cur = old == CH_EMPTY ? k : old;
-            }
-            if (cur == k) {
-                found = true;
-                break;
-            }
-            slot = (slot + 1) & mask;
-        }
-        if (found)
-            atomicAdd(tcount + slot, (uint32_t)__popc(peers));
-        else
-            atomicOr(full, 1u);
-    }
-}
+// 7. Clusters (fast/clusters.c:16-66, 318-382). The pair table and the
+// placing of the points are in at_cluster.cu; here the distinct pairs of
+// the table, and the fallback when the table overflows.
 
 // The occupied slots, in no particular order: (pair, slot).
 __global__ void k_cluster_collect(const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
@@ -867,39 +1070,6 @@ __global__ void k_cluster_collect(const uint64_t *tkeys, uint32_t size, uint64_t
     }
 }
 
-// Cluster r (in pair order): its table slot gets r; its point count and
-// its frame (the frame whose node range holds the larger label).
-__global__ void k_cluster_rank(const uint64_t *skeys, const uint32_t *sslots, int64_t ncl, const uint32_t *tcount,
-                               uint32_t *rank_of_slot, uint32_t *ccount, int nb, const FrameDesc *frames,
-                               int nframes, int32_t *cframe) {
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < ncl; r += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = sslots[r];
-        rank_of_slot[s] = (uint32_t)r;
-        ccount[r] = tcount[s];
-        const int64_t node = (int64_t)(skeys[r] >> nb);
-        int lo = 0, hi = nframes - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (frames[mid].node_off <= node)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        cframe[r] = lo;
-    }
-}
-
-// Each point's cluster index (its pair is in the table).
-__global__ void k_cluster_assign(const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
-                                 const uint32_t *rank_of_slot, uint32_t *cidx) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = key[i];
-        uint32_t slot = ch_hash(k) & mask;
-        for (int p = 0; p < CH_PROBES && tkeys[slot] != k; p++) slot = (slot + 1) & mask;
-        cidx[i] = rank_of_slot[slot];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // 7b. Clusters by the full sort (the fallback): after the stable sort by
 // key, each run of equal keys is a cluster (points in emission order).
@@ -910,11 +1080,13 @@ __global__ void k_cluster_heads(const uint64_t *key, int64_t n, uint32_t *head) 
 }
 
 __global__ void k_cluster_starts(const uint64_t *key, const uint32_t *head, const uint32_t *head_scan, int64_t n,
-                                 int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe) {
+                                 int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe,
+                                 uint64_t *ckey) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         if (!head[i]) continue;
         uint32_t c = head_scan[i];
         cstart[c] = (uint32_t)i;
+        ckey[c] = key[i];
         int64_t node = (int64_t)(key[i] >> nb);
         int lo = 0, hi = nframes - 1;  // the frame whose node range holds node
         while (lo < hi) {
@@ -1470,7 +1642,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             ymin = min(ymin, s_bb[2][w]);
             ymax = max(ymax, s_bb[3][w]);
         }
-        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < prm.tag_width) continue;
+        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < f.tag_width) continue;
         const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
         const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
 
@@ -1528,8 +1700,8 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
             }
             int rev = dot < 0.0f;
             int ok = 1;
-            if (!prm.reversed_border && rev) ok = 0;
-            if (!prm.normal_border && !rev) ok = 0;
+            if (!f.reversed_border && rev) ok = 0;
+            if (!f.normal_border && !rev) ok = 0;
             s_ok = ok;
             s_rev = rev;
         }
@@ -1925,7 +2097,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const Fra
                     double pp = (len[0] + len[1] + len[2]) / 2.0;
                     area = area + sqrt(pp * (pp - len[0]) * (pp - len[1]) * (pp - len[2]));
                 }
-                if (area < 0.95 * (double)prm.tag_width * (double)prm.tag_width) ok = false;
+                if (area < 0.95 * (double)f.tag_width * (double)f.tag_width) ok = false;
             }
             for (int i = 0; ok && i < 4; i++) {
                 // convexity (quads.c:1112-1124)
@@ -2195,7 +2367,7 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             ymin = min(ymin, __shfl_xor_sync(FULL, ymin, o));
             ymax = max(ymax, __shfl_xor_sync(FULL, ymax, o));
         }
-        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < prm.tag_width) continue;
+        if ((int64_t)(xmax - xmin) * (int64_t)(ymax - ymin) < f.tag_width) continue;
         FITW_PROF(2)
         const float cx = (float)((double)(xmin + xmax) * 0.5 + 0.05118);
         const float cy = (float)((double)(ymin + ymax) * 0.5 + -0.028581);
@@ -2234,8 +2406,8 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
             for (int i = nv; i < n; i++) dot = __fadd_rn(dot, s_term[i]);
             const int rev = dot < 0.0f;
             int ok = 1;
-            if (!prm.reversed_border && rev) ok = 0;
-            if (!prm.normal_border && !rev) ok = 0;
+            if (!f.reversed_border && rev) ok = 0;
+            if (!f.normal_border && !rev) ok = 0;
             okrev = ok | rev << 1;
         }
         okrev = __shfl_sync(FULL, okrev, 0);
@@ -2562,7 +2734,7 @@ __global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *fram
                     double pp = (len[0] + len[1] + len[2]) / 2.0;
                     area = area + sqrt(pp * (pp - len[0]) * (pp - len[1]) * (pp - len[2]));
                 }
-                if (area < 0.95 * (double)prm.tag_width * (double)prm.tag_width) ok = false;
+                if (area < 0.95 * (double)f.tag_width * (double)f.tag_width) ok = false;
             }
             for (int i = 0; ok && i < 4; i++) {
                 int i0 = i, i1 = (i + 1) & 3, i2 = (i + 2) & 3;
@@ -3375,9 +3547,20 @@ __device__ __forceinline__ int prefer(int pref, double a, double b) {
 // group depends only on that group's detections in quad order; so the
 // groups are resolved independently (one thread each, the rare groups of
 // two or more), and the survivors are placed by their stable rank by id.
+// The bucket count of the reference's cluster table for a quad image of
+// w x h at one thread (fast/clusters.c:97-103, fast/detector.c:223).
+__device__ __forceinline__ uint64_t ref_buckets(int64_t w, int64_t h) {
+    const int64_t chunk = 1 + (h - 1) / 6;
+    int64_t n = 1024;
+    while (n < chunk * w / 64 && n < 65536) n <<= 1;
+    return (uint64_t)n;
+}
+
 __global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                            const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
-                           const int64_t *out_off, int64_t *out_n) {
+                           const int64_t *out_off, int64_t *out_n, const FrameDesc *frames, RefOrder ref,
+                           const uint32_t *qcl, const uint64_t *ckey, int nb, uint64_t *okey, uint32_t *idx2,
+                           uint32_t *err) {
     __shared__ uint32_t sh[32];
     const int f = blockIdx.x;
     if (f >= nframes) return;
@@ -3395,6 +3578,49 @@ __global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, c
         n += total;
     }
     __syncthreads();
+    if (ref.need[f]) {
+        // detections that share an id take the reference's quad order:
+        // (bucket, key) of their clusters' reference roots
+        // (fast/clusters.c:44, 338-356), then family; the others keep
+        // theirs (only detections of one id are ever compared)
+        const FrameDesc fd = frames[f];
+        const uint64_t nbuck = ref_buckets(fd.qw, fd.qh);
+        const uint32_t nt = ref.nt[f];
+        const uint32_t *tl = ref.tlabel + (int64_t)f * AT_REF_MAXT, *tr = ref.troot + (int64_t)f * AT_REF_MAXT;
+        const uint64_t lmask = ((uint64_t)1 << nb) - 1;
+        uint64_t *k0 = okey + 2 * a, *k1 = k0 + (b - a);
+        for (int64_t p = threadIdx.x; p < n; p += blockDim.x) {
+            const uint32_t s = ix[p];
+            const uint64_t key = ckey[qcl[s / nfam]];
+            const uint32_t lh = (uint32_t)(key >> nb), ll = (uint32_t)(key & lmask);
+            uint32_t th = 0xffffffffu, tlo = 0xffffffffu;
+            for (uint32_t t = 0; t < nt; t++) {
+                if (tl[t] == lh) th = t;
+                if (tl[t] == ll) tlo = t;
+            }
+            if (th != 0xffffffffu && tlo != 0xffffffffu) {
+                const uint64_t rh = tr[th], rl = tr[tlo];
+                if (rh == 0xffffffffu || rl == 0xffffffffu) atomicOr(err, AT_ERR_ORDER);
+                const uint64_t hi = rh > rl ? rh : rl, lo = rh > rl ? rl : rh;
+                const uint64_t cid = hi << 32 | lo;
+                const uint64_t bucket = ((cid * 2654435761ull) >> 32) & (nbuck - 1);
+                k0[p] = bucket << 32 | hi;
+                k1[p] = lo << 8 | (uint64_t)(s % nfam);
+            } else {
+                k0[p] = ~0ull;
+                k1[p] = (uint64_t)p;
+            }
+        }
+        __syncthreads();
+        for (int64_t p = threadIdx.x; p < n; p += blockDim.x) {
+            int64_t r = 0;
+            for (int64_t q = 0; q < n; q++) r += k0[q] < k0[p] || (k0[q] == k0[p] && k1[q] < k1[p]);
+            idx2[a + r] = ix[p];
+        }
+        __syncthreads();
+        for (int64_t p = threadIdx.x; p < n; p += blockDim.x) ix[p] = idx2[a + p];
+        __syncthreads();
+    }
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) rm[i] = 0;
     __syncthreads();
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
@@ -3452,9 +3678,12 @@ __global__ void k_finalize(int nframes, const int64_t *frame_qstart, int nfam, c
 
 // The quads in cluster order (so grouped by frame), and their count.
 __global__ void k_gather_quads(const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                               GpuQuad *out, uint32_t *nq) {
+                               GpuQuad *out, uint32_t *nq, uint32_t *qcl) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (ok[i]) out[scan[i]] = quads[i];
+        if (ok[i]) {
+            out[scan[i]] = quads[i];
+            qcl[scan[i]] = (uint32_t)i;
+        }
         if (i == n - 1) *nq = scan[i] + ok[i];
     }
 }
@@ -3563,6 +3792,19 @@ void launch_threshold(const Launch &L, const FrameDesc *frames, const uint8_t *q
     k_threshold<<<frame_grid(L), 256, 0, L.stream>>>(frames, qim, tmax, tmin, thr, diff);
 }
 
+void launch_decimate_threshold(const Launch &L, const FrameDesc *frames, int64_t max_cells, uint8_t *qim, uint8_t *thr,
+                               int32_t diff) {
+    // blocks per frame: enough regions for the frame with the most cells
+    // (each block finds its region from its frame's width; extra ones exit)
+    k_decimate_threshold<<<dim3((unsigned)max_cells, (unsigned)L.nframes), DT_THREADS, 0, L.stream>>>(frames, qim, thr,
+                                                                                                     diff);
+}
+
+int64_t decimate_threshold_blocks(int64_t qw, int64_t qh) {
+    const int64_t cw = (qw + 3) / 4, ch = (qh + 3) / 4;
+    return ((cw + DT_COLS - 1) / DT_COLS) * ((ch + DT_ROWS - 1) / DT_ROWS);
+}
+
 void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uint8_t *tmp) {
     k_morph<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, tmp, 1);
     k_morph<<<frame_grid(L), 256, 0, L.stream>>>(frames, tmp, thr, 0);
@@ -3574,13 +3816,17 @@ int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr,
     const int64_t rb = (max_qh + 7) / 8;
     k_row_runs<<<dim3((unsigned)(rb < 148 * 8 ? rb : 148 * 8), (unsigned)L.nframes), 256, 0, L.stream>>>(frames, thr,
                                                                                                         runs, row_nruns);
-    k_row_union<<<rg, 256, 0, L.stream>>>(frames, thr, runs, row_nruns);
+    const int64_t nb = (max_qh + UB_ROWS - 1) / UB_ROWS;
+    k_band_union<<<dim3((unsigned)(nb < 148 * 4 ? nb : 148 * 4), (unsigned)L.nframes), 256, 0, L.stream>>>(
+        frames, runs, row_nruns);
+    k_band_join<<<dim3((unsigned)(nb < 148 * 4 ? nb : 148 * 4), (unsigned)L.nframes), 256, 0, L.stream>>>(
+        frames, thr, runs, row_nruns);
     k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
     if (warp_rows(L))
         k_labels_w<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
     else
         k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
-    return 4;
+    return 5;
 }
 
 void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
@@ -3599,63 +3845,9 @@ void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *
         k_point_emit_block<<<frame_grid(L), 256, 0, L.stream>>>(frames, thr, lab, row_pt_off, pt_key, pt_val, nb);
 }
 
-void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount,
-                         uint32_t mask, uint32_t *full) {
-    k_cluster_hash<<<flat_blocks(n, 256), 256, 0, s>>>(key, n, tkeys, tcount, mask, full);
-}
-
 void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
                             uint32_t *count) {
     k_cluster_collect<<<flat_blocks(size, 256), 256, 0, s>>>(tkeys, size, okeys, oslots, count);
-}
-
-// Distinct keys in key order by rank: a warp per key counts the keys
-// smaller than it (its place, the keys being distinct) and stores the key
-// and its value there. n^2 / 32 comparisons a warp-instruction each, spread
-// over the whole GPU: about 12 us for the 3.8k keys of a 4K frame, and under
-// the six passes of a device-wide radix sort up to about 16k keys.
-__global__ void __launch_bounds__(256) k_rank_sort(const uint64_t *kin, const uint32_t *vin, int n, uint64_t *kout,
-                                                   uint32_t *vout) {
-    const int lane = threadIdx.x & 31;
-    const int i = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (i >= n) return;  // the whole warp
-    const uint64_t ki = kin[i];
-    uint32_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-    int j = lane;
-    for (; j + 96 < n; j += 128) {
-        const uint64_t a = kin[j], b = kin[j + 32], c = kin[j + 64], d = kin[j + 96];
-        c0 += a < ki;
-        c1 += b < ki;
-        c2 += c < ki;
-        c3 += d < ki;
-    }
-    for (; j < n; j += 32) c0 += kin[j] < ki;
-    uint32_t cnt = c0 + c1 + c2 + c3;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if (lane == 0) {
-        kout[cnt] = ki;
-        vout[cnt] = vin[i];
-    }
-}
-
-bool launch_sort_distinct(cudaStream_t s, const uint64_t *kin, const uint32_t *vin, int64_t n, uint64_t *kout,
-                          uint32_t *vout) {
-    if (n > RANK_SORT_CAP || n < 1) return false;
-    k_rank_sort<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(kin, vin, (int)n, kout, vout);
-    return true;
-}
-
-void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
-                         const uint32_t *tcount, uint32_t *rank_of_slot, uint32_t *ccount, int nb,
-                         const FrameDesc *frames, int nframes, int32_t *cframe) {
-    k_cluster_rank<<<flat_blocks(ncl, 256), 256, 0, s>>>(skeys, sslots, ncl, tcount, rank_of_slot, ccount, nb, frames,
-                                                        nframes, cframe);
-}
-
-void launch_cluster_assign(cudaStream_t s, const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
-                           const uint32_t *rank_of_slot, uint32_t *cidx) {
-    k_cluster_assign<<<flat_blocks(n, 256), 256, 0, s>>>(key, n, tkeys, mask, rank_of_slot, cidx);
 }
 
 void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head) {
@@ -3663,8 +3855,10 @@ void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32
 }
 
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
-                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe) {
-    k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe);
+                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe,
+                           uint64_t *ckey) {
+    k_cluster_starts<<<flat_blocks(n, 256), 256, 0, s>>>(key, head, head_scan, n, nb, frames, nframes, cstart, cframe,
+                                                         ckey);
 }
 
 // One size class of the warp fit kernel on stream s: enough blocks to fill
@@ -3733,9 +3927,9 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
 }
 
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                         GpuQuad *out, uint32_t *nq) {
+                         GpuQuad *out, uint32_t *nq, uint32_t *qcl) {
     if (n <= 0) return;
-    k_gather_quads<<<flat_blocks(n, 256), 256, 0, s>>>(quads, ok, scan, n, out, nq);
+    k_gather_quads<<<flat_blocks(n, 256), 256, 0, s>>>(quads, ok, scan, n, out, nq, qcl);
 }
 
 void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *nq, int nframes, int nfam,
@@ -3768,6 +3962,9 @@ void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm
 
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
-                     const int64_t *out_off, int64_t *out_n) {
-    k_finalize<<<nframes, 256, 0, s>>>(nframes, frame_qstart, nfam, dets, det_ok, idx, removed, out, out_off, out_n);
+                     const int64_t *out_off, int64_t *out_n, const FrameDesc *frames, const RefOrder &ref,
+                     const uint32_t *qcl, const uint64_t *ckey, int nb, uint64_t *okey, uint32_t *idx2,
+                     uint32_t *err) {
+    k_finalize<<<nframes, 256, 0, s>>>(nframes, frame_qstart, nfam, dets, det_ok, idx, removed, out, out_off, out_n,
+                                       frames, ref, qcl, ckey, nb, okey, idx2, err);
 }

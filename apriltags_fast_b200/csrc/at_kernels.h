@@ -44,6 +44,11 @@ void launch_blur(const Launch &L, const FrameDesc *frames, uint8_t *qim, uint8_t
                  const BlurTaps &taps, bool sharpen);
 void launch_threshold(const Launch &L, const FrameDesc *frames, const uint8_t *qim, uint8_t *tmax, uint8_t *tmin,
                       uint8_t *thr, int32_t diff);
+// Decimate 2 + tile max/min + threshold in one pass (no blur): max_blocks
+// from decimate_threshold_blocks of the batch's largest frame.
+void launch_decimate_threshold(const Launch &L, const FrameDesc *frames, int64_t max_blocks, uint8_t *qim,
+                               uint8_t *thr, int32_t diff);
+int64_t decimate_threshold_blocks(int64_t qw, int64_t qh);
 void launch_deglitch(const Launch &L, const FrameDesc *frames, uint8_t *thr, uint8_t *tmp);
 int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs, uint32_t *row_nruns,
                    uint32_t *lab, int32_t min_px, int64_t max_qh);
@@ -52,28 +57,44 @@ void launch_point_count(const Launch &L, const FrameDesc *frames, const uint8_t 
 void launch_point_emit(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                        const uint64_t *row_pt_off, uint64_t *pt_key, uint64_t *pt_val, int nb);
 void launch_cluster_heads(cudaStream_t s, const uint64_t *key, int64_t n, uint32_t *head);
-void launch_cluster_hash(cudaStream_t s, const uint64_t *key, int64_t n, uint64_t *tkeys, uint32_t *tcount,
-                         uint32_t mask, uint32_t *full);
 void launch_cluster_collect(cudaStream_t s, const uint64_t *tkeys, uint32_t size, uint64_t *okeys, uint32_t *oslots,
                             uint32_t *count);
-// Distinct 64-bit keys with 32-bit values in key order (a rank per key);
-// false (nothing launched) above RANK_SORT_CAP keys.
-#define RANK_SORT_CAP 16384
-bool launch_sort_distinct(cudaStream_t s, const uint64_t *kin, const uint32_t *vin, int64_t n, uint64_t *kout,
-                          uint32_t *vout);
-void launch_cluster_rank(cudaStream_t s, const uint64_t *skeys, const uint32_t *sslots, int64_t ncl,
-                         const uint32_t *tcount, uint32_t *rank_of_slot, uint32_t *ccount, int nb,
-                         const FrameDesc *frames, int nframes, int32_t *cframe);
-void launch_cluster_assign(cudaStream_t s, const uint64_t *key, int64_t n, const uint64_t *tkeys, uint32_t mask,
-                           const uint32_t *rank_of_slot, uint32_t *cidx);
+// Clusters without sorting the points (at_cluster.cu). The pair table:
+// key (label pair), point count, first and last row with points, per slot.
+struct PairTable {
+    uint64_t *keys;
+    uint32_t *count, *ymin, *ymax;
+    uint32_t mask;
+};
+// Scratch of the pair ordering: per pair its frame, per frame its pair count,
+// first pair (nframes + 1) and a cursor, the pairs grouped by frame, and
+// the block sums of the scans (pair_scan_blocks each).
+struct PairScratch {
+    uint32_t *kframe, *fcount, *foff, *fcur;
+    uint64_t *gkeys;
+    uint32_t *gslots, *bsum_a, *bsum_b;
+};
+void launch_pair_hash(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                      const PairTable &T, uint32_t *full, unsigned long long *npoints);
+void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *oslots, int64_t ncl, int nb,
+                       const FrameDesc *frames, int nframes, const PairTable &T, const PairScratch &P,
+                       uint64_t *skeys, uint32_t *sslots, uint32_t *rank_of_slot, uint32_t *ccount, uint32_t *cspan,
+                       uint32_t *cy0, int32_t *cframe, uint32_t *cstart, uint32_t *spanoff);
+int64_t pair_scan_blocks(int64_t ncl);
+void launch_point_place(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                        const PairTable &T, const uint32_t *rank_of_slot, const uint32_t *cstart,
+                        const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0, int64_t ncl,
+                        uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err);
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
-                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe);
+                           int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe,
+                           uint64_t *ckey);
 void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cudaStream_t side3, cudaEvent_t fork,
                       cudaEvent_t join, cudaEvent_t join2, cudaEvent_t join3, const FrameDesc *frames, const GpuParams &prm, const uint8_t *qim,
                       const uint64_t *pts, const uint32_t *cstart, const int32_t *cframe, int64_t nclusters,
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err);
+// also each gathered quad's cluster index (qcl)
 void launch_gather_quads(cudaStream_t s, const GpuQuad *quads, const uint32_t *ok, const uint32_t *scan, int64_t n,
-                         GpuQuad *out, uint32_t *nq);
+                         GpuQuad *out, uint32_t *nq, uint32_t *qcl);
 void launch_frame_bounds(cudaStream_t s, const GpuQuad *quads, const uint32_t *nq, int nframes, int nfam,
                          int64_t *qstart, int64_t *out_off);
 void launch_output(cudaStream_t s, int nframes, const int64_t *qstart, const GpuDetection *out,
@@ -90,6 +111,31 @@ struct DecodeScratch {
 void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm, const GpuFamily *fams,
                    const uint8_t *img, const uint8_t *qim, const GpuQuad *quads, int64_t max_quads,
                    const DecodeScratch &scr, GpuDetection *dets, uint32_t *det_ok);
+// The reference's order of the quads whose detections share an id
+// (at_order.cu). Per frame: whether it has such detections (need), the
+// target components (GPU labels, pixel counts, and after the replay their
+// roots in the reference's packed node numbering); per node, the frame's
+// target runs compacted by row (tlist); per row, their count (trow); per
+// row plus one per frame, the runs above the row (rpre).
+#define AT_REF_MAXT 192
+struct RefOrder {
+    uint32_t *need, *nt;
+    uint32_t *tlabel, *tpx, *troot;
+    uint64_t *tlist;
+    uint32_t *trow;
+    uint32_t *rpre;
+};
+// Bytes of the replay's arrays for rows of at most capr runs (shared
+// memory, or a global scratch region per frame when scratch is not null).
+size_t ref_replay_bytes(int64_t capr);
+bool ref_replay_set_smem(size_t bytes);
+void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
+                      const uint32_t *row_nruns, int nfam, const int64_t *qstart, const GpuDetection *dets,
+                      const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb, int64_t capr,
+                      uint8_t *scratch, size_t scratch_per_frame, const RefOrder &ref, uint32_t *err);
+// okey: 2 u64 + 1 u32 per detection slot (the order keys, a second index)
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,
-                     const int64_t *out_off, int64_t *out_n);
+                     const int64_t *out_off, int64_t *out_n, const FrameDesc *frames, const RefOrder &ref,
+                     const uint32_t *qcl, const uint64_t *ckey, int nb, uint64_t *okey, uint32_t *idx2,
+                     uint32_t *err);

@@ -52,6 +52,7 @@ struct at_server {
     bool stop = false;
     uint64_t next_ticket = 1;
     double bytes_per_pixel = 64.0;  // device bytes per input pixel, learned from the batches
+    int64_t queued_bytes = 0;       // estimated device bytes of the pending and running frames
     at_server_stats st{};
 };
 
@@ -76,6 +77,7 @@ static void worker(at_server *s, int w) {
                 batch.push_back(r);
                 s->pending.pop_front();
             }
+            if (batch.empty()) continue;
             s->st.batches++;
             s->st.in_flight += (int64_t)batch.size();
         }
@@ -113,6 +115,7 @@ static void worker(at_server *s, int w) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
             for (auto &o : out) s->done.push_back(o);
+            for (auto &r : batch) s->queued_bytes -= r.est;
             s->st.completed += (int64_t)batch.size();
             s->st.in_flight -= (int64_t)batch.size();
             if (px > 0 && (double)arena / (double)px > s->bytes_per_pixel) s->bytes_per_pixel = (double)arena / (double)px;
@@ -149,15 +152,44 @@ uint64_t at_server_submit(at_server *s, const at_frame *frame, uint64_t user) {
     std::lock_guard<std::mutex> lk(s->mu);
     const int64_t est = (int64_t)(s->bytes_per_pixel * (double)(frame->width * frame->height));
     const int64_t share = s->cfg.memory_budget / s->cfg.workers;
-    if (s->stop || est > share) {
+    // a frame is admitted while the device bytes of everything pending or
+    // running, this frame included, stay within the budget (and it fits
+    // one worker's share on its own)
+    if (s->stop || est > share || s->queued_bytes + est > s->cfg.memory_budget) {
         s->st.rejected++;
         return 0;
     }
     Request r{s->next_ticket++, user, *frame, now_s(), est};
     s->pending.push_back(r);
+    s->queued_bytes += est;
     s->st.admitted++;
     s->cv_work.notify_one();
     return r.ticket;
+}
+
+int at_server_cancel(at_server *s, uint64_t ticket) {
+    if (s == nullptr) return 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+            if (it->ticket != ticket) continue;
+            at_server_result o;
+            memset(&o, 0, sizeof o);
+            o.ticket = it->ticket;
+            o.user = it->user;
+            o.status = AT_SERVER_CANCELLED;
+            o.worker = -1;
+            o.t_submit = it->t_submit;
+            o.t_start = o.t_done = now_s();
+            s->queued_bytes -= it->est;
+            s->pending.erase(it);
+            s->done.push_back(o);
+            s->st.cancelled++;
+            s->cv_done.notify_all();
+            return 1;
+        }
+    }
+    return 0;
 }
 
 int64_t at_server_poll(at_server *s, at_server_result *out, int64_t max, int32_t wait_ms) {

@@ -6,8 +6,8 @@ family code tables (a 1-module white border, as apriltag_to_image draws
 them), placed by random homographies without overlap, optional filled
 rectangle/ellipse distractors and an illumination ramp, a Gaussian blur,
 rounded and clamped to u8. Tag codes are drawn uniformly from the
-family's code table, with replacement (Config.replacement; without it
-every id in a frame is distinct).
+family's code table, with replacement, so ids may repeat in a frame
+(Config.replacement=False draws distinct ids).
 
     img, truth = make_frame(CONFIGS["1080p"], seed=2)
 
@@ -36,7 +36,7 @@ class Config:
     distractors: int = 0
     ramp: tuple | None = None        # illumination ramp (lo, hi)
     gradient: tuple = (60.0, 190.0)
-    replacement: bool = False        # draw tag codes with replacement (ids may repeat)
+    replacement: bool = True         # draw tag codes with replacement (ids may repeat)
 
 
 CONFIGS = {

@@ -180,7 +180,10 @@ int at_detector_set_batch_split(at_detector *td, int pipelines);
    share (memory_budget / workers) of device memory at the learned bytes
    per pixel, and detects them as one batch, so frames that arrive while a
    batch is on the GPU are admitted to the next one and overlap it. A frame
-   that alone exceeds a worker's share is rejected. Each frame's
+   is rejected when it alone exceeds a worker's share, or when the device
+   bytes of all pending and running frames with it would exceed the
+   budget (bytes are estimated per input pixel from the batches so far, so
+   a flood of requests is turned away instead of queued). Each frame's
    detections equal at_detect's for that frame alone. The pixels must stay
    valid and unchanged until the frame's result has been polled. */
 typedef struct at_server at_server;
@@ -189,9 +192,10 @@ typedef struct at_server_config {
     int32_t max_batch;     /* frames per batch (default 16) */
     int64_t memory_budget; /* device bytes for all workers' frames (default 24 GiB) */
 } at_server_config;
+#define AT_SERVER_CANCELLED (-1) /* at_server_result.status of a cancelled request */
 typedef struct at_server_result {
     uint64_t ticket, user;   /* from at_server_submit */
-    int32_t status;          /* 0, or the worker detector's at_detector_last_error */
+    int32_t status;          /* 0, AT_SERVER_CANCELLED, or the worker detector's at_detector_last_error */
     int32_t batch_frames;    /* frames in the batch it ran in */
     int32_t worker;
     int32_t pad;
@@ -200,13 +204,18 @@ typedef struct at_server_result {
     double t_submit, t_start, t_done; /* seconds, steady clock */
 } at_server_result;
 typedef struct at_server_stats {
-    int64_t admitted, rejected, completed, batches, in_flight, pending;
+    int64_t admitted, rejected, completed, batches, in_flight, pending, cancelled;
     int64_t peak_arena_bytes; /* the largest worker arena seen */
     double bytes_per_pixel;   /* the admission estimate in use */
 } at_server_stats;
 at_server *at_server_create(const at_detector *params, const at_server_config *cfg);
 /* Returns the request's ticket, or 0 when the frame is invalid or rejected. */
 uint64_t at_server_submit(at_server *s, const at_frame *frame, uint64_t user);
+/* Cancels a request that is still queued: it leaves the queue, and its
+   result (status AT_SERVER_CANCELLED, no detections) is delivered by
+   at_server_poll. Returns 1, or 0 when the ticket is unknown or its frame
+   is already on the GPU or done (it then completes normally). */
+int at_server_cancel(at_server *s, uint64_t ticket);
 /* Copies up to max finished results (waiting up to wait_ms for the first);
    returns how many. */
 int64_t at_server_poll(at_server *s, at_server_result *out, int64_t max, int32_t wait_ms);

@@ -7,6 +7,7 @@ import pytest
 
 import apriltags_fast_b200 as AT
 from apriltags_fast_b200 import synth
+from oracle import oracle as O
 from tests import helpers as H
 
 pytestmark = pytest.mark.gpu
@@ -104,6 +105,32 @@ def test_uneven_batch_with_family_sets_equals_single():
         assert all(int(x["family"]) == (0 if masks[i] == 1 else 1) for x in one)
 
 
+def test_uneven_batch_of_64_equals_reference_per_frame():
+    """The batched workload: 64 frames of sizes drawn from 640x480 to
+    3840x2160, each with 0-40 tags of tag36h11 or tag25h9 (codes drawn with
+    replacement) and its own family set, in one batch. Each frame's
+    detections and quad count equal the reference's own (oracle/_ref, one
+    thread) run on that frame alone with that frame's family, in its order;
+    the family index is the detector's (0 or 1)."""
+    if O.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    frames, fams = synth.uneven_batch(64, 5)
+    det = AT.Detector(["tag36h11", "tag25h9"], 2)
+    masks = [1 if f == "tag36h11" else 2 for f in fams]
+    batch = det.detect_batch(frames, family_masks=masks)
+    nq = list(det.last_batch_nquads)
+    sizes = set()
+    for i, f in enumerate(frames):
+        ref, ref_nq = O.ref_detect(f, [fams[i]], [2])
+        got = [d.key() for d in batch[i]]
+        fi = 0 if fams[i] == "tag36h11" else 1
+        assert all(g[0] == fi for g in got), i
+        assert [g[1:] for g in got] == [r[1:] for r in ref], i
+        assert nq[i] == ref_nq, i
+        sizes.add(f.shape)
+    assert len(sizes) == 4
+
+
 def test_batch_split_equals_one_pipeline():
     """A batch spread over 2-4 pipelines (helper detectors on their own
     threads) gives the same detections and quad counts, frame by frame, as
@@ -132,3 +159,48 @@ def test_shutdown_with_batch_pipelines_then_detect_again():
     det.shutdown()
     again = [d.tobytes() for d in det.detect_batch(frames, as_arrays=True)]
     assert again == first
+
+
+def test_server_cancel_queued_requests():
+    """Requests cancelled while still queued come back with status
+    SERVER_CANCELLED and no detections; the others complete unchanged."""
+    det = AT.Detector(["tag36h11"], 2)
+    frames = synth.serve_mix(4, 21) + H.golden_images()
+    alone = _alone(det, frames)
+    big = synth.make_frame(synth.CONFIGS["serve_2160p"], 5)[0]
+    srv = AT.Server(det, workers=1, max_batch=1)
+    try:
+        first = srv.submit(big, user=99)  # keeps the one worker busy
+        tickets = [(srv.submit(f, user=i), i) for i, f in enumerate(frames) for _ in range(2)]
+        cancelled = {t for t, _ in tickets[1::2] if srv.cancel(t)}
+        assert len(cancelled) >= len(tickets) // 2 - 1
+        res = _drain(srv, len(tickets) + 1)
+        assert len(res) == len(tickets) + 1
+        for r in res:
+            if r["ticket"] in cancelled:
+                assert r["status"] == AT.SERVER_CANCELLED and len(r["detections"]) == 0
+            elif r["user"] != 99:
+                assert r["status"] == 0
+                assert (r["detections"].tobytes(), r["nquads"]) == alone[r["user"]]
+        st = srv.stats()
+        assert st["cancelled"] == len(cancelled) and st["pending"] == 0
+    finally:
+        srv.close()
+
+
+def test_server_rejects_when_queued_bytes_exceed_budget():
+    """A burst bigger than the budget: the frames whose queued device bytes
+    would pass the budget are turned away; the admitted ones finish."""
+    det = AT.Detector(["tag36h11"], 2)
+    img = H.golden_images()[0]
+    srv = AT.Server(det, workers=1, max_batch=2, memory_budget=80 << 20)
+    try:
+        tickets = [srv.submit(img, user=i) for i in range(40)]
+        admitted = [t for t in tickets if t > 0]
+        assert 0 < len(admitted) < len(tickets)
+        res = _drain(srv, len(admitted))
+        assert len(res) == len(admitted) and all(r["status"] == 0 for r in res)
+        st = srv.stats()
+        assert st["rejected"] == len(tickets) - len(admitted)
+    finally:
+        srv.close()

@@ -141,3 +141,36 @@ def test_oracle_equals_reference(seed):
     r = O.detect(img, [H.oracle_family(f) for f in fams], bits, p, order=O.ORDER_REF)
     assert len(r.quads) == nq
     assert r.dets == ref
+
+
+def _config_frame(name, seed, replacement=True):
+    from apriltags_fast_b200 import synth
+
+    cfg = synth.Config(**{**synth.CONFIGS[name].__dict__, "replacement": replacement})
+    return cfg, synth.make_frame(cfg, seed)[0]
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [0, 5, 1001])
+def test_oracle_equals_reference_1080p(seed):
+    """The 1920x1080 workload (24 tags, 200 distractors, codes drawn with
+    replacement), decimate 2, bits 2: the oracle equals the reference in
+    its own order, and the quad count too."""
+    cfg, img = _config_frame("1080p", seed)
+    fams = list(cfg.families)
+    ref, nq = O.ref_detect(img, fams, [2] * len(fams))
+    r = O.detect(img, [H.oracle_family(f) for f in fams], [2] * len(fams), O.default_params(), order=O.ORDER_REF)
+    assert len(r.quads) == nq and r.dets == ref and len(ref) > 10
+
+
+@needs_ref
+@pytest.mark.parametrize("dec", [2.0, 1.0])
+def test_oracle_equals_reference_4032x3024(dec):
+    """The large-frame stress workload (two families, 80 tags, 1000
+    distractors, an illumination ramp) at decimate 1 and 2."""
+    cfg, img = _config_frame("4032x3024", 7)
+    fams = list(cfg.families)
+    p = O.default_params(quad_decimate=dec)
+    ref, nq = O.ref_detect(img, fams, [2, 2], p)
+    r = O.detect(img, [H.oracle_family(f) for f in fams], [2, 2], p, order=O.ORDER_REF)
+    assert len(r.quads) == nq and r.dets == ref and len(ref) > 20
