@@ -100,7 +100,8 @@ class FrameResult(C.Structure):
     _fields_ = [("first", C.c_int64), ("count", C.c_int64), ("nquads", C.c_int64)]
 
 
-DIAG = {"quad_image": 0, "threshold": 1, "labels": 2, "points": 3, "clusters": 4, "quads": 5, "sizes": 6}
+DIAG = {"quad_image": 0, "threshold": 1, "labels": 2, "points": 3, "clusters": 4, "quads": 5, "sizes": 6,
+        "order_roots": 7}
 QUAD_DTYPE = np.dtype([("p", np.float32, (4, 2)), ("reversed_border", np.int32), ("frame", np.int32)])
 # at_detection as a numpy record (168 bytes)
 DETECTION_DTYPE = np.dtype([("family", np.int32), ("id", np.int32), ("hamming", np.int32),
@@ -304,7 +305,9 @@ class Detector:
     def diag(self, what: str) -> np.ndarray:
         """An intermediate array of the last detection (frame 0), for
         stage-by-stage checks: quad_image, threshold, labels, points,
-        clusters, quads or sizes."""
+        clusters, quads, sizes or order_roots (rows of (smallest node,
+        root) for the components beside quads whose ids repeat, in the
+        reference's packed node numbering)."""
         code = DIAG[what]
         sizes = np.zeros(6, np.int64)
         self._L.at_detector_diag(self._td, DIAG["sizes"], sizes.ctypes.data, 48)
@@ -323,6 +326,8 @@ class Detector:
             return buf.view(np.uint64)
         if what == "clusters":
             return buf.view(np.uint32)
+        if what == "order_roots":
+            return buf.view(np.uint32).reshape(-1, 2)
         return buf.view(QUAD_DTYPE)
 
     def family_name(self, d: Detection) -> str:

@@ -97,6 +97,8 @@ enum {
     B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_QNUM, B_FIRST, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
     B_HYMIN, B_HYMAX, B_CSPAN, B_CY0, B_SPANOFF, B_PKFRAME, B_PGKEYS, B_PGSLOTS, B_PFRAMES, B_PBSUM, B_SEG,
     B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
+    B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RLCNT, B_RNBAND, B_RLTOP, B_RLPX, B_RLBOT,
+    B_RLPX2,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -665,18 +667,45 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_RPRE].ensure((rows + n) * 4));
         CK(B[B_ROKEY].ensure(nd * 16));
         CK(B[B_RIDX2].ensure(nd * 4));
+        CK(B[B_RFIN].ensure(n * AT_REF_MAXT * 4));
+        CK(B[B_RFINB].ensure(n * AT_REF_MAXT * 4));
+        CK(B[B_RBSLOT].ensure(nodes * 2));
+        CK(B[B_RBINFO].ensure(nodes * 8));
+        CK(B[B_ROUTROOT].ensure(nodes * 4));
+        CK(B[B_RBM].ensure(rows * 4));
+        CK(B[B_RBSTART].ensure((rows + n) * 4));
+        CK(B[B_RLCNT].ensure((rows + n) * 4));
+        CK(B[B_RNBAND].ensure(n * 4));
+        CK(B[B_RLTOP].ensure(nodes * 4));
+        CK(B[B_RLPX].ensure(nodes * 4));
+        CK(B[B_RLBOT].ensure(nodes * 4));
+        CK(B[B_RLPX2].ensure(nodes * 4));
         CK(cudaMemsetAsync(B[B_RTROOT].p, 0xff, n * AT_REF_MAXT * 4, st));
-        const RefOrder ro{B[B_RNEED].as<uint32_t>(), B[B_RNT].as<uint32_t>(),  B[B_RTLAB].as<uint32_t>(),
-                          B[B_RTPX].as<uint32_t>(),  B[B_RTROOT].as<uint32_t>(), B[B_RTLIST].as<uint64_t>(),
-                          B[B_RTROW].as<uint32_t>(), B[B_RPRE].as<uint32_t>()};
+        CK(cudaMemsetAsync(B[B_RFINB].p, 0xff, n * AT_REF_MAXT * 4, st));
+        const RefOrder ro{B[B_RNEED].as<uint32_t>(),   B[B_RNT].as<uint32_t>(),     B[B_RTLAB].as<uint32_t>(),
+                          B[B_RTPX].as<uint32_t>(),    B[B_RTROOT].as<uint32_t>(),  B[B_RTLIST].as<uint64_t>(),
+                          B[B_RTROW].as<uint32_t>(),   B[B_RPRE].as<uint32_t>(),    B[B_RFIN].as<uint32_t>(),
+                          B[B_RFINB].as<uint32_t>(),   B[B_RBSTART].as<uint32_t>(), B[B_RLCNT].as<uint32_t>(),
+                          B[B_RNBAND].as<uint32_t>(),  B[B_RLTOP].as<uint32_t>(),   B[B_RLPX].as<uint32_t>(),
+                          B[B_RLBOT].as<uint32_t>(),   B[B_RLPX2].as<uint32_t>(),   B[B_RBSLOT].as<uint16_t>(),
+                          B[B_RBINFO].as<uint64_t>(),  B[B_ROUTROOT].as<uint32_t>(), B[B_RBM].as<uint32_t>()};
         int64_t capr = 1;
         for (auto &f : fd) capr = f.qw - 1 > capr ? f.qw - 1 : capr;
-        const size_t rbytes = ref_replay_bytes(capr);
+        const size_t rbytes = ref_replay_bytes(capr), fbytes = ref_frontier_bytes(capr);
+        if (nodes >= ((int64_t)1 << 31)) {  // the replay marks symbols with the top bit of a node id
+            set_error(in, 2, "batch too large for the order replay (node ids above 2^31)");
+            return false;
+        }
+        if (capr > REF_PCAP || fbytes > AT_REF_SMEM_MAX) {
+            set_error(in, 2, "quad image too wide for the order replay (" + std::to_string(capr + 1) + " px)");
+            return false;
+        }
         uint8_t *rscr = nullptr;
         if (rbytes > AT_REF_SMEM_MAX) {
-            CK(B[B_RSCR].ensure(rbytes * n));
+            CK(B[B_RSCR].ensure(rbytes * n * REF_BAND_BLOCKS));
             rscr = B[B_RSCR].as<uint8_t>();
-        } else if (rbytes > in->ref_smem) {
+        }
+        if (in->ref_smem == 0) {
             if (!ref_replay_set_smem(AT_REF_SMEM_MAX)) {
                 set_error(in, 1, "cudaFuncSetAttribute for the order replay failed");
                 return false;
@@ -686,7 +715,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         launch_ref_order(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), in->nfam, B[B_QSTART].as<int64_t>(),
                          B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>(), B[B_QCL].as<uint32_t>(), ckey, nb,
                          capr, rscr, rbytes, ro, B[B_ERR].as<uint32_t>());
-        in->launches += 3;
+        in->launches += 7;
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
                         B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(), B[B_OUTN].as<int64_t>(), dfr, ro,
@@ -1008,6 +1037,27 @@ int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap
     case AT_DIAG_SIZES:
         memcpy(dst, sizes, (size_t)(cap < 48 ? cap : 48));
         return 48;
+    case AT_DIAG_ORDER_ROOTS: {
+        // frame 0: the targets' GPU labels to packed numbers (node_off 0)
+        uint32_t nt = 0;
+        const int64_t qw = in->last_qw, qh = in->last_qh;
+        if (qw * qh == 0 || !B[B_RNT].p || !B[B_RPRE].p) return 0;
+        if (cudaMemcpy(&nt, B[B_RNT].p, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+        if (nt > AT_REF_MAXT) return -1;
+        std::vector<uint32_t> lab(nt), root(nt), pre(qh + 1), out(2 * nt);
+        if (nt > 0 && (cudaMemcpy(lab.data(), B[B_RTLAB].p, 4 * nt, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                       cudaMemcpy(root.data(), B[B_RTROOT].p, 4 * nt, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                       cudaMemcpy(pre.data(), B[B_RPRE].p, 4 * (qh + 1), cudaMemcpyDeviceToHost) != cudaSuccess))
+            return -1;
+        for (uint32_t t = 0; t < nt; t++) {
+            const int64_t nd = lab[t];
+            out[2 * t] = nd < qw * qh ? pre[nd / qw] + (uint32_t)(nd % qw) : pre[qh] + (uint32_t)(nd - qw * qh);
+            out[2 * t + 1] = root[t];
+        }
+        const int64_t nbytes = 8 * (int64_t)nt;
+        if (dst && cap > 0) memcpy(dst, out.data(), (size_t)(nbytes < cap ? nbytes : cap));
+        return nbytes;
+    }
     default: return -1;
     }
     int64_t n = bytes < cap ? bytes : cap;

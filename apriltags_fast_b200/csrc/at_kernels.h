@@ -118,21 +118,39 @@ void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm
 // target runs compacted by row (tlist); per row, their count (trow); per
 // row plus one per frame, the runs above the row (rpre).
 #define AT_REF_MAXT 192
+#define REF_BAND 16         // rows per band of the replay, at most
+#define REF_PCAP 4160       // target runs per band, at most (a row always fits: quad images up to 4161 px wide)
+#define REF_BAND_BLOCKS 32  // replay blocks per frame when the replay works in a global scratch
 struct RefOrder {
     uint32_t *need, *nt;
     uint32_t *tlabel, *tpx, *troot;
     uint64_t *tlist;
     uint32_t *trow;
     uint32_t *rpre;
+    uint32_t *fin, *finb;     // per target: its root (node or symbol) and the band where it was found
+    // bands (rows + one per frame each): first row of each band and the last
+    // band's end; the band's component counts; per frame: the band count
+    uint32_t *bstart, *lcnt, *nband;
+    // per node (at the rows of the band edges, at_order.cu):
+    uint32_t *ltop, *lpx;     //   top row: each run's band component, their pixels
+    uint32_t *lbot, *lpx2;    //   bottom row: each run's band component, the others' pixels
+    uint16_t *bslot;          //   row above a band: each target run's slot
+    uint64_t *binfo;          //   row above a band: each slot, pixels | first run << 32 | target << 48
+    uint32_t *outroot;        //   bottom row: each run's root after the band
+    uint32_t *bm;             // per row: slots at the row above a band
 };
-// Bytes of the replay's arrays for rows of at most capr runs (shared
-// memory, or a global scratch region per frame when scratch is not null).
+// Shared-memory bytes of the band replay (rows of at most capr runs), of the
+// band components and of the frontier pass; above AT_REF_SMEM_MAX the band
+// replay takes a global scratch of that size per block (REF_BAND_BLOCKS
+// blocks per frame).
 size_t ref_replay_bytes(int64_t capr);
+size_t ref_local_bytes();
+size_t ref_frontier_bytes(int64_t capr);
 bool ref_replay_set_smem(size_t bytes);
 void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                       const uint32_t *row_nruns, int nfam, const int64_t *qstart, const GpuDetection *dets,
                       const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb, int64_t capr,
-                      uint8_t *scratch, size_t scratch_per_frame, const RefOrder &ref, uint32_t *err);
+                      uint8_t *scratch, size_t scratch_per_block, const RefOrder &ref, uint32_t *err);
 // okey: 2 u64 + 1 u32 per detection slot (the order keys, a second index)
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,

@@ -18,14 +18,21 @@
 // kernels find that root for the few components that matter and give the
 // final stage the reference's order keys:
 //
-//   k_ref_targets  per frame: the ids that two or more detections share;
-//                  the components of their quads are the targets (their GPU
-//                  labels and pixel counts); the packed run numbering.
-//   k_ref_mark     the runs of the target components, row by row, compacted
-//                  (start, end, index in row, value, target).
-//   k_ref_replay   a warp per frame sweeps the rows and replays the
-//                  reference's unions of the target runs (see below).
-//   k_finalize     (at_kernels.cu) orders those detections by the keys.
+//   k_ref_targets   per frame: the ids that two or more detections share;
+//                   the components of their quads are the targets (their
+//                   GPU labels and pixel counts); the packed run numbering.
+//   k_ref_mark      the runs of the target components, row by row, compacted
+//                   (start, end, index in row, value, target).
+//   k_ref_cut       the rows of each frame in bands.
+//   k_ref_local     the band's own components of target runs (all bands at
+//                   once), summarised by those reaching its top and bottom.
+//   k_ref_frontier  per frame, band after band: the sets of target runs at
+//                   each band's upper edge as the reference has them there.
+//   k_ref_band      a warp per band replays the reference's unions of the
+//                   band's target runs (see below), the incoming sets'
+//                   roots as symbols.
+//   k_ref_resolve   per frame: the symbols resolved from the top down.
+//   k_finalize      (at_kernels.cu) orders those detections by the keys.
 //
 // The replay. Before row y, each set of target runs that touches row y-1
 // is a "slot" with its root and pixel count. The reference's calls of row
@@ -205,9 +212,9 @@ __global__ void __launch_bounds__(256) k_ref_mark(const FrameDesc *frames, const
 }
 
 // ---------------------------------------------------------------------------
-// The replay, a warp per frame. Its arrays live in shared memory, or for
-// very wide frames in a global scratch of the same layout (one region per
-// frame); `capr` bounds the runs of a row.
+// The replay of a band of rows, a warp each. Its arrays live in shared
+// memory, or for very wide frames in a global scratch of the same layout
+// (one region per block); `capr` bounds the runs of a row.
 
 struct ReplayArrays {
     uint32_t *p_se;   // previous row's open target runs: start | end << 16
@@ -303,264 +310,754 @@ __device__ __forceinline__ uint32_t fold_find(const uint16_t *par, uint32_t x) {
     return x;
 }
 
-__global__ void __launch_bounds__(32) k_ref_replay(const FrameDesc *frames, RefOrder ref, int64_t capr,
-                                                   uint8_t *scratch, size_t scratch_per_frame, uint32_t *err) {
+// Roots in the band replay: a node id, or REF_SYM | j, "the root of the
+// band's incoming slot j" (known only once the bands above are resolved).
+#define REF_SYM 0x80000000u
+
+// One row of the reference's unions over the open target runs, for a warp:
+// the row's runs (c_*, n) against the previous row's (p_*, np, with their
+// slots s_*, m); afterwards the slots and previous runs describe this row.
+// Slots that no call reaches are whole components: fin[t] gets their root.
+// Returns false when the call arrays are too small (err set).
+struct RowState {
+    int64_t m, np;
+};
+
+__device__ bool replay_row(ReplayArrays &A, RowState &S, int64_t n, bool link, uint32_t rbase, uint32_t vnode,
+                           int64_t capr, uint32_t *fin, uint32_t *finb, uint32_t band, uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int64_t m = S.m, np = S.np;
+    const int64_t E = m + n + 1, vn = m + n;
+    __syncwarp();
+    for (int64_t e = lane; e < E; e += 32) {
+        A.e_par[e] = (uint16_t)e;
+        A.e_fpar[e] = (uint16_t)e;
+        A.e_max[e] = 0;
+        A.e_c0[e] = 0xffffffffu;
+        A.e_c1[e] = 0;
+        if (e < m) {
+            A.e_R[e] = A.s_R[e];
+            A.e_Z[e] = A.s_Z[e];
+            A.e_flag[e] = 0;
+        } else if (e < vn) {
+            const uint32_t se = A.c_se[e - m];
+            A.e_R[e] = rbase + A.c_j[e - m];
+            A.e_Z[e] = (se >> 16) - (se & 0xffffu) + 1;
+            A.e_flag[e] = REF_TOUCHED;
+        } else {
+            A.e_R[e] = vnode;
+            A.e_Z[e] = 1;
+            A.e_flag[e] = link ? REF_TOUCHED : 0;
+        }
+    }
+    // the calls, in the reference's order: each run, its touching runs
+    // above in order (fast/unionfind.c:112-196), then the last column
+    int64_t nc = 0;
+    if (np > 0) {
+        for (int64_t i0 = 0; i0 < n; i0 += 32) {
+            const int64_t i = i0 + lane;
+            int64_t k0 = 0, cnt = 0;
+            int64_t a0 = 0, a1 = 0;
+            uint8_t v = 0;
+            if (i < n) {
+                a0 = A.c_se[i] & 0xffffu;
+                a1 = A.c_se[i] >> 16;
+                v = A.c_v[i];
+                int64_t lo = 0, hi = np;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if ((int64_t)(A.p_se[mid] >> 16) + 1 < a0)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                k0 = lo;
+                for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
+                    if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) cnt++;
+            }
+            uint32_t total;
+            const uint32_t off = warp_excl_scan((uint32_t)cnt, &total);
+            if (nc + total + 1 > 2 * capr + 2) {  // more calls than the arrays hold
+                if (lane == 0) atomicOr(err, AT_ERR_ORDER);
+                return false;
+            }
+            int64_t o = nc + off;
+            if (i < n)
+                for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
+                    if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) {
+                        A.call_a[o] = (uint16_t)(m + i);
+                        A.call_b[o] = A.p_slot[k];
+                        o++;
+                    }
+            nc += total;
+        }
+    }
+    if (link) {
+        if (lane == 0) {
+            A.call_a[nc] = (uint16_t)(vn - 1);
+            A.call_b[nc] = (uint16_t)vn;
+        }
+        nc++;
+    }
+    __syncwarp();
+    // groups
+    for (int64_t c = lane; c < nc; c += 32) {
+        el_unite(A.e_par, A.call_a[c], A.call_b[c]);
+        A.e_flag[A.call_b[c]] = REF_TOUCHED;
+    }
+    __syncwarp();
+    // every element's group root (read-only walks into e_tot, then copied:
+    // a halving write racing a final write could leave a non-root parent)
+    for (int64_t e = lane; e < E; e += 32) {
+        uint32_t x = (uint32_t)e;
+        while (A.e_par[x] != x) x = A.e_par[x];
+        A.e_tot[e] = x;
+    }
+    __syncwarp();
+    for (int64_t e = lane; e < E; e += 32) {
+        A.e_par[e] = (uint16_t)A.e_tot[e];
+        A.e_tot[e] = 0;
+    }
+    __syncwarp();
+    // per group: pixels, the largest set that existed before the row, and
+    // the range of its calls
+    for (int64_t e = lane; e < E; e += 32) {
+        if (!A.e_flag[e]) continue;
+        const uint32_t g = A.e_par[e];
+        atomicAdd(&A.e_tot[g], A.e_Z[e]);
+        if (e < m || e == vn) atomicMax(&A.e_max[g], (unsigned long long)A.e_Z[e] << 16 | (uint64_t)e);
+    }
+    for (int64_t c = lane; c < nc; c += 32) {
+        const uint32_t g = A.e_par[A.call_a[c]];
+        atomicMin(&A.e_c0[g], (uint32_t)c);
+        atomicMax(&A.e_c1[g], (uint32_t)c);
+    }
+    __syncwarp();
+    // each group's root and pixels, into its root element
+    for (int64_t g = lane; g < E; g += 32) {
+        if (!A.e_flag[g] || A.e_par[g] != g) continue;
+        const unsigned long long mx = A.e_max[g];
+        const uint32_t zmax = (uint32_t)(mx >> 16), tot = A.e_tot[g];
+        if (mx != 0 && zmax > tot - zmax) {
+            A.e_R[g] = A.e_R[mx & 0xffffu];
+            A.e_Z[g] = tot;
+            continue;
+        }
+        // no set outweighs the rest: the reference's calls one by one
+        for (uint32_t c = A.e_c0[g]; c <= A.e_c1[g] && c < (uint32_t)nc; c++) {
+            const uint32_t a = A.call_a[c];
+            if (A.e_par[a] != g) continue;
+            const uint32_t ra = fold_find(A.e_fpar, a), rb = fold_find(A.e_fpar, A.call_b[c]);
+            if (ra == rb) continue;
+            const uint32_t za = A.e_Z[ra], zb = A.e_Z[rb];
+            if (za > zb) {
+                A.e_fpar[rb] = (uint16_t)ra;
+                A.e_Z[ra] = za + zb;
+            } else {
+                A.e_fpar[ra] = (uint16_t)rb;
+                A.e_Z[rb] = za + zb;
+            }
+        }
+        const uint32_t r = fold_find(A.e_fpar, (uint32_t)g);
+        const uint32_t R = A.e_R[r], Z = A.e_Z[r];
+        A.e_R[g] = R;
+        A.e_Z[g] = Z;
+    }
+    __syncwarp();
+    // a slot no call reached is a whole component: its root is final
+    for (int64_t e = lane; e < m; e += 32) {
+        const uint32_t t = A.s_t[e];
+        if (A.e_flag[e] || t == REF_NONE) continue;
+        fin[t] = A.s_R[e];
+        finb[t] = band;
+    }
+    // the new slots: one per group of this row's runs, numbered by its
+    // first run (e_tot of the root is free again and holds that run)
+    for (int64_t i = lane; i < n; i += 32) A.e_tot[A.e_par[m + i]] = 0xffffffffu;
+    __syncwarp();
+    for (int64_t i = lane; i < n; i += 32) atomicMin(&A.e_tot[A.e_par[m + i]], (uint32_t)i);
+    __syncwarp();
+    int64_t mnew = 0;
+    for (int64_t i0 = 0; i0 < n; i0 += 32) {
+        const int64_t i = i0 + lane;
+        uint32_t g = 0;
+        bool first = false;
+        if (i < n) {
+            g = A.e_par[m + i];
+            first = A.e_tot[g] == (uint32_t)i;
+        }
+        const uint32_t bal = __ballot_sync(0xffffffffu, first);
+        if (first) {
+            const int64_t k = mnew + __popc(bal & lt);
+            A.e_c0[g] = (uint32_t)k;  // the group's new slot
+            A.s_R[k] = A.e_R[g];
+            A.s_Z[k] = A.e_Z[g];
+            A.s_t[k] = A.c_t[i];
+        }
+        mnew += __popc(bal);
+    }
+    __syncwarp();
+    // this row's runs, with their slots, for the next row
+    for (int64_t i = lane; i < n; i += 32) {
+        A.p_se[i] = A.c_se[i];
+        A.p_v[i] = A.c_v[i];
+        A.p_slot[i] = (uint16_t)A.e_c0[A.e_par[m + i]];
+    }
+    S.m = mnew;
+    S.np = n;
+    __syncwarp();
+    return true;
+}
+
+// Loads the target runs of row y (rbase: its first node) into c_*;
+// returns their count and whether the row's last-column link joins one.
+__device__ int64_t load_row(ReplayArrays &A, const RefOrder &ref, const FrameDesc &fd, int64_t y, bool *link) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t tr = ref.trow[fd.row0 + y];
+    const int64_t n = tr & 0x7fffffffu;
+    const uint32_t rbase = (uint32_t)(fd.node_off + y * fd.qw);
+    for (int64_t j = lane; j < n; j += 32) {
+        const uint64_t e = ref.tlist[rbase + j];
+        A.c_se[j] = (uint32_t)e;
+        A.c_v[j] = (uint8_t)(e >> 48);
+        A.c_j[j] = (uint16_t)(e >> 32);
+        A.c_t[j] = (uint8_t)(e >> 56);
+    }
+    *link = (tr >> 31) != 0;
+    return n;
+}
+
+
+// ---------------------------------------------------------------------------
+// Bands. The rows of a frame go in bands (at most REF_BAND rows and
+// REF_PCAP target runs each), replayed in parallel. A band's replay needs
+// the sets of target runs that touch the row above it as the reference has
+// them there, with their pixel counts. Which runs are together and how many
+// pixels a set holds do not depend on which root wins, so these come from
+// an order-free union-find in two steps: k_ref_local joins the runs inside
+// each band (all bands at once) and summarises the band by its components
+// that reach its top and bottom rows; k_ref_frontier then walks the bands
+// of a frame from the top joining only those summaries. A band's replay
+// carries the incoming sets' roots as symbols, and k_ref_resolve puts the
+// roots in from the top down.
+//
+// Band b covers rows bstart[b] .. bstart[b + 1] - 1. Node-indexed arrays,
+// at the nodes of a row y (node_off + y qw + i):
+//   ltop[j]    top row of a band: the band component of target run j,
+//              numbered by first run among the components that reach it
+//   lpx[c]     top row: pixels of band component c
+//   lbot[j]    bottom row: run j's component, c (one reaching the top row)
+//              or 0x80000000 | k (the k-th of the others)
+//   lpx2[k]    bottom row: pixels of the k-th other component
+//   bslot[j]   row above a band: the slot (prefix set) of target run j
+//   binfo[s]   row above a band: slot s, pixels | first run << 32 |
+//              target << 48
+//   outroot[j] the bottom row of a band: the root of run j's set after it
+// and per row: bm[y] the slots at the row above a band; per band:
+// lcnt[b] = components reaching the top | the others reaching the bottom << 16.
+
+#define REF_KNONE 0x3fffffffu  // no run yet: above every run index, below the flags
+#define REF_KTOP 0x80000000u   // numbered: the component's index
+#define REF_KBOT 0x40000000u
+
+// Adds `val` to arr[key] for the active lanes, one atomic per distinct key
+// in the warp. Every lane of the warp calls it.
+__device__ __forceinline__ void warp_add_by_key(uint32_t *arr, uint32_t key, uint32_t val, bool active) {
+    const uint32_t am = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const uint32_t peers = __match_any_sync(am, key);
+    const uint32_t sum = __reduce_add_sync(peers, val);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
+}
+
+__device__ __forceinline__ uint32_t pu_find(volatile uint32_t *par, uint32_t x) {
+    uint32_t p = par[x];
+    while (p != x) {
+        const uint32_t pp = par[p];
+        if (pp != p) par[x] = pp;
+        x = p;
+        p = par[x];
+    }
+    return x;
+}
+
+// Lock-free hooking of the larger root under the smaller (connectivity only).
+__device__ __forceinline__ void pu_unite(uint32_t *par, uint32_t a, uint32_t b) {
+    volatile uint32_t *vp = par;
+    for (;;) {
+        a = pu_find(vp, a);
+        b = pu_find(vp, b);
+        if (a == b) return;
+        if (a < b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(par + a, a, b) == a) return;
+    }
+}
+
+// The first index in runs [lo, hi) (start | end << 16, sorted) whose end
+// reaches column a0 - 1.
+__device__ __forceinline__ uint32_t first_reaching(const uint32_t *se, uint32_t lo, uint32_t hi, int64_t a0) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((int64_t)(se[mid] >> 16) + 1 < a0)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The band cut of each frame, a warp per frame: bands of up to REF_BAND
+// rows whose target runs stay within REF_PCAP.
+__global__ void __launch_bounds__(32) k_ref_cut(const FrameDesc *frames, RefOrder ref) {
+    const int f = blockIdx.x;
+    if (!ref.need[f]) return;
+    const FrameDesc fd = frames[f];
+    const int lane = threadIdx.x;
+    uint32_t *bs = ref.bstart + fd.row0 + f;
+    uint32_t nb = 0, acc = 0;
+    int rows = 0;
+    for (int64_t y0 = 0; y0 < fd.qh; y0 += 32) {
+        const int64_t y = y0 + lane;
+        const uint32_t c = y < fd.qh ? (ref.trow[fd.row0 + y] & 0x7fffffffu) : 0u;
+        const int kn = fd.qh - y0 < 32 ? (int)(fd.qh - y0) : 32;
+        for (int k = 0; k < kn; k++) {
+            const uint32_t ck = __shfl_sync(0xffffffffu, c, k);
+            if (rows == 0 || rows == REF_BAND || acc + ck > REF_PCAP) {
+                if (lane == 0) bs[nb] = (uint32_t)(y0 + k);
+                nb++;
+                acc = 0;
+                rows = 0;
+            }
+            acc += ck;
+            rows++;
+        }
+    }
+    if (lane == 0) {
+        bs[nb] = (uint32_t)fd.qh;
+        ref.nband[f] = nb;
+    }
+}
+
+// The shared-memory layout of k_ref_local: REF_PCAP runs and a last-column
+// node per row.
+struct LocalArrays {
+    uint32_t *se, *par, *Z, *tot, *key;
+    uint8_t *v;
+};
+__host__ __device__ inline size_t ref_local_carve(uint8_t *base, LocalArrays *A) {
+    const int64_t cape = REF_PCAP + REF_BAND;
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        uint8_t *p = base + at;
+        at = ref_align(at + bytes);
+        return p;
+    };
+    LocalArrays a;
+    a.se = (uint32_t *)take(4 * REF_PCAP);
+    a.par = (uint32_t *)take(4 * cape);
+    a.Z = (uint32_t *)take(4 * cape);
+    a.tot = (uint32_t *)take(4 * cape);
+    a.key = (uint32_t *)take(4 * cape);
+    a.v = take(REF_PCAP);
+    if (A) *A = a;
+    return at;
+}
+size_t ref_local_bytes() { return ref_local_carve(nullptr, nullptr); }
+
+// A block per band (the frame's bands taken in turn by its blocks): the
+// band's components, their pixels, and the summaries named above.
+__global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefOrder ref, uint32_t *err) {
     extern __shared__ __align__(16) uint8_t s_mem[];
-    __shared__ uint8_t s_done[AT_REF_MAXT];
-    __shared__ uint32_t s_ndone;
+    __shared__ uint32_t s_roff[REF_BAND + 1];
+    __shared__ uint8_t s_link[REF_BAND];
+    __shared__ uint32_t s_ntop, s_nnon;
+    const int f = blockIdx.y;
+    if (!ref.need[f]) return;
+    const FrameDesc fd = frames[f];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    LocalArrays A;
+    ref_local_carve(s_mem, &A);
+    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const int64_t nb = ref.nband[f];
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const int64_t y0 = bs[b], y1 = bs[b + 1];
+        const int nr = (int)(y1 - y0);
+        if (tid < 32) {
+            uint32_t c = 0, lk = 0;
+            if (tid < nr) {
+                const uint32_t tr = ref.trow[fd.row0 + y0 + tid];
+                c = tr & 0x7fffffffu;
+                lk = tr >> 31;
+            }
+            uint32_t total;
+            const uint32_t off = warp_excl_scan(c, &total);
+            if (tid < nr) {
+                s_roff[tid] = off;
+                s_link[tid] = (uint8_t)lk;
+            }
+            if (tid == 0) s_roff[nr] = total;
+        }
+        __syncthreads();
+        const uint32_t L = s_roff[nr];
+        if (L > REF_PCAP) {  // the cut keeps bands within REF_PCAP when a row fits
+            if (tid == 0) atomicOr(err, AT_ERR_ORDER);
+            return;
+        }
+        const int64_t E = L + nr;
+        // elements: the band's runs [0, L), then the last-column node of
+        // each row's link [L, L + nr)
+        for (uint32_t l = tid; l < L; l += nt) {
+            int r = 0;
+            while (s_roff[r + 1] <= l) r++;
+            const uint64_t e = ref.tlist[fd.node_off + (y0 + r) * fd.qw + (l - s_roff[r])];
+            A.se[l] = (uint32_t)e;
+            A.v[l] = (uint8_t)(e >> 48);
+            A.par[l] = l;
+            A.Z[l] = (((uint32_t)e >> 16) & 0xffffu) - ((uint32_t)e & 0xffffu) + 1;
+            A.tot[l] = 0;
+            A.key[l] = REF_KNONE;
+        }
+        for (int r = tid; r < nr; r += nt) {
+            A.par[L + r] = L + r;
+            A.Z[L + r] = s_link[r] ? 1u : 0u;
+            A.tot[L + r] = 0;
+            A.key[L + r] = REF_KNONE;
+        }
+        __syncthreads();
+        for (uint32_t l = tid; l < L; l += nt) {
+            int r = 0;
+            while (s_roff[r + 1] <= l) r++;
+            if (r == 0) continue;
+            const int64_t a0 = A.se[l] & 0xffffu, a1 = A.se[l] >> 16;
+            const uint8_t v = A.v[l];
+            const uint32_t hi = s_roff[r];
+            for (uint32_t k = first_reaching(A.se, s_roff[r - 1], hi, a0); k < hi && (int64_t)(A.se[k] & 0xffffu) <= a1 + 1;
+                 k++)
+                if (A.v[k] == v && runs_touch(a0, a1, A.se[k] & 0xffffu, A.se[k] >> 16, v)) pu_unite(A.par, l, k);
+        }
+        for (int r = tid; r < nr; r += nt)
+            if (s_link[r] && s_roff[r + 1] > s_roff[r]) pu_unite(A.par, s_roff[r + 1] - 1, L + r);
+        __syncthreads();
+        // each element's component (into Z, once its pixels are read)
+        for (int64_t e0 = 0; e0 < E; e0 += nt) {
+            const int64_t e = e0 + tid;
+            const bool act = e < E;
+            uint32_t x = 0, z = 0;
+            if (act) {
+                x = (uint32_t)e;
+                while (A.par[x] != x) x = A.par[x];
+                z = A.Z[e];
+                A.Z[e] = x;  // only this thread reads or writes Z[e] here
+            }
+            warp_add_by_key(A.tot, x, z, act);
+        }
+        __syncthreads();
+        // the components that reach the top row, numbered by first run
+        const uint32_t n0 = s_roff[1];
+        const int64_t rt = fd.node_off + y0 * fd.qw, rb = fd.node_off + (y1 - 1) * fd.qw;
+        for (uint32_t l = tid; l < n0; l += nt) atomicMin(&A.key[A.Z[l]], l);
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t k0 = 0;
+            for (uint32_t i0 = 0; i0 < n0; i0 += 32) {
+                const uint32_t i = i0 + tid;
+                uint32_t g = 0;
+                bool first = false;
+                if (i < n0) {
+                    g = A.Z[i];
+                    first = A.key[g] == i;
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, first);
+                if (first) {
+                    const uint32_t c = k0 + __popc(bal & lt);
+                    A.key[g] = REF_KTOP | c;
+                    ref.lpx[rt + c] = A.tot[g];
+                }
+                k0 += __popc(bal);
+            }
+            if (tid == 0) s_ntop = k0;
+        }
+        __syncthreads();
+        for (uint32_t l = tid; l < n0; l += nt) ref.ltop[rt + l] = A.key[A.Z[l]] & 0xffffu;
+        // the bottom row's other components, numbered by first run
+        const uint32_t lb = s_roff[nr - 1], nbot = L - lb;
+        for (uint32_t i = tid; i < nbot; i += nt) {
+            const uint32_t g = A.Z[lb + i];
+            if (A.key[g] < REF_KTOP) atomicMin(&A.key[g], i);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t k0 = 0;
+            for (uint32_t i0 = 0; i0 < nbot; i0 += 32) {
+                const uint32_t i = i0 + tid;
+                uint32_t g = 0;
+                bool first = false;
+                if (i < nbot) {
+                    g = A.Z[lb + i];
+                    first = A.key[g] == i;
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, first);
+                if (first) {
+                    const uint32_t k = k0 + __popc(bal & lt);
+                    A.key[g] = REF_KBOT | k;
+                    ref.lpx2[rb + k] = A.tot[g];
+                }
+                k0 += __popc(bal);
+            }
+            if (tid == 0) s_nnon = k0;
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < nbot; i += nt) {
+            const uint32_t kg = A.key[A.Z[lb + i]];
+            ref.lbot[rb + i] = (kg & REF_KTOP) ? (kg & 0xffffu) : (0x80000000u | (kg & 0xffffu));
+        }
+        if (tid == 0) ref.lcnt[fd.row0 + f + b] = s_ntop | s_nnon << 16;
+        __syncthreads();
+    }
+}
+
+// The shared-memory layout of k_ref_frontier (rows of at most capr runs).
+struct FrontArrays {
+    uint32_t *f_se, *s_Z, *par, *Z, *tot, *key, *bk;
+    uint16_t *f_slot;
+    uint8_t *f_v;
+};
+__host__ __device__ inline size_t ref_front_carve(uint8_t *base, int64_t capr, FrontArrays *A) {
+    const int64_t cape = 2 * capr + 2;
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        uint8_t *p = base + at;
+        at = ref_align(at + bytes);
+        return p;
+    };
+    FrontArrays a;
+    a.f_se = (uint32_t *)take(4 * capr);
+    a.s_Z = (uint32_t *)take(4 * (capr + 1));
+    a.par = (uint32_t *)take(4 * cape);
+    a.Z = (uint32_t *)take(4 * cape);
+    a.tot = (uint32_t *)take(4 * cape);
+    a.key = (uint32_t *)take(4 * (cape + capr + 1));
+    a.bk = (uint32_t *)take(4 * capr);
+    a.f_slot = (uint16_t *)take(2 * capr);
+    a.f_v = take(capr);
+    if (A) *A = a;
+    return at;
+}
+size_t ref_frontier_bytes(int64_t capr) { return ref_front_carve(nullptr, capr, nullptr); }
+
+// A block per frame, band after band: the prefix sets at the bottom row of
+// each band (slots), from the slots above and the band's summaries.
+__global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, RefOrder ref, int64_t capr) {
+    extern __shared__ __align__(16) uint8_t s_mem[];
+    __shared__ uint32_t s_m;
+    const int f = blockIdx.x;
+    if (!ref.need[f]) return;
+    const FrameDesc fd = frames[f];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    FrontArrays A;
+    ref_front_carve(s_mem, capr, &A);
+    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const int64_t nb = ref.nband[f];
+    int64_t m = 0, nf = 0;  // the slots and runs of the row above the band
+    for (int64_t b = 0; b < nb; b++) {
+        const int64_t y0 = bs[b], y1 = bs[b + 1];
+        const uint32_t lc = ref.lcnt[fd.row0 + f + b];
+        const int64_t ntop = lc & 0xffffu, nnon = lc >> 16;
+        const int64_t rt = fd.node_off + y0 * fd.qw, rb = fd.node_off + (y1 - 1) * fd.qw;
+        const int64_t n0 = ref.trow[fd.row0 + y0] & 0x7fffffffu, nbot = ref.trow[fd.row0 + y1 - 1] & 0x7fffffffu;
+        const bool boundary = y1 < fd.qh;
+        // elements: the slots [0, m), the band's components that reach its
+        // top row [m, m + ntop); keys of the bottom row's sets: those
+        // elements, then the band's other components [E, E + nnon)
+        const int64_t E = m + ntop;
+        for (int64_t e = tid; e < E; e += nt) {
+            A.par[e] = (uint32_t)e;
+            A.tot[e] = 0;
+            A.Z[e] = e < m ? A.s_Z[e] : ref.lpx[rt + (e - m)];
+        }
+        for (int64_t e = tid; e < E + nnon; e += nt) A.key[e] = REF_KNONE;
+        __syncthreads();
+        if (nf > 0)
+            for (int64_t j = tid; j < n0; j += nt) {
+                const uint32_t se = (uint32_t)ref.tlist[rt + j];
+                const uint8_t v = (uint8_t)(ref.tlist[rt + j] >> 48);
+                const int64_t a0 = se & 0xffffu, a1 = se >> 16;
+                const uint32_t c = ref.ltop[rt + j];
+                for (uint32_t k = first_reaching(A.f_se, 0, (uint32_t)nf, a0);
+                     k < nf && (int64_t)(A.f_se[k] & 0xffffu) <= a1 + 1; k++)
+                    if (A.f_v[k] == v && runs_touch(a0, a1, A.f_se[k] & 0xffffu, A.f_se[k] >> 16, v))
+                        pu_unite(A.par, A.f_slot[k], (uint32_t)(m + c));
+            }
+        __syncthreads();
+        for (int64_t e0 = 0; e0 < E; e0 += nt) {
+            const int64_t e = e0 + tid;
+            const bool act = e < E;
+            uint32_t x = 0, z = 0;
+            if (act) {
+                x = (uint32_t)e;
+                while (A.par[x] != x) x = A.par[x];
+                z = A.Z[e];
+                A.Z[e] = x;  // only this thread reads or writes Z[e] here
+            }
+            warp_add_by_key(A.tot, x, z, act);
+        }
+        __syncthreads();
+        // the bottom row's sets, numbered by first run: the new slots
+        for (int64_t j = tid; j < nbot; j += nt) {
+            const uint32_t lb = ref.lbot[rb + j];
+            const uint32_t g = (lb & 0x80000000u) ? (uint32_t)E + (lb & 0xffffu) : A.Z[m + lb];
+            A.bk[j] = g;
+            atomicMin(&A.key[g], (uint32_t)j);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t k0 = 0;
+            for (int64_t i0 = 0; i0 < nbot; i0 += 32) {
+                const int64_t i = i0 + tid;
+                uint32_t g = 0;
+                bool first = false;
+                if (i < nbot) {
+                    g = A.bk[i];
+                    first = A.key[g] == (uint32_t)i;
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, first);
+                if (first) {
+                    const uint32_t k = k0 + __popc(bal & lt);
+                    const uint32_t px = g < (uint32_t)E ? A.tot[g] : ref.lpx2[rb + (g - E)];
+                    A.s_Z[k] = px;
+                    A.key[g] = REF_KTOP | k;
+                    if (boundary)
+                        ref.binfo[rb + k] =
+                            (uint64_t)px | (uint64_t)i << 32 | (uint64_t)(uint8_t)(ref.tlist[rb + i] >> 56) << 48;
+                }
+                k0 += __popc(bal);
+            }
+            if (tid == 0) {
+                s_m = k0;
+                if (boundary) ref.bm[fd.row0 + y1 - 1] = k0;
+            }
+        }
+        __syncthreads();
+        for (int64_t j = tid; j < nbot; j += nt) {
+            const uint32_t slot = A.key[A.bk[j]] & 0xffffu;
+            const uint64_t te = ref.tlist[rb + j];
+            A.f_se[j] = (uint32_t)te;
+            A.f_v[j] = (uint8_t)(te >> 48);
+            A.f_slot[j] = (uint16_t)slot;
+            if (boundary) ref.bslot[rb + j] = (uint16_t)slot;
+        }
+        m = s_m;
+        nf = nbot;
+        __syncthreads();
+    }
+}
+
+// The replay of one band, a warp each (the frame's bands taken in turn by
+// its blocks), the incoming sets' roots as symbols.
+__global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrder ref, int64_t capr,
+                                                 uint8_t *scratch, size_t scratch_per_block, uint32_t *err) {
+    extern __shared__ __align__(16) uint8_t s_mem[];
+    const int f = blockIdx.y;
+    if (!ref.need[f]) return;
+    const int lane = threadIdx.x;
+    const FrameDesc fd = frames[f];
+    ReplayArrays A;
+    ref_carve(scratch ? scratch + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * scratch_per_block : s_mem, capr, &A);
+    uint32_t *fin = ref.fin + (int64_t)f * AT_REF_MAXT, *finb = ref.finb + (int64_t)f * AT_REF_MAXT;
+    const uint32_t vbase = (uint32_t)(fd.node_off + (int64_t)fd.qw * fd.qh);
+    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const int64_t nb = ref.nband[f];
+    for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const int64_t y0 = bs[b], y1 = bs[b + 1];
+        RowState S{0, 0};
+        if (b > 0) {
+            // the incoming sets: the row above with its slots, roots as symbols
+            const int64_t ya = y0 - 1;
+            const int64_t ra = fd.node_off + ya * fd.qw;
+            const int64_t na = ref.trow[fd.row0 + ya] & 0x7fffffffu;
+            const int64_t ma = ref.bm[fd.row0 + ya];
+            for (int64_t j = lane; j < na; j += 32) {
+                const uint64_t e = ref.tlist[ra + j];
+                A.p_se[j] = (uint32_t)e;
+                A.p_v[j] = (uint8_t)(e >> 48);
+                A.p_slot[j] = ref.bslot[ra + j];
+            }
+            for (int64_t k = lane; k < ma; k += 32) {
+                const uint64_t bi = ref.binfo[ra + k];
+                A.s_R[k] = REF_SYM | (uint32_t)k;
+                A.s_Z[k] = (uint32_t)bi;
+                A.s_t[k] = (uint8_t)(bi >> 48);
+            }
+            S.m = ma;
+            S.np = na;
+        }
+        __syncwarp();
+        for (int64_t y = y0; y < y1; y++) {
+            bool link = false;
+            const int64_t n = load_row(A, ref, fd, y, &link);
+            if (n == 0 && S.np == 0) continue;
+            if (!replay_row(A, S, n, link && n > 0, (uint32_t)(fd.node_off + y * fd.qw), vbase + (uint32_t)(y - 1), capr,
+                            fin, finb, (uint32_t)b, err))
+                return;
+        }
+        // the roots of the sets of the band's last row, for the band below;
+        // after the last band every open set is a whole component
+        if (y1 < fd.qh) {
+            const int64_t rb = fd.node_off + (y1 - 1) * fd.qw;
+            for (int64_t j = lane; j < S.np; j += 32) ref.outroot[rb + j] = A.s_R[A.p_slot[j]];
+        } else {
+            for (int64_t k = lane; k < S.m; k += 32) {
+                const uint32_t t = A.s_t[k];
+                if (t == REF_NONE) continue;
+                fin[t] = A.s_R[k];
+                finb[t] = (uint32_t)b;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// A warp per frame: the symbols replaced band by band from the top, each
+// target's root, then the reference's packed node numbers.
+__global__ void __launch_bounds__(32) k_ref_resolve(const FrameDesc *frames, RefOrder ref, int64_t capr) {
+    extern __shared__ __align__(16) uint32_t s_res[];  // two arrays of capr + 1
     const int f = blockIdx.x;
     if (!ref.need[f]) return;
     const int lane = threadIdx.x;
-    const uint32_t lt = (1u << lane) - 1u;
     const FrameDesc fd = frames[f];
-    ReplayArrays A;
-    ref_carve(scratch ? scratch + (size_t)f * scratch_per_frame : s_mem, capr, &A);
     const uint32_t nt = ref.nt[f];
-    const uint32_t *tpx = ref.tpx + (int64_t)f * AT_REF_MAXT;
+    const uint32_t *fin = ref.fin + (int64_t)f * AT_REF_MAXT, *finb = ref.finb + (int64_t)f * AT_REF_MAXT;
     uint32_t *troot = ref.troot + (int64_t)f * AT_REF_MAXT;
-    for (uint32_t t = lane; t < AT_REF_MAXT; t += 32) s_done[t] = t < nt ? 0 : 1;
-    if (lane == 0) s_ndone = 0;
-    __syncwarp();
-    const uint32_t vbase = (uint32_t)(fd.node_off + (int64_t)fd.qw * fd.qh);
-    int64_t m = 0, np = 0;  // slots carried, open target runs of the previous row
-    for (int64_t y = 0; y < fd.qh && s_ndone < nt; y++) {
-        const uint32_t tr = ref.trow[fd.row0 + y];
-        const int64_t nraw = tr & 0x7fffffffu;
-        if (nraw == 0 && np == 0) continue;  // nothing open above, nothing here: m is 0 too
-        const uint32_t rbase = (uint32_t)(fd.node_off + y * fd.qw);
-        // this row's target runs whose component is still open
-        int64_t n = 0;
-        bool last_kept = false;
-        for (int64_t j0 = 0; j0 < nraw; j0 += 32) {
-            const int64_t j = j0 + lane;
-            uint64_t e = 0;
-            bool keep = false;
-            if (j < nraw) {
-                e = ref.tlist[rbase + j];
-                keep = !s_done[e >> 56];
+    uint32_t *cur = s_res, *nxt = s_res + capr + 1;
+    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const int64_t nb = ref.nband[f];
+    for (int64_t b = 0; b < nb; b++) {
+        for (uint32_t t = lane; t < nt; t += 32) {
+            if (finb[t] != (uint32_t)b) continue;
+            const uint32_t R = fin[t];
+            troot[t] = (R & REF_SYM) ? cur[R & ~REF_SYM] : R;
+        }
+        if (b + 1 < nb) {
+            const int64_t yb = bs[b + 1] - 1;
+            const int64_t rb = fd.node_off + yb * fd.qw;
+            const int64_t mb = ref.bm[fd.row0 + yb];
+            for (int64_t k = lane; k < mb; k += 32) {
+                const uint32_t rep = (uint32_t)(ref.binfo[rb + k] >> 32) & 0xffffu;
+                const uint32_t R = ref.outroot[rb + rep];
+                nxt[k] = (R & REF_SYM) ? cur[R & ~REF_SYM] : R;
             }
-            const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-            if (keep) {
-                const int64_t o = n + __popc(bal & lt);
-                A.c_se[o] = (uint32_t)e;
-                A.c_v[o] = (uint8_t)(e >> 48);
-                A.c_j[o] = (uint16_t)(e >> 32);
-                A.c_t[o] = (uint8_t)(e >> 56);
-            }
-            if (j == nraw - 1) last_kept = keep;
-            n += __popc(bal);
+            __syncwarp();
+            uint32_t *t = cur;
+            cur = nxt;
+            nxt = t;
         }
-        last_kept = __shfl_sync(0xffffffffu, last_kept, (int)((nraw - 1) & 31)) && nraw > 0;
-        const bool link = (tr >> 31) && last_kept;
-        const int64_t E = m + n + 1, vn = m + n;
-        __syncwarp();
-        for (int64_t e = lane; e < E; e += 32) {
-            A.e_par[e] = (uint16_t)e;
-            A.e_fpar[e] = (uint16_t)e;
-            A.e_tot[e] = 0;
-            A.e_max[e] = 0;
-            A.e_c0[e] = 0xffffffffu;
-            A.e_c1[e] = 0;
-            if (e < m) {
-                A.e_R[e] = A.s_R[e];
-                A.e_Z[e] = A.s_Z[e];
-                A.e_flag[e] = 0;
-            } else if (e < vn) {
-                const uint32_t se = A.c_se[e - m];
-                A.e_R[e] = rbase + A.c_j[e - m];
-                A.e_Z[e] = (se >> 16) - (se & 0xffffu) + 1;
-                A.e_flag[e] = REF_TOUCHED;
-            } else {
-                A.e_R[e] = vbase + (uint32_t)(y - 1);
-                A.e_Z[e] = 1;
-                A.e_flag[e] = link ? REF_TOUCHED : 0;
-            }
-        }
-        // the calls, in the reference's order: each run, its touching runs
-        // above in order (fast/unionfind.c:112-196), then the last column
-        int64_t nc = 0;
-        if (np > 0) {
-            for (int64_t i0 = 0; i0 < n; i0 += 32) {
-                const int64_t i = i0 + lane;
-                int64_t k0 = 0, cnt = 0;
-                int64_t a0 = 0, a1 = 0;
-                uint8_t v = 0;
-                if (i < n) {
-                    a0 = A.c_se[i] & 0xffffu;
-                    a1 = A.c_se[i] >> 16;
-                    v = A.c_v[i];
-                    int64_t lo = 0, hi = np;
-                    while (lo < hi) {
-                        const int64_t mid = (lo + hi) >> 1;
-                        if ((int64_t)(A.p_se[mid] >> 16) + 1 < a0)
-                            lo = mid + 1;
-                        else
-                            hi = mid;
-                    }
-                    k0 = lo;
-                    for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
-                        if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) cnt++;
-                }
-                uint32_t incl = (uint32_t)cnt;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-                if (nc + total + 1 > 2 * capr + 2) {  // more calls than the arrays hold
-                    if (lane == 0) atomicOr(err, AT_ERR_ORDER);
-                    return;
-                }
-                int64_t o = nc + incl - cnt;
-                if (i < n)
-                    for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
-                        if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) {
-                            A.call_a[o] = (uint16_t)(m + i);
-                            A.call_b[o] = A.p_slot[k];
-                            o++;
-                        }
-                nc += total;
-            }
-        }
-        if (link) {
-            if (lane == 0) {
-                A.call_a[nc] = (uint16_t)(vn - 1);
-                A.call_b[nc] = (uint16_t)vn;
-            }
-            nc++;
-        }
-        __syncwarp();
-        // groups
-        for (int64_t c = lane; c < nc; c += 32) {
-            el_unite(A.e_par, A.call_a[c], A.call_b[c]);
-            A.e_flag[A.call_b[c]] = REF_TOUCHED;
-        }
-        __syncwarp();
-        // every element's group root (read-only walks into e_tot, then
-        // copied: a halving write racing a final write could leave a
-        // non-root parent)
-        for (int64_t e = lane; e < E; e += 32) {
-            uint32_t x = (uint32_t)e;
-            while (A.e_par[x] != x) x = A.e_par[x];
-            A.e_tot[e] = x;
-        }
-        __syncwarp();
-        for (int64_t e = lane; e < E; e += 32) {
-            A.e_par[e] = (uint16_t)A.e_tot[e];
-            A.e_tot[e] = 0;
-        }
-        __syncwarp();
-        // per group: pixels, the largest set that existed before the row,
-        // and the range of its calls
-        for (int64_t e = lane; e < E; e += 32) {
-            if (!A.e_flag[e]) continue;
-            const uint32_t g = A.e_par[e];
-            atomicAdd(&A.e_tot[g], A.e_Z[e]);
-            if (e < m || e == vn) atomicMax(&A.e_max[g], (unsigned long long)A.e_Z[e] << 16 | (uint64_t)e);
-        }
-        for (int64_t c = lane; c < nc; c += 32) {
-            const uint32_t g = A.e_par[A.call_a[c]];
-            atomicMin(&A.e_c0[g], (uint32_t)c);
-            atomicMax(&A.e_c1[g], (uint32_t)c);
-        }
-        __syncwarp();
-        // each group's root and pixels, into its root element
-        for (int64_t g = lane; g < E; g += 32) {
-            if (!A.e_flag[g] || A.e_par[g] != g) continue;
-            const unsigned long long mx = A.e_max[g];
-            const uint32_t zmax = (uint32_t)(mx >> 16), tot = A.e_tot[g];
-            if (mx != 0 && zmax > tot - zmax) {
-                A.e_R[g] = A.e_R[mx & 0xffffu];
-                A.e_Z[g] = tot;
-                continue;
-            }
-            // no set outweighs the rest: the reference's calls one by one
-            for (uint32_t c = A.e_c0[g]; c <= A.e_c1[g] && c < (uint32_t)nc; c++) {
-                const uint32_t a = A.call_a[c];
-                if (A.e_par[a] != g) continue;
-                const uint32_t ra = fold_find(A.e_fpar, a), rb = fold_find(A.e_fpar, A.call_b[c]);
-                if (ra == rb) continue;
-                const uint32_t za = A.e_Z[ra], zb = A.e_Z[rb];
-                if (za > zb) {
-                    A.e_fpar[rb] = (uint16_t)ra;
-                    A.e_Z[ra] = za + zb;
-                } else {
-                    A.e_fpar[ra] = (uint16_t)rb;
-                    A.e_Z[rb] = za + zb;
-                }
-            }
-            const uint32_t r = fold_find(A.e_fpar, (uint32_t)g);
-            const uint32_t R = A.e_R[r], Z = A.e_Z[r];
-            A.e_R[g] = R;
-            A.e_Z[g] = Z;
-        }
-        __syncwarp();
-        // a slot no call reached is a whole component: its root is final
-        for (int64_t e = lane; e < m; e += 32) {
-            const uint32_t t = A.s_t[e];
-            if (A.e_flag[e] || t == REF_NONE || s_done[t]) continue;
-            troot[t] = A.s_R[e];
-            s_done[t] = 1;
-            atomicAdd(&s_ndone, 1u);
-        }
-        // the new slots: one per group of this row's runs, numbered by its
-        // first run (e_tot of the root is free again and holds that run)
-        for (int64_t i = lane; i < n; i += 32) A.e_tot[A.e_par[m + i]] = 0xffffffffu;
-        __syncwarp();
-        for (int64_t i = lane; i < n; i += 32) atomicMin(&A.e_tot[A.e_par[m + i]], (uint32_t)i);
-        __syncwarp();
-        int64_t mnew = 0;
-        for (int64_t i0 = 0; i0 < n; i0 += 32) {
-            const int64_t i = i0 + lane;
-            uint32_t g = 0;
-            bool first = false;
-            if (i < n) {
-                g = A.e_par[m + i];
-                first = A.e_tot[g] == (uint32_t)i;
-            }
-            const uint32_t bal = __ballot_sync(0xffffffffu, first);
-            if (first) {
-                const int64_t k = mnew + __popc(bal & lt);
-                A.e_c0[g] = (uint32_t)k;  // the group's new slot
-                const uint32_t t = A.c_t[i], Z = A.e_Z[g];
-                A.s_R[k] = A.e_R[g];
-                A.s_Z[k] = Z;
-                A.s_t[k] = (uint8_t)t;
-                // more than half of the component: no later call can move the root
-                if (!s_done[t] && Z > tpx[t] - Z) {
-                    troot[t] = A.e_R[g];
-                    s_done[t] = 1;
-                    atomicAdd(&s_ndone, 1u);
-                }
-            }
-            mnew += __popc(bal);
-        }
-        __syncwarp();
-        // the open runs of this row, with their slots, for the next row
-        int64_t npn = 0;
-        for (int64_t i0 = 0; i0 < n; i0 += 32) {
-            const int64_t i = i0 + lane;
-            const bool keep = i < n && !s_done[A.c_t[i]];
-            const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-            if (keep) {
-                const int64_t o = npn + __popc(bal & lt);
-                A.p_se[o] = A.c_se[i];
-                A.p_v[o] = A.c_v[i];
-                A.p_slot[o] = (uint16_t)A.e_c0[A.e_par[m + i]];
-            }
-            npn += __popc(bal);
-        }
-        m = mnew;
-        np = npn;
-        __syncwarp();
-    }
-    // the sets still open at the bottom are whole components
-    for (int64_t k = lane; k < m; k += 32) {
-        const uint32_t t = A.s_t[k];
-        if (t == REF_NONE || s_done[t]) continue;
-        troot[t] = A.s_R[k];
-        s_done[t] = 1;
     }
     __syncwarp();
     // GPU node ids -> the reference's packed node numbers (a target left
@@ -580,17 +1077,27 @@ __global__ void __launch_bounds__(32) k_ref_replay(const FrameDesc *frames, RefO
 void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                       const uint32_t *row_nruns, int nfam, const int64_t *qstart, const GpuDetection *dets,
                       const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb, int64_t capr,
-                      uint8_t *scratch, size_t scratch_per_frame, const RefOrder &ref, uint32_t *err) {
+                      uint8_t *scratch, size_t scratch_per_block, const RefOrder &ref, uint32_t *err) {
     k_ref_targets<<<L.nframes, 256, 0, L.stream>>>(frames, nfam, qstart, dets, det_ok, qcl, ckey, nb, runs, row_nruns,
                                                    ref, err);
     const int64_t b = (L.max_qh + 7) / 8;
     const dim3 grid((unsigned)(b < 1 ? 1 : b < 148 ? b : 148), (unsigned)L.nframes);
     k_ref_mark<<<grid, 256, 0, L.stream>>>(frames, thr, runs, row_nruns, ref);
+    k_ref_cut<<<L.nframes, 32, 0, L.stream>>>(frames, ref);
+    const int64_t gb = (L.max_qh + REF_BAND - 1) / REF_BAND;
+    const unsigned bands = (unsigned)(gb < 1 ? 1 : gb);
+    k_ref_local<<<dim3(bands, (unsigned)L.nframes), 256, ref_local_bytes(), L.stream>>>(frames, ref, err);
+    k_ref_frontier<<<L.nframes, 256, ref_frontier_bytes(capr), L.stream>>>(frames, ref, capr);
     const size_t smem = scratch ? 0 : ref_replay_bytes(capr);
-    k_ref_replay<<<L.nframes, 32, smem, L.stream>>>(frames, ref, capr, scratch, scratch_per_frame, err);
+    k_ref_band<<<dim3(scratch ? REF_BAND_BLOCKS : bands, (unsigned)L.nframes), 32, smem, L.stream>>>(
+        frames, ref, capr, scratch, scratch_per_block, err);
+    k_ref_resolve<<<L.nframes, 32, 8 * (capr + 1), L.stream>>>(frames, ref, capr);
 }
 
 bool ref_replay_set_smem(size_t bytes) {
-    return cudaFuncSetAttribute(k_ref_replay, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
-           cudaSuccess;
+    return cudaFuncSetAttribute(k_ref_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess &&
+           cudaFuncSetAttribute(k_ref_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess &&
+           cudaFuncSetAttribute(k_ref_frontier, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_ref_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
 }

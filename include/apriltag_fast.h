@@ -237,7 +237,12 @@ void at_server_destroy(at_server *s);
      AT_DIAG_QUADS       per fitted quad: 8 f32 corners (quad image
                          coordinates) then i32 reversed_border, i32 frame
      AT_DIAG_SIZES       i64 qw, qh, points, clusters, quads, and the number
-                         of this library's kernels launched so far */
+                         of this library's kernels launched so far
+     AT_DIAG_ORDER_ROOTS u32 pairs, one per component next to a quad whose
+                         detection shares its id with another: the
+                         component's smallest node and the root that the
+                         reference's union order leaves it, both numbered
+                         as the reference packs its union-find nodes */
 enum {
     AT_DIAG_QUAD_IMAGE = 0,
     AT_DIAG_THRESHOLD = 1,
@@ -245,9 +250,26 @@ enum {
     AT_DIAG_POINTS = 3,
     AT_DIAG_CLUSTERS = 4,
     AT_DIAG_QUADS = 5,
-    AT_DIAG_SIZES = 6
+    AT_DIAG_SIZES = 6,
+    AT_DIAG_ORDER_ROOTS = 7
 };
 int64_t at_detector_diag(const at_detector *td, int what, void *dst, int64_t cap);
+
+/* Tag poses of all detections of the last at_detect / at_detect_batch, in
+   one launch on the GPU (a thread per detection): what the reference's
+   estimate_tag_pose_orthogonal_iteration gives with 50 iterations for each
+   detection (apriltag_pose.c:490-547), camera intrinsics fx, fy, cx, cy in
+   pixels and the tag's side in metres: the refined pose (R row-major, t)
+   and its object-space error, and the second local minimum (err2 HUGE_VAL
+   when there is none; estimate_tag_pose picks the smaller error). out[i]
+   belongs to td->detections[i]. Returns 0, 1 for bad arguments, 2 for a
+   CUDA error. No counterpart in the native API of the reference. */
+typedef struct at_pose {
+    double R[9], t[3], err;
+    double R2[9], t2[3], err2;
+} at_pose;
+int at_estimate_poses(const at_detector *td, double tagsize, double fx, double fy, double cx, double cy,
+                      at_pose *out);
 
 /* The threshold stage without any device allocation (it has no counterpart
    in the reference). For callers that cannot call cudaMalloc: a frame loop

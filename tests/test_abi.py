@@ -13,7 +13,7 @@ from oracle import oracle as O
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "apriltag_fast.h")
 UPSTREAM_HEADERS = [os.path.join(ROOT, "include", h) for h in (
-    "apriltag.h", "common/matd.h", "common/image_u8.h", "tag16h5.h", "tag25h9.h", "tag36h10.h", "tag36h11.h",
+    "apriltag.h", "apriltag_pose.h", "common/matd.h", "common/image_u8.h", "tag16h5.h", "tag25h9.h", "tag36h10.h", "tag36h11.h",
     "tagCircle21h7.h", "tagCircle49h12.h", "tagCustom48h12.h", "tagStandard41h12.h", "tagStandard52h13.h")]
 
 
@@ -37,8 +37,9 @@ def test_library_exports_the_upstream_api():
     L = C.CDLL(AT.LIB_PATH)
     names = []
     for h in UPSTREAM_HEADERS:
-        names += declared_functions(h, r"(?:apriltag|matd|image_u8|tag)\w+")
-    assert "apriltag_detector_detect" in names and "tag36h11_create" in names and len(names) >= 35
+        names += declared_functions(h, r"(?:apriltag|matd|image_u8|tag|estimate)\w+")
+    assert "apriltag_detector_detect" in names and "tag36h11_create" in names and len(names) >= 38
+    assert "estimate_tag_pose" in names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 
@@ -60,6 +61,7 @@ def test_upstream_struct_layouts_match_reference(tmp_path):
                       "nquads 72 tf 80 wp 88 mutex 96 fast 136 fb 144 fc 152")
     assert out[2] == "detection 112 family 0 id 8 hamming 12 dm 16 H 24 c 32 p 48"
     assert out[3] == "qtp 28 zarray 24 matd 16 image_u8 24 timeprofile 16"
+    assert out[4] == "info 48 det 0 tagsize 8 fx 16 fy 24 cx 32 cy 40 pose 16 R 0 t 8"
 
 
 def test_struct_layouts_match_reference():

@@ -157,6 +157,26 @@ def test_1080p_duplicate_ids_in_reference_order():
     assert repeated >= 15  # most frames keep both copies of a repeated id
 
 
+def test_order_roots_equal_the_oracle_roots():
+    """Stage check of the order replay: for each component beside a quad
+    whose id repeats, the root that the GPU's replay finds equals the root
+    of the reference's sequential union by size, as the oracle computes it
+    (fast/unionfind.c:15-45, 152-196), in the reference's node numbering."""
+    cfg, frames = _dup_seeds("1080p", 6, start=3000)
+    det = AT.Detector(list(cfg.families), 2)
+    fams = [H.oracle_family(f) for f in cfg.families]
+    checked = 0
+    for seed, img in frames:
+        det.detect(img)
+        pairs = det.diag("order_roots")
+        r = O.detect(img, fams, [2] * len(fams), O.default_params(), order=O.ORDER_REF)
+        for label, root in pairs:
+            assert r.label[label] == label, (seed, label)
+            assert r.ref_root[label] == root, (seed, label, int(r.ref_root[label]), int(root))
+        checked += len(pairs)
+    assert checked >= 20
+
+
 def test_1080p_duplicate_ids_batched():
     """The same frames in one batch (the order replay runs per frame)."""
     if O.ref_lib() is None:

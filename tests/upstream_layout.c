@@ -3,6 +3,7 @@
 #include <stdio.h>
 #include <stddef.h>
 #include "apriltag.h"
+#include "apriltag_pose.h"
 int main(void) {
     printf("family %zu ncodes %zu codes %zu wab %zu tw %zu rb %zu nbits %zu bx %zu by %zu h %zu name %zu impl %zu\n",
         sizeof(apriltag_family_t), offsetof(apriltag_family_t, ncodes), offsetof(apriltag_family_t, codes), offsetof(apriltag_family_t, width_at_border),
@@ -18,5 +19,9 @@ int main(void) {
         offsetof(apriltag_detection_t, id), offsetof(apriltag_detection_t, hamming), offsetof(apriltag_detection_t, decision_margin), offsetof(apriltag_detection_t, H),
         offsetof(apriltag_detection_t, c), offsetof(apriltag_detection_t, p));
     printf("qtp %zu zarray %zu matd %zu image_u8 %zu timeprofile %zu\n", sizeof(struct apriltag_quad_thresh_params), sizeof(zarray_t), sizeof(matd_t), sizeof(image_u8_t), sizeof(timeprofile_t));
+    printf("info %zu det %zu tagsize %zu fx %zu fy %zu cx %zu cy %zu pose %zu R %zu t %zu\n", sizeof(apriltag_detection_info_t),
+        offsetof(apriltag_detection_info_t, det), offsetof(apriltag_detection_info_t, tagsize), offsetof(apriltag_detection_info_t, fx),
+        offsetof(apriltag_detection_info_t, fy), offsetof(apriltag_detection_info_t, cx), offsetof(apriltag_detection_info_t, cy),
+        sizeof(apriltag_pose_t), offsetof(apriltag_pose_t, R), offsetof(apriltag_pose_t, t));
     return 0;
 }
