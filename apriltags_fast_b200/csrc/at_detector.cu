@@ -97,7 +97,7 @@ enum {
     B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_QNUM, B_FIRST, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
     B_HYMIN, B_HYMAX, B_CSPAN, B_CY0, B_SPANOFF, B_PKFRAME, B_PGKEYS, B_PGSLOTS, B_PFRAMES, B_PBSUM, B_SEG,
     B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
-    B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RLCNT, B_RNBAND, B_RLTOP, B_RLPX, B_RLBOT,
+    B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RBWIDE, B_RDESC, B_RNBAND, B_RFSCR, B_RLTOP, B_RLPX, B_RLBOT,
     B_RLPX2,
     B_CUB, B_ERR, B_NBUF
 };
@@ -674,7 +674,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_ROUTROOT].ensure(nodes * 4));
         CK(B[B_RBM].ensure(rows * 4));
         CK(B[B_RBSTART].ensure((rows + n) * 4));
-        CK(B[B_RLCNT].ensure((rows + n) * 4));
+        CK(B[B_RBWIDE].ensure((rows + n) * 4));
+        CK(B[B_RDESC].ensure((rows + n) * 16));
         CK(B[B_RNBAND].ensure(n * 4));
         CK(B[B_RLTOP].ensure(nodes * 4));
         CK(B[B_RLPX].ensure(nodes * 4));
@@ -685,25 +686,33 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         const RefOrder ro{B[B_RNEED].as<uint32_t>(),   B[B_RNT].as<uint32_t>(),     B[B_RTLAB].as<uint32_t>(),
                           B[B_RTPX].as<uint32_t>(),    B[B_RTROOT].as<uint32_t>(),  B[B_RTLIST].as<uint64_t>(),
                           B[B_RTROW].as<uint32_t>(),   B[B_RPRE].as<uint32_t>(),    B[B_RFIN].as<uint32_t>(),
-                          B[B_RFINB].as<uint32_t>(),   B[B_RBSTART].as<uint32_t>(), B[B_RLCNT].as<uint32_t>(),
-                          B[B_RNBAND].as<uint32_t>(),  B[B_RLTOP].as<uint32_t>(),   B[B_RLPX].as<uint32_t>(),
+                          B[B_RFINB].as<uint32_t>(),   B[B_RBSTART].as<uint32_t>(), B[B_RBWIDE].as<uint32_t>(),
+                          B[B_RDESC].as<uint4>(),      B[B_RNBAND].as<uint32_t>(),  B[B_RLTOP].as<uint32_t>(),
+                          B[B_RLPX].as<uint32_t>(),
                           B[B_RLBOT].as<uint32_t>(),   B[B_RLPX2].as<uint32_t>(),   B[B_RBSLOT].as<uint16_t>(),
                           B[B_RBINFO].as<uint64_t>(),  B[B_ROUTROOT].as<uint32_t>(), B[B_RBM].as<uint32_t>()};
         int64_t capr = 1;
         for (auto &f : fd) capr = f.qw - 1 > capr ? f.qw - 1 : capr;
-        const size_t rbytes = ref_replay_bytes(capr), fbytes = ref_frontier_bytes(capr);
         if (nodes >= ((int64_t)1 << 31)) {  // the replay marks symbols with the top bit of a node id
             set_error(in, 2, "batch too large for the order replay (node ids above 2^31)");
             return false;
         }
-        if (capr > REF_PCAP || fbytes > AT_REF_SMEM_MAX) {
+        if (capr > REF_PCAP) {
             set_error(in, 2, "quad image too wide for the order replay (" + std::to_string(capr + 1) + " px)");
             return false;
         }
-        uint8_t *rscr = nullptr;
-        if (rbytes > AT_REF_SMEM_MAX) {
-            CK(B[B_RSCR].ensure(rbytes * n * REF_BAND_BLOCKS));
-            rscr = B[B_RSCR].as<uint8_t>();
+        // the frontier pass and the wide-row replay work in global scratch
+        // when their arrays do not fit the shared memory
+        RefPlan plan{capr, capr > REF_PCAP_MIN ? capr : REF_PCAP_MIN, nullptr, 0, nullptr, 0};
+        if (ref_frontier_bytes(capr, true) > AT_REF_SMEM_MAX) {
+            plan.front_bytes = ref_frontier_bytes(capr, false);
+            CK(B[B_RFSCR].ensure(plan.front_bytes * n));
+            plan.front_scratch = B[B_RFSCR].as<uint8_t>();
+        }
+        if (capr > REF_SMALLR && ref_band_bytes(capr, true) > AT_REF_SMEM_MAX) {
+            plan.band_bytes = ref_replay_bytes(capr);
+            CK(B[B_RSCR].ensure(plan.band_bytes * n * REF_BAND_BLOCKS));
+            plan.band_scratch = B[B_RSCR].as<uint8_t>();
         }
         if (in->ref_smem == 0) {
             if (!ref_replay_set_smem(AT_REF_SMEM_MAX)) {
@@ -714,8 +723,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         }
         launch_ref_order(L, dfr, thr, runs, B[B_ROWRUNS].as<uint32_t>(), in->nfam, B[B_QSTART].as<int64_t>(),
                          B[B_DETS].as<GpuDetection>(), B[B_DETOK].as<uint32_t>(), B[B_QCL].as<uint32_t>(), ckey, nb,
-                         capr, rscr, rbytes, ro, B[B_ERR].as<uint32_t>());
-        in->launches += 7;
+                         plan, ro, B[B_ERR].as<uint32_t>());
+        in->launches += ref_order_launches(plan);
         launch_finalize(st, (int)n, B[B_QSTART].as<int64_t>(), in->nfam, B[B_DETS].as<GpuDetection>(),
                         B[B_DETOK].as<uint32_t>(), B[B_DIDX].as<uint32_t>(), B[B_DRM].as<uint8_t>(),
                         B[B_OUT].as<GpuDetection>(), B[B_OUTOFF].as<int64_t>(), B[B_OUTN].as<int64_t>(), dfr, ro,

@@ -119,7 +119,9 @@ void launch_decode(cudaStream_t s, const FrameDesc *frames, const GpuParams &prm
 // row plus one per frame, the runs above the row (rpre).
 #define AT_REF_MAXT 192
 #define REF_BAND 16         // rows per band of the replay, at most
-#define REF_PCAP 4160       // target runs per band, at most (a row always fits: quad images up to 4161 px wide)
+#define REF_PCAP 4160       // target runs of a row, at most (quad images up to 4161 px wide)
+#define REF_PCAP_MIN 2048   // target runs per band, at most, when every row has fewer
+#define REF_SMALLR 256      // the replay's narrow class: rows of at most this many target runs
 #define REF_BAND_BLOCKS 32  // replay blocks per frame when the replay works in a global scratch
 struct RefOrder {
     uint32_t *need, *nt;
@@ -128,29 +130,41 @@ struct RefOrder {
     uint32_t *trow;
     uint32_t *rpre;
     uint32_t *fin, *finb;     // per target: its root (node or symbol) and the band where it was found
-    // bands (rows + one per frame each): first row of each band and the last
-    // band's end; the band's component counts; per frame: the band count
-    uint32_t *bstart, *lcnt, *nband;
+    // per band (rows + one per frame each): first row (and the end after the
+    // last band), the widest row, the band's summary (at_order.cu); per
+    // frame: the band count
+    uint32_t *bstart, *bwide;
+    uint4 *desc;
+    uint32_t *nband;
     // per node (at the rows of the band edges, at_order.cu):
     uint32_t *ltop, *lpx;     //   top row: each run's band component, their pixels
     uint32_t *lbot, *lpx2;    //   bottom row: each run's band component, the others' pixels
     uint16_t *bslot;          //   row above a band: each target run's slot
     uint64_t *binfo;          //   row above a band: each slot, pixels | first run << 32 | target << 48
-    uint32_t *outroot;        //   bottom row: each run's root after the band
+    uint32_t *outroot;        //   row above a band: each slot's root after the band above
     uint32_t *bm;             // per row: slots at the row above a band
 };
-// Shared-memory bytes of the band replay (rows of at most capr runs), of the
-// band components and of the frontier pass; above AT_REF_SMEM_MAX the band
-// replay takes a global scratch of that size per block (REF_BAND_BLOCKS
-// blocks per frame).
+// The sizes the order replay runs at: capr, the most runs in a row of the
+// batch; pcap, the most target runs of a band; global scratch regions (a
+// frame's, a block's) for the frontier pass and the wide-row replay when
+// their arrays exceed the shared memory (else null).
+struct RefPlan {
+    int64_t capr, pcap;
+    uint8_t *front_scratch;
+    size_t front_bytes;
+    uint8_t *band_scratch;
+    size_t band_bytes;
+};
 size_t ref_replay_bytes(int64_t capr);
-size_t ref_local_bytes();
-size_t ref_frontier_bytes(int64_t capr);
+size_t ref_band_bytes(int64_t capr, bool staged);
+size_t ref_local_bytes(int64_t pcap);
+size_t ref_frontier_bytes(int64_t capr, bool staged);
 bool ref_replay_set_smem(size_t bytes);
+int ref_order_launches(const RefPlan &P);
 void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                       const uint32_t *row_nruns, int nfam, const int64_t *qstart, const GpuDetection *dets,
-                      const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb, int64_t capr,
-                      uint8_t *scratch, size_t scratch_per_block, const RefOrder &ref, uint32_t *err);
+                      const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb,
+                      const RefPlan &P, const RefOrder &ref, uint32_t *err);
 // okey: 2 u64 + 1 u32 per detection slot (the order keys, a second index)
 void launch_finalize(cudaStream_t s, int nframes, const int64_t *frame_qstart, int nfam, const GpuDetection *dets,
                      const uint32_t *det_ok, uint32_t *idx, uint8_t *removed, GpuDetection *out,

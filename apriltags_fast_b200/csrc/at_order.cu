@@ -323,7 +323,7 @@ struct RowState {
     int64_t m, np;
 };
 
-__device__ bool replay_row(ReplayArrays &A, RowState &S, int64_t n, bool link, uint32_t rbase, uint32_t vnode,
+__device__ __forceinline__ bool replay_row(ReplayArrays &A, RowState &S, int64_t n, bool link, uint32_t rbase, uint32_t vnode,
                            int64_t capr, uint32_t *fin, uint32_t *finb, uint32_t band, uint32_t *err) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -510,30 +510,11 @@ __device__ bool replay_row(ReplayArrays &A, RowState &S, int64_t n, bool link, u
     return true;
 }
 
-// Loads the target runs of row y (rbase: its first node) into c_*;
-// returns their count and whether the row's last-column link joins one.
-__device__ int64_t load_row(ReplayArrays &A, const RefOrder &ref, const FrameDesc &fd, int64_t y, bool *link) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t tr = ref.trow[fd.row0 + y];
-    const int64_t n = tr & 0x7fffffffu;
-    const uint32_t rbase = (uint32_t)(fd.node_off + y * fd.qw);
-    for (int64_t j = lane; j < n; j += 32) {
-        const uint64_t e = ref.tlist[rbase + j];
-        A.c_se[j] = (uint32_t)e;
-        A.c_v[j] = (uint8_t)(e >> 48);
-        A.c_j[j] = (uint16_t)(e >> 32);
-        A.c_t[j] = (uint8_t)(e >> 56);
-    }
-    *link = (tr >> 31) != 0;
-    return n;
-}
-
-
 // ---------------------------------------------------------------------------
-// Bands. The rows of a frame go in bands (at most REF_BAND rows and
-// REF_PCAP target runs each), replayed in parallel. A band's replay needs
-// the sets of target runs that touch the row above it as the reference has
-// them there, with their pixel counts. Which runs are together and how many
+// Bands. The rows of a frame go in bands (at most REF_BAND rows and pcap
+// target runs each), replayed in parallel. A band's replay needs the sets
+// of target runs that touch the row above it as the reference has them
+// there, with their pixel counts. Which runs are together and how many
 // pixels a set holds do not depend on which root wins, so these come from
 // an order-free union-find in two steps: k_ref_local joins the runs inside
 // each band (all bands at once) and summarises the band by its components
@@ -542,8 +523,12 @@ __device__ int64_t load_row(ReplayArrays &A, const RefOrder &ref, const FrameDes
 // carries the incoming sets' roots as symbols, and k_ref_resolve puts the
 // roots in from the top down.
 //
-// Band b covers rows bstart[b] .. bstart[b + 1] - 1. Node-indexed arrays,
-// at the nodes of a row y (node_off + y qw + i):
+// Per band b (at row0 + frame + b): bstart[b] its first row (and the end
+// after the last band), bwide[b] the most target runs of one of its rows or
+// of the row above, desc[b] = (first row, end row, components reaching the
+// top | others reaching the bottom << 16, runs of the top row | of the
+// bottom row << 16). Node-indexed arrays, at the nodes of a row y
+// (node_off + y qw + i):
 //   ltop[j]    top row of a band: the band component of target run j,
 //              numbered by first run among the components that reach it
 //   lpx[c]     top row: pixels of band component c
@@ -553,9 +538,9 @@ __device__ int64_t load_row(ReplayArrays &A, const RefOrder &ref, const FrameDes
 //   bslot[j]   row above a band: the slot (prefix set) of target run j
 //   binfo[s]   row above a band: slot s, pixels | first run << 32 |
 //              target << 48
-//   outroot[j] the bottom row of a band: the root of run j's set after it
-// and per row: bm[y] the slots at the row above a band; per band:
-// lcnt[b] = components reaching the top | the others reaching the bottom << 16.
+//   outroot[s] row above a band: the root of slot s's set after the band
+//              above (a node or a symbol of that band)
+// and per row: bm[y] the slots at the row above a band.
 
 #define REF_KNONE 0x3fffffffu  // no run yet: above every run index, below the flags
 #define REF_KTOP 0x80000000u   // numbered: the component's index
@@ -611,46 +596,86 @@ __device__ __forceinline__ uint32_t first_reaching(const uint32_t *se, uint32_t 
     return lo;
 }
 
-// The band cut of each frame, a warp per frame: bands of up to REF_BAND
-// rows whose target runs stay within REF_PCAP.
-__global__ void __launch_bounds__(32) k_ref_cut(const FrameDesc *frames, RefOrder ref) {
+// Asynchronous global -> shared copies (sm_80 and later), for staging the
+// next row or band while the current one is worked on.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// The band cut of each frame, a warp per frame: the rows in blocks of
+// REF_BAND, each block one band, or several when its target runs exceed
+// pcap (cut greedily, whole rows). bwide[b]: the most target runs in a row
+// of band b or in the row above it (the replay's row capacity).
+__global__ void __launch_bounds__(32) k_ref_cut(const FrameDesc *frames, RefOrder ref, uint32_t pcap) {
     const int f = blockIdx.x;
     if (!ref.need[f]) return;
     const FrameDesc fd = frames[f];
     const int lane = threadIdx.x;
-    uint32_t *bs = ref.bstart + fd.row0 + f;
-    uint32_t nb = 0, acc = 0;
-    int rows = 0;
-    for (int64_t y0 = 0; y0 < fd.qh; y0 += 32) {
-        const int64_t y = y0 + lane;
-        const uint32_t c = y < fd.qh ? (ref.trow[fd.row0 + y] & 0x7fffffffu) : 0u;
-        const int kn = fd.qh - y0 < 32 ? (int)(fd.qh - y0) : 32;
-        for (int k = 0; k < kn; k++) {
-            const uint32_t ck = __shfl_sync(0xffffffffu, c, k);
-            if (rows == 0 || rows == REF_BAND || acc + ck > REF_PCAP) {
-                if (lane == 0) bs[nb] = (uint32_t)(y0 + k);
-                nb++;
-                acc = 0;
-                rows = 0;
+    uint32_t *bs = ref.bstart + fd.row0 + f, *bw = ref.bwide + fd.row0 + f;
+    const uint32_t *tr = ref.trow + fd.row0;
+    const int64_t nblk = (fd.qh + REF_BAND - 1) / REF_BAND;
+    uint32_t base = 0;
+    for (int64_t k0 = 0; k0 < nblk; k0 += 32) {
+        const int64_t k = k0 + lane;
+        const int64_t y0 = k * REF_BAND;
+        const int nr = k < nblk ? (int)(fd.qh - y0 < REF_BAND ? fd.qh - y0 : REF_BAND) : 0;
+        uint32_t c[REF_BAND];
+        uint32_t above = 0, nbk = 0, acc = 0;
+        if (nr > 0 && y0 > 0) above = tr[y0 - 1] & 0x7fffffffu;
+#pragma unroll
+        for (int r = 0; r < REF_BAND; r++) c[r] = r < nr ? (tr[y0 + r] & 0x7fffffffu) : 0u;
+#pragma unroll
+        for (int r = 0; r < REF_BAND; r++)
+            if (r < nr) {
+                if (r == 0 || acc + c[r] > pcap) {
+                    nbk++;
+                    acc = 0;
+                }
+                acc += c[r];
             }
-            acc += ck;
-            rows++;
+        uint32_t total;
+        const uint32_t off = warp_excl_scan(nbk, &total);
+        if (nr > 0) {
+            uint32_t bi = base + off, wide = 0;
+            acc = 0;
+#pragma unroll
+            for (int r = 0; r < REF_BAND; r++)
+                if (r < nr) {
+                    if (r == 0 || acc + c[r] > pcap) {
+                        if (r > 0) bw[bi++] = wide;
+                        bs[bi] = (uint32_t)(y0 + r);
+                        acc = 0;
+                        wide = r == 0 ? above : c[r - 1];
+                    }
+                    acc += c[r];
+                    wide = wide > c[r] ? wide : c[r];
+                }
+            bw[bi] = wide;
         }
+        base += total;
     }
     if (lane == 0) {
-        bs[nb] = (uint32_t)fd.qh;
-        ref.nband[f] = nb;
+        bs[base] = (uint32_t)fd.qh;
+        ref.nband[f] = base;
     }
 }
 
-// The shared-memory layout of k_ref_local: REF_PCAP runs and a last-column
+// The shared-memory layout of k_ref_local: pcap runs and a last-column
 // node per row.
 struct LocalArrays {
     uint32_t *se, *par, *Z, *tot, *key;
     uint8_t *v;
 };
-__host__ __device__ inline size_t ref_local_carve(uint8_t *base, LocalArrays *A) {
-    const int64_t cape = REF_PCAP + REF_BAND;
+__host__ __device__ inline size_t ref_local_carve(uint8_t *base, int64_t pcap, LocalArrays *A) {
+    const int64_t cape = pcap + REF_BAND;
     size_t at = 0;
     auto take = [&](size_t bytes) {
         uint8_t *p = base + at;
@@ -658,20 +683,21 @@ __host__ __device__ inline size_t ref_local_carve(uint8_t *base, LocalArrays *A)
         return p;
     };
     LocalArrays a;
-    a.se = (uint32_t *)take(4 * REF_PCAP);
+    a.se = (uint32_t *)take(4 * pcap);
     a.par = (uint32_t *)take(4 * cape);
     a.Z = (uint32_t *)take(4 * cape);
     a.tot = (uint32_t *)take(4 * cape);
     a.key = (uint32_t *)take(4 * cape);
-    a.v = take(REF_PCAP);
+    a.v = take(pcap);
     if (A) *A = a;
     return at;
 }
-size_t ref_local_bytes() { return ref_local_carve(nullptr, nullptr); }
+size_t ref_local_bytes(int64_t pcap) { return ref_local_carve(nullptr, pcap, nullptr); }
 
 // A block per band (the frame's bands taken in turn by its blocks): the
 // band's components, their pixels, and the summaries named above.
-__global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefOrder ref, uint32_t *err) {
+__global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefOrder ref, uint32_t pcap,
+                                                   uint32_t *err) {
     extern __shared__ __align__(16) uint8_t s_mem[];
     __shared__ uint32_t s_roff[REF_BAND + 1];
     __shared__ uint8_t s_link[REF_BAND];
@@ -682,7 +708,7 @@ __global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefO
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     const uint32_t lt = (1u << lane) - 1u;
     LocalArrays A;
-    ref_local_carve(s_mem, &A);
+    ref_local_carve(s_mem, pcap, &A);
     const uint32_t *bs = ref.bstart + fd.row0 + f;
     const int64_t nb = ref.nband[f];
     for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
@@ -705,7 +731,7 @@ __global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefO
         }
         __syncthreads();
         const uint32_t L = s_roff[nr];
-        if (L > REF_PCAP) {  // the cut keeps bands within REF_PCAP when a row fits
+        if (L > pcap) {  // the cut keeps bands within pcap when a row fits
             if (tid == 0) atomicOr(err, AT_ERR_ORDER);
             return;
         }
@@ -817,16 +843,24 @@ __global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefO
             const uint32_t kg = A.key[A.Z[lb + i]];
             ref.lbot[rb + i] = (kg & REF_KTOP) ? (kg & 0xffffu) : (0x80000000u | (kg & 0xffffu));
         }
-        if (tid == 0) ref.lcnt[fd.row0 + f + b] = s_ntop | s_nnon << 16;
+        if (tid == 0)
+            ref.desc[fd.row0 + f + b] = make_uint4((uint32_t)y0, (uint32_t)y1, s_ntop | s_nnon << 16, n0 | nbot << 16);
         __syncthreads();
     }
 }
 
-// The shared-memory layout of k_ref_frontier (rows of at most capr runs).
+// The frontier pass's arrays (rows of at most capr runs), and the staging
+// of one band's summaries (two of them, the next band's copies landing
+// while this band is worked on).
 struct FrontArrays {
     uint32_t *f_se, *s_Z, *par, *Z, *tot, *key, *bk;
     uint16_t *f_slot;
     uint8_t *f_v;
+};
+struct FrontStage {
+    const uint64_t *top_tl, *bot_tl;  // target runs of the band's top and bottom rows
+    const uint32_t *top_c, *bot_c;    // their band components (ltop, lbot)
+    const uint32_t *px, *px2;         // lpx, lpx2
 };
 __host__ __device__ inline size_t ref_front_carve(uint8_t *base, int64_t capr, FrontArrays *A) {
     const int64_t cape = 2 * capr + 2;
@@ -849,11 +883,54 @@ __host__ __device__ inline size_t ref_front_carve(uint8_t *base, int64_t capr, F
     if (A) *A = a;
     return at;
 }
-size_t ref_frontier_bytes(int64_t capr) { return ref_front_carve(nullptr, capr, nullptr); }
+__host__ __device__ inline size_t ref_stage_carve(uint8_t *base, int64_t capr, FrontStage *S) {
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        uint8_t *p = base + at;
+        at = ref_align(at + bytes);
+        return p;
+    };
+    FrontStage s;
+    s.top_tl = (const uint64_t *)take(8 * capr);
+    s.bot_tl = (const uint64_t *)take(8 * capr);
+    s.top_c = (const uint32_t *)take(4 * capr);
+    s.bot_c = (const uint32_t *)take(4 * capr);
+    s.px = (const uint32_t *)take(4 * capr);
+    s.px2 = (const uint32_t *)take(4 * capr);
+    if (S) *S = s;
+    return at;
+}
+size_t ref_frontier_bytes(int64_t capr, bool staged) {
+    return ref_front_carve(nullptr, capr, nullptr) + (staged ? 2 * ref_stage_carve(nullptr, capr, nullptr) : 0);
+}
+
+// A band's summaries: staged copies (issued by every thread of the block)
+// or, without staging, the global arrays themselves.
+__device__ __forceinline__ void front_issue(const FrontStage &S, const RefOrder &ref, const FrameDesc &fd, uint4 d,
+                                            int tid, int nt) {
+    const int64_t rt = fd.node_off + (int64_t)d.x * fd.qw, rb = fd.node_off + (int64_t)(d.y - 1) * fd.qw;
+    const uint32_t ntop = d.z & 0xffffu, nnon = d.z >> 16, n0 = d.w & 0xffffu, nbot = d.w >> 16;
+    for (uint32_t j = tid; j < n0; j += nt) {
+        cp_async8((void *)(S.top_tl + j), ref.tlist + rt + j);
+        cp_async4((void *)(S.top_c + j), ref.ltop + rt + j);
+    }
+    for (uint32_t j = tid; j < ntop; j += nt) cp_async4((void *)(S.px + j), ref.lpx + rt + j);
+    for (uint32_t j = tid; j < nbot; j += nt) {
+        cp_async8((void *)(S.bot_tl + j), ref.tlist + rb + j);
+        cp_async4((void *)(S.bot_c + j), ref.lbot + rb + j);
+    }
+    for (uint32_t j = tid; j < nnon; j += nt) cp_async4((void *)(S.px2 + j), ref.lpx2 + rb + j);
+}
+__device__ __forceinline__ FrontStage front_direct(const RefOrder &ref, const FrameDesc &fd, uint4 d) {
+    const int64_t rt = fd.node_off + (int64_t)d.x * fd.qw, rb = fd.node_off + (int64_t)(d.y - 1) * fd.qw;
+    return FrontStage{ref.tlist + rt, ref.tlist + rb, ref.ltop + rt, ref.lbot + rb, ref.lpx + rt, ref.lpx2 + rb};
+}
 
 // A block per frame, band after band: the prefix sets at the bottom row of
-// each band (slots), from the slots above and the band's summaries.
-__global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, RefOrder ref, int64_t capr) {
+// each band (slots), from the slots above and the band's summaries. With
+// `scratch`, the arrays live there (a region per frame) and nothing is staged.
+__global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, RefOrder ref, int64_t capr,
+                                                      uint8_t *scratch, size_t scratch_per_block) {
     extern __shared__ __align__(16) uint8_t s_mem[];
     __shared__ uint32_t s_m;
     const int f = blockIdx.x;
@@ -861,17 +938,31 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
     const FrameDesc fd = frames[f];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     const uint32_t lt = (1u << lane) - 1u;
+    const bool staged = scratch == nullptr;
     FrontArrays A;
-    ref_front_carve(s_mem, capr, &A);
-    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const size_t fb = ref_front_carve(staged ? s_mem : scratch + (size_t)f * scratch_per_block, capr, &A);
+    const size_t sb = ref_stage_carve(nullptr, capr, nullptr);
+    auto stage = [&](int64_t i) {  // staging buffer i (0 or 1)
+        FrontStage S;
+        ref_stage_carve(s_mem + fb + (size_t)i * sb, capr, &S);
+        return S;
+    };
+    const uint4 *desc = ref.desc + fd.row0 + f;
     const int64_t nb = ref.nband[f];
+    uint4 d0 = desc[0], d1 = nb > 1 ? desc[1] : make_uint4(0, 0, 0, 0);
+    if (staged) front_issue(stage(0), ref, fd, d0, tid, nt);
+    cp_async_commit();
     int64_t m = 0, nf = 0;  // the slots and runs of the row above the band
     for (int64_t b = 0; b < nb; b++) {
-        const int64_t y0 = bs[b], y1 = bs[b + 1];
-        const uint32_t lc = ref.lcnt[fd.row0 + f + b];
-        const int64_t ntop = lc & 0xffffu, nnon = lc >> 16;
-        const int64_t rt = fd.node_off + y0 * fd.qw, rb = fd.node_off + (y1 - 1) * fd.qw;
-        const int64_t n0 = ref.trow[fd.row0 + y0] & 0x7fffffffu, nbot = ref.trow[fd.row0 + y1 - 1] & 0x7fffffffu;
+        const uint4 d2 = b + 2 < nb ? desc[b + 2] : make_uint4(0, 0, 0, 0);
+        if (staged && b + 1 < nb) front_issue(stage((b + 1) & 1), ref, fd, d1, tid, nt);
+        cp_async_commit();
+        cp_async_wait_one();
+        __syncthreads();
+        const FrontStage S = staged ? stage(b & 1) : front_direct(ref, fd, d0);
+        const int64_t y1 = d0.y;
+        const int64_t ntop = d0.z & 0xffffu, nnon = d0.z >> 16, n0 = d0.w & 0xffffu, nbot = d0.w >> 16;
+        const int64_t rb = fd.node_off + (y1 - 1) * fd.qw;
         const bool boundary = y1 < fd.qh;
         // elements: the slots [0, m), the band's components that reach its
         // top row [m, m + ntop); keys of the bottom row's sets: those
@@ -880,16 +971,17 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
         for (int64_t e = tid; e < E; e += nt) {
             A.par[e] = (uint32_t)e;
             A.tot[e] = 0;
-            A.Z[e] = e < m ? A.s_Z[e] : ref.lpx[rt + (e - m)];
+            A.Z[e] = e < m ? A.s_Z[e] : S.px[e - m];
         }
         for (int64_t e = tid; e < E + nnon; e += nt) A.key[e] = REF_KNONE;
         __syncthreads();
         if (nf > 0)
             for (int64_t j = tid; j < n0; j += nt) {
-                const uint32_t se = (uint32_t)ref.tlist[rt + j];
-                const uint8_t v = (uint8_t)(ref.tlist[rt + j] >> 48);
+                const uint64_t te = S.top_tl[j];
+                const uint32_t se = (uint32_t)te;
+                const uint8_t v = (uint8_t)(te >> 48);
                 const int64_t a0 = se & 0xffffu, a1 = se >> 16;
-                const uint32_t c = ref.ltop[rt + j];
+                const uint32_t c = S.top_c[j];
                 for (uint32_t k = first_reaching(A.f_se, 0, (uint32_t)nf, a0);
                      k < nf && (int64_t)(A.f_se[k] & 0xffffu) <= a1 + 1; k++)
                     if (A.f_v[k] == v && runs_touch(a0, a1, A.f_se[k] & 0xffffu, A.f_se[k] >> 16, v))
@@ -911,7 +1003,7 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
         __syncthreads();
         // the bottom row's sets, numbered by first run: the new slots
         for (int64_t j = tid; j < nbot; j += nt) {
-            const uint32_t lb = ref.lbot[rb + j];
+            const uint32_t lb = S.bot_c[j];
             const uint32_t g = (lb & 0x80000000u) ? (uint32_t)E + (lb & 0xffffu) : A.Z[m + lb];
             A.bk[j] = g;
             atomicMin(&A.key[g], (uint32_t)j);
@@ -930,12 +1022,11 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
                 const uint32_t bal = __ballot_sync(0xffffffffu, first);
                 if (first) {
                     const uint32_t k = k0 + __popc(bal & lt);
-                    const uint32_t px = g < (uint32_t)E ? A.tot[g] : ref.lpx2[rb + (g - E)];
+                    const uint32_t px = g < (uint32_t)E ? A.tot[g] : S.px2[g - E];
                     A.s_Z[k] = px;
                     A.key[g] = REF_KTOP | k;
                     if (boundary)
-                        ref.binfo[rb + k] =
-                            (uint64_t)px | (uint64_t)i << 32 | (uint64_t)(uint8_t)(ref.tlist[rb + i] >> 56) << 48;
+                        ref.binfo[rb + k] = (uint64_t)px | (uint64_t)i << 32 | (uint64_t)(uint8_t)(S.bot_tl[i] >> 56) << 48;
                 }
                 k0 += __popc(bal);
             }
@@ -947,7 +1038,7 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
         __syncthreads();
         for (int64_t j = tid; j < nbot; j += nt) {
             const uint32_t slot = A.key[A.bk[j]] & 0xffffu;
-            const uint64_t te = ref.tlist[rb + j];
+            const uint64_t te = S.bot_tl[j];
             A.f_se[j] = (uint32_t)te;
             A.f_v[j] = (uint8_t)(te >> 48);
             A.f_slot[j] = (uint16_t)slot;
@@ -955,27 +1046,54 @@ __global__ void __launch_bounds__(256) k_ref_frontier(const FrameDesc *frames, R
         }
         m = s_m;
         nf = nbot;
+        d0 = d1;
+        d1 = d2;
         __syncthreads();
     }
+    cp_async_wait_all();
+}
+
+size_t ref_band_bytes(int64_t capr, bool staged) {
+    return ref_replay_bytes(capr) + (staged ? ref_align(8 * capr) : 0);
 }
 
 // The replay of one band, a warp each (the frame's bands taken in turn by
-// its blocks), the incoming sets' roots as symbols.
-__global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrder ref, int64_t capr,
-                                                 uint8_t *scratch, size_t scratch_per_block, uint32_t *err) {
+// its blocks), the incoming sets' roots as symbols. A launch takes the
+// bands whose rows hold more than `lo` and at most `hi` target runs (bwide)
+// and has arrays for capr; with `scratch` they live there (a region per
+// block) and rows are read in place, else each row's runs are staged while
+// the row above is replayed.
+__global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrder ref, int64_t capr, uint32_t lo,
+                                                 uint32_t hi, uint8_t *scratch, size_t scratch_per_block,
+                                                 uint32_t *err) {
     extern __shared__ __align__(16) uint8_t s_mem[];
     const int f = blockIdx.y;
     if (!ref.need[f]) return;
     const int lane = threadIdx.x;
     const FrameDesc fd = frames[f];
+    const bool staged = scratch == nullptr;
     ReplayArrays A;
-    ref_carve(scratch ? scratch + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * scratch_per_block : s_mem, capr, &A);
+    const size_t rbytes =
+        ref_carve(staged ? s_mem : scratch + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * scratch_per_block, capr, &A);
+    uint64_t *stg = reinterpret_cast<uint64_t *>(s_mem + rbytes);
     uint32_t *fin = ref.fin + (int64_t)f * AT_REF_MAXT, *finb = ref.finb + (int64_t)f * AT_REF_MAXT;
     const uint32_t vbase = (uint32_t)(fd.node_off + (int64_t)fd.qw * fd.qh);
-    const uint32_t *bs = ref.bstart + fd.row0 + f;
+    const uint4 *desc = ref.desc + fd.row0 + f;
+    const uint32_t *bw = ref.bwide + fd.row0 + f;
     const int64_t nb = ref.nband[f];
     for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
-        const int64_t y0 = bs[b], y1 = bs[b + 1];
+        const uint32_t wide = bw[b];
+        if (wide <= lo || wide > hi) continue;
+        const uint4 d = desc[b];
+        const int64_t y0 = d.x, y1 = d.y;
+        const int nr = (int)(y1 - y0);
+        // the band's row records (count | link << 31), lane r for row y0 + r
+        const uint32_t trl = lane < nr ? ref.trow[fd.row0 + y0 + lane] : 0u;
+        if (staged) {
+            const int64_t n = __shfl_sync(0xffffffffu, trl, 0) & 0x7fffffffu, rbase = fd.node_off + y0 * fd.qw;
+            for (int64_t j = lane; j < n; j += 32) cp_async8(stg + j, ref.tlist + rbase + j);
+            cp_async_commit();
+        }
         RowState S{0, 0};
         if (b > 0) {
             // the incoming sets: the row above with its slots, roots as symbols
@@ -998,20 +1116,47 @@ __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrd
             S.m = ma;
             S.np = na;
         }
-        __syncwarp();
         for (int64_t y = y0; y < y1; y++) {
-            bool link = false;
-            const int64_t n = load_row(A, ref, fd, y, &link);
+            const uint32_t tr = __shfl_sync(0xffffffffu, trl, (int)(y - y0));
+            const int64_t n = tr & 0x7fffffffu;
+            const bool link = (tr >> 31) != 0;
+            const int64_t rbase = fd.node_off + y * fd.qw;
+            const uint64_t *src = ref.tlist + rbase;
+            if (staged) {
+                cp_async_wait_all();
+                src = stg;
+            }
+            __syncwarp();
+            for (int64_t j = lane; j < n; j += 32) {
+                const uint64_t e = src[j];
+                A.c_se[j] = (uint32_t)e;
+                A.c_v[j] = (uint8_t)(e >> 48);
+                A.c_j[j] = (uint16_t)(e >> 32);
+                A.c_t[j] = (uint8_t)(e >> 56);
+            }
+            __syncwarp();
+            if (staged && y + 1 < y1) {
+                const uint32_t tn = __shfl_sync(0xffffffffu, trl, (int)(y + 1 - y0)) & 0x7fffffffu;
+                for (int64_t j = lane; j < tn; j += 32) cp_async8(stg + j, ref.tlist + rbase + fd.qw + j);
+                cp_async_commit();
+            }
             if (n == 0 && S.np == 0) continue;
-            if (!replay_row(A, S, n, link && n > 0, (uint32_t)(fd.node_off + y * fd.qw), vbase + (uint32_t)(y - 1), capr,
-                            fin, finb, (uint32_t)b, err))
+            if (!replay_row(A, S, n, link && n > 0, (uint32_t)rbase, vbase + (uint32_t)(y - 1), capr, fin, finb,
+                            (uint32_t)b, err)) {
+                cp_async_wait_all();
                 return;
+            }
         }
-        // the roots of the sets of the band's last row, for the band below;
-        // after the last band every open set is a whole component
+        // the roots of the sets at the band's last row, per slot of the
+        // boundary below (through the slot's first run); after the last
+        // band every open set is a whole component
         if (y1 < fd.qh) {
             const int64_t rb = fd.node_off + (y1 - 1) * fd.qw;
-            for (int64_t j = lane; j < S.np; j += 32) ref.outroot[rb + j] = A.s_R[A.p_slot[j]];
+            const int64_t mb = ref.bm[fd.row0 + y1 - 1];
+            for (int64_t k = lane; k < mb; k += 32) {
+                const uint32_t rep = (uint32_t)(ref.binfo[rb + k] >> 32) & 0xffffu;
+                ref.outroot[rb + k] = A.s_R[A.p_slot[rep]];
+            }
         } else {
             for (int64_t k = lane; k < S.m; k += 32) {
                 const uint32_t t = A.s_t[k];
@@ -1024,50 +1169,78 @@ __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrd
     }
 }
 
-// A warp per frame: the symbols replaced band by band from the top, each
-// target's root, then the reference's packed node numbers.
-__global__ void __launch_bounds__(32) k_ref_resolve(const FrameDesc *frames, RefOrder ref, int64_t capr) {
+// A block per frame: the symbols replaced band by band from the top (the
+// roots of a band's incoming slots are those of the slots' sets after the
+// band above), each target's root, then the reference's packed node
+// numbers. Each band is a barrier and a shared-memory step; the global
+// reads of 8 bands are issued together.
+#define REF_RES_CHUNK 8
+__global__ void __launch_bounds__(256) k_ref_resolve(const FrameDesc *frames, RefOrder ref, int64_t capr) {
     extern __shared__ __align__(16) uint32_t s_res[];  // two arrays of capr + 1
+    __shared__ int64_t s_rb[REF_RES_CHUNK];
+    __shared__ uint32_t s_mb[REF_RES_CHUNK];
     const int f = blockIdx.x;
     if (!ref.need[f]) return;
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, nth = blockDim.x;
     const FrameDesc fd = frames[f];
     const uint32_t nt = ref.nt[f];
-    const uint32_t *fin = ref.fin + (int64_t)f * AT_REF_MAXT, *finb = ref.finb + (int64_t)f * AT_REF_MAXT;
-    uint32_t *troot = ref.troot + (int64_t)f * AT_REF_MAXT;
-    uint32_t *cur = s_res, *nxt = s_res + capr + 1;
-    const uint32_t *bs = ref.bstart + fd.row0 + f;
-    const int64_t nb = ref.nband[f];
-    for (int64_t b = 0; b < nb; b++) {
-        for (uint32_t t = lane; t < nt; t += 32) {
-            if (finb[t] != (uint32_t)b) continue;
-            const uint32_t R = fin[t];
-            troot[t] = (R & REF_SYM) ? cur[R & ~REF_SYM] : R;
-        }
-        if (b + 1 < nb) {
-            const int64_t yb = bs[b + 1] - 1;
-            const int64_t rb = fd.node_off + yb * fd.qw;
-            const int64_t mb = ref.bm[fd.row0 + yb];
-            for (int64_t k = lane; k < mb; k += 32) {
-                const uint32_t rep = (uint32_t)(ref.binfo[rb + k] >> 32) & 0xffffu;
-                const uint32_t R = ref.outroot[rb + rep];
-                nxt[k] = (R & REF_SYM) ? cur[R & ~REF_SYM] : R;
-            }
-            __syncwarp();
-            uint32_t *t = cur;
-            cur = nxt;
-            nxt = t;
-        }
+    uint32_t my_fin = 0, my_finb = 0xffffffffu, my_root = 0xffffffffu;
+    if (tid < (int)nt) {
+        my_fin = ref.fin[(int64_t)f * AT_REF_MAXT + tid];
+        my_finb = ref.finb[(int64_t)f * AT_REF_MAXT + tid];
     }
-    __syncwarp();
+    uint32_t *cur = s_res, *nxt = s_res + capr + 1;
+    const uint4 *desc = ref.desc + fd.row0 + f;
+    const int64_t nb = ref.nband[f];
+    for (int64_t b0 = 0; b0 < nb; b0 += REF_RES_CHUNK) {
+        if (tid < REF_RES_CHUNK) {
+            const int64_t b = b0 + tid;
+            uint32_t mb = 0;
+            int64_t rb = 0;
+            if (b + 1 < nb) {
+                const int64_t yb = (int64_t)desc[b].y - 1;
+                rb = fd.node_off + yb * fd.qw;
+                mb = ref.bm[fd.row0 + yb];
+            }
+            s_rb[tid] = rb;
+            s_mb[tid] = mb;
+        }
+        __syncthreads();
+        uint32_t R[REF_RES_CHUNK];
+#pragma unroll
+        for (int i = 0; i < REF_RES_CHUNK; i++) R[i] = (uint32_t)tid < s_mb[i] ? ref.outroot[s_rb[i] + tid] : 0u;
+#pragma unroll
+        for (int i = 0; i < REF_RES_CHUNK; i++) {
+            const int64_t b = b0 + i;
+            if (b < nb) {
+                if (my_finb == (uint32_t)b) my_root = (my_fin & REF_SYM) ? cur[my_fin & ~REF_SYM] : my_fin;
+                if (b + 1 < nb) {
+                    const uint32_t mb = s_mb[i];
+                    if ((uint32_t)tid < mb) nxt[tid] = (R[i] & REF_SYM) ? cur[R[i] & ~REF_SYM] : R[i];
+                    for (uint32_t k = tid + nth; k < mb; k += nth) {
+                        const uint32_t Rk = ref.outroot[s_rb[i] + k];
+                        nxt[k] = (Rk & REF_SYM) ? cur[Rk & ~REF_SYM] : Rk;
+                    }
+                    __syncthreads();
+                    uint32_t *t = cur;
+                    cur = nxt;
+                    nxt = t;
+                }
+            }
+        }
+        __syncthreads();
+    }
     // GPU node ids -> the reference's packed node numbers (a target left
     // without a root keeps 0xffffffff, which the final stage reports)
-    const uint32_t *pre = ref.rpre + fd.row0 + f;
-    for (uint32_t t = lane; t < nt; t += 32) {
-        if (troot[t] == 0xffffffffu) continue;
-        const int64_t nd = (int64_t)troot[t] - fd.node_off;
-        const int64_t qpx = (int64_t)fd.qw * fd.qh;
-        troot[t] = nd < qpx ? pre[nd / fd.qw] + (uint32_t)(nd % fd.qw) : pre[fd.qh] + (uint32_t)(nd - qpx);
+    if (tid < (int)nt) {
+        uint32_t r = my_root;
+        if (r != 0xffffffffu) {
+            const uint32_t *pre = ref.rpre + fd.row0 + f;
+            const int64_t nd = (int64_t)r - fd.node_off;
+            const int64_t qpx = (int64_t)fd.qw * fd.qh;
+            r = nd < qpx ? pre[nd / fd.qw] + (uint32_t)(nd % fd.qw) : pre[fd.qh] + (uint32_t)(nd - qpx);
+        }
+        ref.troot[(int64_t)f * AT_REF_MAXT + tid] = r;
     }
 }
 
@@ -1076,23 +1249,32 @@ __global__ void __launch_bounds__(32) k_ref_resolve(const FrameDesc *frames, Ref
 
 void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                       const uint32_t *row_nruns, int nfam, const int64_t *qstart, const GpuDetection *dets,
-                      const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb, int64_t capr,
-                      uint8_t *scratch, size_t scratch_per_block, const RefOrder &ref, uint32_t *err) {
+                      const uint32_t *det_ok, const uint32_t *qcl, const uint64_t *ckey, int nb,
+                      const RefPlan &P, const RefOrder &ref, uint32_t *err) {
     k_ref_targets<<<L.nframes, 256, 0, L.stream>>>(frames, nfam, qstart, dets, det_ok, qcl, ckey, nb, runs, row_nruns,
                                                    ref, err);
     const int64_t b = (L.max_qh + 7) / 8;
     const dim3 grid((unsigned)(b < 1 ? 1 : b < 148 ? b : 148), (unsigned)L.nframes);
     k_ref_mark<<<grid, 256, 0, L.stream>>>(frames, thr, runs, row_nruns, ref);
-    k_ref_cut<<<L.nframes, 32, 0, L.stream>>>(frames, ref);
+    k_ref_cut<<<L.nframes, 32, 0, L.stream>>>(frames, ref, (uint32_t)P.pcap);
     const int64_t gb = (L.max_qh + REF_BAND - 1) / REF_BAND;
     const unsigned bands = (unsigned)(gb < 1 ? 1 : gb);
-    k_ref_local<<<dim3(bands, (unsigned)L.nframes), 256, ref_local_bytes(), L.stream>>>(frames, ref, err);
-    k_ref_frontier<<<L.nframes, 256, ref_frontier_bytes(capr), L.stream>>>(frames, ref, capr);
-    const size_t smem = scratch ? 0 : ref_replay_bytes(capr);
-    k_ref_band<<<dim3(scratch ? REF_BAND_BLOCKS : bands, (unsigned)L.nframes), 32, smem, L.stream>>>(
-        frames, ref, capr, scratch, scratch_per_block, err);
-    k_ref_resolve<<<L.nframes, 32, 8 * (capr + 1), L.stream>>>(frames, ref, capr);
+    k_ref_local<<<dim3(bands, (unsigned)L.nframes), 256, ref_local_bytes(P.pcap), L.stream>>>(frames, ref,
+                                                                                            (uint32_t)P.pcap, err);
+    k_ref_frontier<<<L.nframes, 128, P.front_scratch ? 0 : ref_frontier_bytes(P.capr, true), L.stream>>>(
+        frames, ref, P.capr, P.front_scratch, P.front_bytes);
+    // bands of narrow rows, many blocks per SM; then the others
+    const int64_t small = P.capr < REF_SMALLR ? P.capr : REF_SMALLR;
+    k_ref_band<<<dim3(bands, (unsigned)L.nframes), 32, ref_band_bytes(small, true), L.stream>>>(
+        frames, ref, small, 0u, (uint32_t)small, nullptr, 0, err);
+    if (P.capr > REF_SMALLR)
+        k_ref_band<<<dim3(P.band_scratch ? REF_BAND_BLOCKS : bands, (unsigned)L.nframes), 32,
+                     P.band_scratch ? 0 : ref_band_bytes(P.capr, true), L.stream>>>(
+            frames, ref, P.capr, (uint32_t)REF_SMALLR, 0xffffffffu, P.band_scratch, P.band_bytes, err);
+    k_ref_resolve<<<L.nframes, 256, 8 * (P.capr + 1), L.stream>>>(frames, ref, P.capr);
 }
+
+int ref_order_launches(const RefPlan &P) { return P.capr > REF_SMALLR ? 8 : 7; }
 
 bool ref_replay_set_smem(size_t bytes) {
     return cudaFuncSetAttribute(k_ref_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess &&
