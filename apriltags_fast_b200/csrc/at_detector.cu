@@ -97,7 +97,7 @@ enum {
     B_SMXE, B_SMXI, B_QUADS, B_QOK, B_QSCAN, B_QUADSC, B_DETS, B_DETOK, B_OUT, B_QSTART, B_OUTOFF, B_OUTN, B_DIDX, B_DRM, B_MINID, B_FLIST, B_FCNT, B_QCORN, B_QH, B_QHOK, B_QNUM, B_FIRST, B_HKEYS, B_HCOUNT, B_HRANK, B_HOKEYS, B_HOSLOTS, B_HSKEYS, B_HSSLOTS, B_HCCOUNT, B_HMISC,
     B_HYMIN, B_HYMAX, B_CSPAN, B_CY0, B_SPANOFF, B_PKFRAME, B_PGKEYS, B_PGSLOTS, B_PFRAMES, B_PBSUM, B_SEG,
     B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
-    B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RBWIDE, B_RDESC, B_RNBAND, B_RFSCR, B_RLTOP, B_RLPX, B_RLBOT,
+    B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RBWIDE, B_RDESC, B_RNBAND, B_RFSCR, B_RTCH, B_RLTOP, B_RLPX, B_RLBOT,
     B_RLPX2,
     B_CUB, B_ERR, B_NBUF
 };
@@ -677,6 +677,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_RBWIDE].ensure((rows + n) * 4));
         CK(B[B_RDESC].ensure((rows + n) * 16));
         CK(B[B_RNBAND].ensure(n * 4));
+        CK(B[B_RTCH].ensure(nodes * 4));
         CK(B[B_RLTOP].ensure(nodes * 4));
         CK(B[B_RLPX].ensure(nodes * 4));
         CK(B[B_RLBOT].ensure(nodes * 4));
@@ -687,7 +688,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                           B[B_RTPX].as<uint32_t>(),    B[B_RTROOT].as<uint32_t>(),  B[B_RTLIST].as<uint64_t>(),
                           B[B_RTROW].as<uint32_t>(),   B[B_RPRE].as<uint32_t>(),    B[B_RFIN].as<uint32_t>(),
                           B[B_RFINB].as<uint32_t>(),   B[B_RBSTART].as<uint32_t>(), B[B_RBWIDE].as<uint32_t>(),
-                          B[B_RDESC].as<uint4>(),      B[B_RNBAND].as<uint32_t>(),  B[B_RLTOP].as<uint32_t>(),
+                          B[B_RDESC].as<uint4>(),      B[B_RNBAND].as<uint32_t>(),  B[B_RTCH].as<uint32_t>(),
+                          B[B_RLTOP].as<uint32_t>(),
                           B[B_RLPX].as<uint32_t>(),
                           B[B_RLBOT].as<uint32_t>(),   B[B_RLPX2].as<uint32_t>(),   B[B_RBSLOT].as<uint16_t>(),
                           B[B_RBINFO].as<uint64_t>(),  B[B_ROUTROOT].as<uint32_t>(), B[B_RBM].as<uint32_t>()};

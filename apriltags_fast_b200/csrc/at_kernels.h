@@ -137,6 +137,7 @@ struct RefOrder {
     uint4 *desc;
     uint32_t *nband;
     // per node (at the rows of the band edges, at_order.cu):
+    uint32_t *tch;            //   each target run: the target runs above it touches (first | last << 16)
     uint32_t *ltop, *lpx;     //   top row: each run's band component, their pixels
     uint32_t *lbot, *lpx2;    //   bottom row: each run's band component, the others' pixels
     uint16_t *bslot;          //   row above a band: each target run's slot

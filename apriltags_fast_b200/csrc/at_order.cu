@@ -221,13 +221,23 @@ struct ReplayArrays {
     uint8_t *p_v;
     uint16_t *p_slot;
     uint32_t *c_se;   // this row's target runs
+    uint32_t *c_tch;  //   the range of runs above each touches (first | last << 16; 0xffff: none)
     uint8_t *c_v, *c_t;
     uint16_t *c_j;
-    uint16_t *call_a, *call_b;  // the calls in the reference's order: (run element, slot element)
-    uint16_t *e_par, *e_fpar;   // elements: slots [0, m), runs [m, m + n), the last-column node m + n
-    uint32_t *e_R, *e_Z, *e_tot, *e_c0, *e_c1;
-    unsigned long long *e_max;
+    uint16_t *r_slot; //   the first slot each touches (0xffff: none)
+    uint16_t *r_key;  //   its group key: the group's root slot, or m + i when it touches none
+    // per slot (m): the union-find of the row's groups, each slot's group,
+    // whether a run touches it; per group root: its slots' pixels, its
+    // runs' pixels, its largest slot (pixels << 16 | slot)
+    uint16_t *e_par, *e_grp;
     uint8_t *e_flag;
+    uint32_t *e_c1, *e_tot;
+    unsigned long long *e_max;
+    // per element (slots [0, m), runs m + i): the call-by-call replay's
+    // union-find, roots and pixels; per group key: its first run, and its
+    // root and pixels after the row
+    uint16_t *e_fpar;
+    uint32_t *e_R, *e_Z, *e_c0, *f_R, *f_Z;
     uint32_t *s_R, *s_Z;        // slots carried to the next row
     uint8_t *s_t;
 };
@@ -236,7 +246,7 @@ __host__ __device__ inline size_t ref_align(size_t x) { return (x + 15) & ~(size
 
 // Carves the arrays out of `base`; returns the bytes used.
 __host__ __device__ inline size_t ref_carve(uint8_t *base, int64_t capr, ReplayArrays *A) {
-    const int64_t cape = 2 * capr + 2, capc = 2 * capr + 2;
+    const int64_t cape = 2 * capr + 2, caps = capr + 1;
     size_t at = 0;
     auto take = [&](size_t bytes) {
         uint8_t *p = base + at;
@@ -246,25 +256,29 @@ __host__ __device__ inline size_t ref_carve(uint8_t *base, int64_t capr, ReplayA
     ReplayArrays a;
     a.p_se = (uint32_t *)take(4 * capr);
     a.c_se = (uint32_t *)take(4 * capr);
+    a.c_tch = (uint32_t *)take(4 * capr);
     a.e_R = (uint32_t *)take(4 * cape);
     a.e_Z = (uint32_t *)take(4 * cape);
-    a.e_tot = (uint32_t *)take(4 * cape);
     a.e_c0 = (uint32_t *)take(4 * cape);
-    a.e_c1 = (uint32_t *)take(4 * cape);
-    a.e_max = (unsigned long long *)take(8 * cape);
-    a.s_R = (uint32_t *)take(4 * (capr + 1));
-    a.s_Z = (uint32_t *)take(4 * (capr + 1));
+    a.f_R = (uint32_t *)take(4 * cape);
+    a.f_Z = (uint32_t *)take(4 * cape);
+    a.e_tot = (uint32_t *)take(4 * caps);
+    a.e_c1 = (uint32_t *)take(4 * caps);
+    a.e_max = (unsigned long long *)take(8 * caps);
+    a.s_R = (uint32_t *)take(4 * caps);
+    a.s_Z = (uint32_t *)take(4 * caps);
     a.p_slot = (uint16_t *)take(2 * capr);
     a.c_j = (uint16_t *)take(2 * capr);
-    a.call_a = (uint16_t *)take(2 * capc);
-    a.call_b = (uint16_t *)take(2 * capc);
-    a.e_par = (uint16_t *)take(2 * cape);
+    a.r_slot = (uint16_t *)take(2 * capr);
+    a.r_key = (uint16_t *)take(2 * capr);
+    a.e_par = (uint16_t *)take(2 * caps);
+    a.e_grp = (uint16_t *)take(2 * caps);
     a.e_fpar = (uint16_t *)take(2 * cape);
     a.p_v = take(capr);
     a.c_v = take(capr);
     a.c_t = take(capr);
-    a.e_flag = take(cape);
-    a.s_t = take(capr + 1);
+    a.e_flag = take(caps);
+    a.s_t = take(caps);
     if (A) *A = a;
     return at;
 }
@@ -314,200 +328,195 @@ __device__ __forceinline__ uint32_t fold_find(const uint16_t *par, uint32_t x) {
 // band's incoming slot j" (known only once the bands above are resolved).
 #define REF_SYM 0x80000000u
 
-// One row of the reference's unions over the open target runs, for a warp:
-// the row's runs (c_*, n) against the previous row's (p_*, np, with their
-// slots s_*, m); afterwards the slots and previous runs describe this row.
-// Slots that no call reaches are whole components: fin[t] gets their root.
-// Returns false when the call arrays are too small (err set).
+// The state between rows of a band's replay: m slots (the sets of target
+// runs that touch the previous row: s_R, s_Z, s_t) and the previous row's
+// np target runs (p_*, each with its slot).
 struct RowState {
-    int64_t m, np;
+    int m, np;
 };
 
-__device__ __forceinline__ bool replay_row(ReplayArrays &A, RowState &S, int64_t n, bool link, uint32_t rbase, uint32_t vnode,
-                           int64_t capr, uint32_t *fin, uint32_t *finb, uint32_t band, uint32_t *err) {
+// Adds `val` to arr[key] for the active lanes, one atomic per distinct key
+// in the warp. Every lane of the warp calls it.
+__device__ __forceinline__ void warp_add_by_key(uint32_t *arr, uint32_t key, uint32_t val, bool active) {
+    const uint32_t am = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const uint32_t peers = __match_any_sync(am, key);
+    const uint32_t sum = __reduce_add_sync(peers, val);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
+}
+
+__device__ __forceinline__ uint32_t run_len(uint32_t se) { return (se >> 16) - (se & 0xffffu) + 1; }
+
+// A row of the reference's calls (fast/unionfind.c:112-196): each run of
+// the row in order, with each run above it touches, in order; then the
+// last-column link. A run joins the sets (slots) of the runs it touches, so
+// the row's groups are the slots joined through runs that touch several
+// slots, each with the runs that touch it, and the runs that touch none
+// (each alone). A group in which one slot holds more pixels than all its
+// other slots and runs together keeps that slot's root, whatever the order
+// (that slot is the b side of each call it meets and wins: the a side
+// needs strictly more). Any other group is replayed call by call by one
+// lane. The link then joins one pixel to the last run's set, taking the
+// root only from a set of one pixel.
+__device__ __forceinline__ void replay_row(ReplayArrays &A, RowState &S, int n, bool link, uint32_t rbase,
+                                           uint32_t vnode, uint32_t *fin, uint32_t *finb, uint32_t band) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    const int64_t m = S.m, np = S.np;
-    const int64_t E = m + n + 1, vn = m + n;
-    __syncwarp();
-    for (int64_t e = lane; e < E; e += 32) {
-        A.e_par[e] = (uint16_t)e;
-        A.e_fpar[e] = (uint16_t)e;
-        A.e_max[e] = 0;
-        A.e_c0[e] = 0xffffffffu;
-        A.e_c1[e] = 0;
-        if (e < m) {
-            A.e_R[e] = A.s_R[e];
-            A.e_Z[e] = A.s_Z[e];
-            A.e_flag[e] = 0;
-        } else if (e < vn) {
-            const uint32_t se = A.c_se[e - m];
-            A.e_R[e] = rbase + A.c_j[e - m];
-            A.e_Z[e] = (se >> 16) - (se & 0xffffu) + 1;
-            A.e_flag[e] = REF_TOUCHED;
-        } else {
-            A.e_R[e] = vnode;
-            A.e_Z[e] = 1;
-            A.e_flag[e] = link ? REF_TOUCHED : 0;
-        }
+    const int m = S.m;
+    // slots: their own set (union-find over slots), roots and sizes for
+    // the call-by-call replays, sums per group
+    for (int s = lane; s < m; s += 32) {
+        A.e_par[s] = (uint16_t)s;
+        A.e_fpar[s] = (uint16_t)s;
+        A.e_R[s] = A.s_R[s];
+        A.e_Z[s] = A.s_Z[s];
+        A.e_flag[s] = 0;
+        A.e_tot[s] = 0;
+        A.e_c1[s] = 0;
+        A.e_max[s] = 0;
     }
-    // the calls, in the reference's order: each run, its touching runs
-    // above in order (fast/unionfind.c:112-196), then the last column
-    int64_t nc = 0;
-    if (np > 0) {
-        for (int64_t i0 = 0; i0 < n; i0 += 32) {
-            const int64_t i = i0 + lane;
-            int64_t k0 = 0, cnt = 0;
-            int64_t a0 = 0, a1 = 0;
-            uint8_t v = 0;
-            if (i < n) {
-                a0 = A.c_se[i] & 0xffffu;
-                a1 = A.c_se[i] >> 16;
-                v = A.c_v[i];
-                int64_t lo = 0, hi = np;
-                while (lo < hi) {
-                    const int64_t mid = (lo + hi) >> 1;
-                    if ((int64_t)(A.p_se[mid] >> 16) + 1 < a0)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
+    for (int e = lane; e < m + n; e += 32) A.e_c0[e] = 0xffffffffu;
+    __syncwarp();
+    // each run: the first slot it touches (r_slot, 0xffff: none); the
+    // slots a run touches are joined
+    for (int i = lane; i < n; i += 32) {
+        uint32_t s1 = 0xffffu;
+        const uint32_t tc = A.c_tch[i];
+        const uint8_t v = A.c_v[i];
+        if ((tc & 0xffffu) != 0xffffu)
+            for (uint32_t k = tc & 0xffffu; k <= (tc >> 16); k++)
+                if (A.p_v[k] == v) {
+                    const uint32_t s = A.p_slot[k];
+                    A.e_flag[s] = REF_TOUCHED;
+                    if (s1 == 0xffffu)
+                        s1 = s;
+                    else if (s != s1)
+                        el_unite(A.e_par, s1, s);
                 }
-                k0 = lo;
-                for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
-                    if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) cnt++;
-            }
-            uint32_t total;
-            const uint32_t off = warp_excl_scan((uint32_t)cnt, &total);
-            if (nc + total + 1 > 2 * capr + 2) {  // more calls than the arrays hold
-                if (lane == 0) atomicOr(err, AT_ERR_ORDER);
-                return false;
-            }
-            int64_t o = nc + off;
-            if (i < n)
-                for (int64_t k = k0; k < np && (int64_t)(A.p_se[k] & 0xffffu) <= a1 + 1; k++)
-                    if (A.p_v[k] == v && runs_touch(a0, a1, A.p_se[k] & 0xffffu, A.p_se[k] >> 16, v)) {
-                        A.call_a[o] = (uint16_t)(m + i);
-                        A.call_b[o] = A.p_slot[k];
-                        o++;
-                    }
-            nc += total;
-        }
-    }
-    if (link) {
-        if (lane == 0) {
-            A.call_a[nc] = (uint16_t)(vn - 1);
-            A.call_b[nc] = (uint16_t)vn;
-        }
-        nc++;
+        A.r_slot[i] = (uint16_t)s1;
     }
     __syncwarp();
-    // groups
-    for (int64_t c = lane; c < nc; c += 32) {
-        el_unite(A.e_par, A.call_a[c], A.call_b[c]);
-        A.e_flag[A.call_b[c]] = REF_TOUCHED;
-    }
-    __syncwarp();
-    // every element's group root (read-only walks into e_tot, then copied:
-    // a halving write racing a final write could leave a non-root parent)
-    for (int64_t e = lane; e < E; e += 32) {
-        uint32_t x = (uint32_t)e;
+    // each slot's group (its root slot)
+    for (int s = lane; s < m; s += 32) {
+        uint32_t x = (uint32_t)s;
         while (A.e_par[x] != x) x = A.e_par[x];
-        A.e_tot[e] = x;
+        A.e_grp[s] = (uint16_t)x;
     }
     __syncwarp();
-    for (int64_t e = lane; e < E; e += 32) {
-        A.e_par[e] = (uint16_t)A.e_tot[e];
-        A.e_tot[e] = 0;
+    // per group: the pixels of its slots and of its runs, its largest slot;
+    // per key (group root slot g, or m + i for a run that touches none,
+    // r_key[i] for run i): its first run
+    for (int s = lane; s < m; s += 32)
+        if (A.e_flag[s]) {
+            const uint32_t g = A.e_grp[s];
+            atomicAdd(&A.e_c1[g], A.s_Z[s]);
+            atomicMax(&A.e_max[g], (unsigned long long)A.s_Z[s] << 16 | (uint64_t)s);
+        }
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        uint32_t key = 0, z = 0;
+        bool touched = false;
+        if (i < n) {
+            const uint32_t s = A.r_slot[i];
+            touched = s != 0xffffu;
+            key = touched ? A.e_grp[s] : (uint32_t)(m + i);
+            z = run_len(A.c_se[i]);
+            A.r_key[i] = (uint16_t)key;
+            atomicMin(&A.e_c0[key], (uint32_t)i);
+        }
+        warp_add_by_key(A.e_tot, key, z, touched);
     }
     __syncwarp();
-    // per group: pixels, the largest set that existed before the row, and
-    // the range of its calls
-    for (int64_t e = lane; e < E; e += 32) {
-        if (!A.e_flag[e]) continue;
-        const uint32_t g = A.e_par[e];
-        atomicAdd(&A.e_tot[g], A.e_Z[e]);
-        if (e < m || e == vn) atomicMax(&A.e_max[g], (unsigned long long)A.e_Z[e] << 16 | (uint64_t)e);
-    }
-    for (int64_t c = lane; c < nc; c += 32) {
-        const uint32_t g = A.e_par[A.call_a[c]];
-        atomicMin(&A.e_c0[g], (uint32_t)c);
-        atomicMax(&A.e_c1[g], (uint32_t)c);
-    }
-    __syncwarp();
-    // each group's root and pixels, into its root element
-    for (int64_t g = lane; g < E; g += 32) {
-        if (!A.e_flag[g] || A.e_par[g] != g) continue;
+    // each group's root and pixels after the row (f_R, f_Z at its key)
+    for (int g = lane; g < m; g += 32) {
+        if (!A.e_flag[g] || A.e_grp[g] != g) continue;
         const unsigned long long mx = A.e_max[g];
-        const uint32_t zmax = (uint32_t)(mx >> 16), tot = A.e_tot[g];
-        if (mx != 0 && zmax > tot - zmax) {
-            A.e_R[g] = A.e_R[mx & 0xffffu];
-            A.e_Z[g] = tot;
-            continue;
-        }
-        // no set outweighs the rest: the reference's calls one by one
-        for (uint32_t c = A.e_c0[g]; c <= A.e_c1[g] && c < (uint32_t)nc; c++) {
-            const uint32_t a = A.call_a[c];
-            if (A.e_par[a] != g) continue;
-            const uint32_t ra = fold_find(A.e_fpar, a), rb = fold_find(A.e_fpar, A.call_b[c]);
-            if (ra == rb) continue;
-            const uint32_t za = A.e_Z[ra], zb = A.e_Z[rb];
-            if (za > zb) {
-                A.e_fpar[rb] = (uint16_t)ra;
-                A.e_Z[ra] = za + zb;
-            } else {
-                A.e_fpar[ra] = (uint16_t)rb;
-                A.e_Z[rb] = za + zb;
+        const uint32_t zmax = (uint32_t)(mx >> 16), tot = A.e_c1[g] + A.e_tot[g];
+        uint32_t R, Z;
+        if (zmax > tot - zmax) {
+            R = A.s_R[mx & 0xffffu];
+            Z = tot;
+        } else {  // the group's calls one by one
+            for (int i = (int)A.e_c0[g]; i < n; i++) {
+                if (A.r_key[i] != g) continue;
+                const uint32_t a = (uint32_t)(m + i);
+                A.e_fpar[a] = (uint16_t)a;
+                A.e_Z[a] = run_len(A.c_se[i]);
+                A.e_R[a] = rbase + A.c_j[i];
+                const uint32_t tc = A.c_tch[i];
+                const uint8_t v = A.c_v[i];
+                for (uint32_t k = tc & 0xffffu; k <= (tc >> 16); k++) {
+                    if (A.p_v[k] != v) continue;
+                    const uint32_t ra = fold_find(A.e_fpar, a), rb = fold_find(A.e_fpar, A.p_slot[k]);
+                    if (ra == rb) continue;
+                    const uint32_t za = A.e_Z[ra], zb = A.e_Z[rb];
+                    if (za > zb) {
+                        A.e_fpar[rb] = (uint16_t)ra;
+                        A.e_Z[ra] = za + zb;
+                    } else {
+                        A.e_fpar[ra] = (uint16_t)rb;
+                        A.e_Z[rb] = za + zb;
+                    }
+                }
             }
+            const uint32_t r = fold_find(A.e_fpar, (uint32_t)g);
+            R = A.e_R[r];
+            Z = A.e_Z[r];
         }
-        const uint32_t r = fold_find(A.e_fpar, (uint32_t)g);
-        const uint32_t R = A.e_R[r], Z = A.e_Z[r];
-        A.e_R[g] = R;
-        A.e_Z[g] = Z;
+        A.f_R[g] = R;
+        A.f_Z[g] = Z;
     }
-    __syncwarp();
-    // a slot no call reached is a whole component: its root is final
-    for (int64_t e = lane; e < m; e += 32) {
-        const uint32_t t = A.s_t[e];
-        if (A.e_flag[e] || t == REF_NONE) continue;
-        fin[t] = A.s_R[e];
+    // a slot no run touches is a whole component: its root is final
+    for (int s = lane; s < m; s += 32) {
+        const uint32_t t = A.s_t[s];
+        if (A.e_flag[s] || t == REF_NONE) continue;
+        fin[t] = A.s_R[s];
         finb[t] = band;
     }
-    // the new slots: one per group of this row's runs, numbered by its
-    // first run (e_tot of the root is free again and holds that run)
-    for (int64_t i = lane; i < n; i += 32) A.e_tot[A.e_par[m + i]] = 0xffffffffu;
+    for (int i = lane; i < n; i += 32)
+        if (A.r_slot[i] == 0xffffu) {
+            A.f_R[m + i] = rbase + A.c_j[i];
+            A.f_Z[m + i] = run_len(A.c_se[i]);
+        }
     __syncwarp();
-    for (int64_t i = lane; i < n; i += 32) atomicMin(&A.e_tot[A.e_par[m + i]], (uint32_t)i);
+    // the last-column link
+    if (link && lane == 0) {
+        const uint32_t key = A.r_key[n - 1];
+        const uint32_t Z = A.f_Z[key];
+        if (Z <= 1) A.f_R[key] = vnode;
+        A.f_Z[key] = Z + 1;
+    }
     __syncwarp();
-    int64_t mnew = 0;
-    for (int64_t i0 = 0; i0 < n; i0 += 32) {
-        const int64_t i = i0 + lane;
-        uint32_t g = 0;
+    // the new slots, numbered by first run
+    int mnew = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        uint32_t key = 0;
         bool first = false;
         if (i < n) {
-            g = A.e_par[m + i];
-            first = A.e_tot[g] == (uint32_t)i;
+            key = A.r_key[i];
+            first = A.e_c0[key] == (uint32_t)i;
         }
         const uint32_t bal = __ballot_sync(0xffffffffu, first);
         if (first) {
-            const int64_t k = mnew + __popc(bal & lt);
-            A.e_c0[g] = (uint32_t)k;  // the group's new slot
-            A.s_R[k] = A.e_R[g];
-            A.s_Z[k] = A.e_Z[g];
+            const int k = mnew + __popc(bal & lt);
+            A.s_R[k] = A.f_R[key];
+            A.s_Z[k] = A.f_Z[key];
             A.s_t[k] = A.c_t[i];
+            A.e_c0[key] = 0x80000000u | (uint32_t)k;
         }
         mnew += __popc(bal);
     }
     __syncwarp();
     // this row's runs, with their slots, for the next row
-    for (int64_t i = lane; i < n; i += 32) {
+    for (int i = lane; i < n; i += 32) {
         A.p_se[i] = A.c_se[i];
         A.p_v[i] = A.c_v[i];
-        A.p_slot[i] = (uint16_t)A.e_c0[A.e_par[m + i]];
+        A.p_slot[i] = (uint16_t)(A.e_c0[A.r_key[i]] & 0xffffu);
     }
     S.m = mnew;
     S.np = n;
     __syncwarp();
-    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -545,16 +554,6 @@ __device__ __forceinline__ bool replay_row(ReplayArrays &A, RowState &S, int64_t
 #define REF_KNONE 0x3fffffffu  // no run yet: above every run index, below the flags
 #define REF_KTOP 0x80000000u   // numbered: the component's index
 #define REF_KBOT 0x40000000u
-
-// Adds `val` to arr[key] for the active lanes, one atomic per distinct key
-// in the warp. Every lane of the warp calls it.
-__device__ __forceinline__ void warp_add_by_key(uint32_t *arr, uint32_t key, uint32_t val, bool active) {
-    const uint32_t am = __ballot_sync(0xffffffffu, active);
-    if (!active) return;
-    const uint32_t peers = __match_any_sync(am, key);
-    const uint32_t sum = __reduce_add_sync(peers, val);
-    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&arr[key], sum);
-}
 
 __device__ __forceinline__ uint32_t pu_find(volatile uint32_t *par, uint32_t x) {
     uint32_t p = par[x];
@@ -762,10 +761,16 @@ __global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefO
             if (r == 0) continue;
             const int64_t a0 = A.se[l] & 0xffffu, a1 = A.se[l] >> 16;
             const uint8_t v = A.v[l];
-            const uint32_t hi = s_roff[r];
-            for (uint32_t k = first_reaching(A.se, s_roff[r - 1], hi, a0); k < hi && (int64_t)(A.se[k] & 0xffffu) <= a1 + 1;
-                 k++)
-                if (A.v[k] == v && runs_touch(a0, a1, A.se[k] & 0xffffu, A.se[k] >> 16, v)) pu_unite(A.par, l, k);
+            const uint32_t lo = s_roff[r - 1], hi = s_roff[r];
+            uint32_t klo = 0xffffu, khi = 0;
+            for (uint32_t k = first_reaching(A.se, lo, hi, a0); k < hi && (int64_t)(A.se[k] & 0xffffu) <= a1 + 1; k++)
+                if (A.v[k] == v && runs_touch(a0, a1, A.se[k] & 0xffffu, A.se[k] >> 16, v)) {
+                    pu_unite(A.par, l, k);
+                    if (klo == 0xffffu) klo = k - lo;
+                    khi = k - lo;
+                }
+            // the runs above that this run touches, for the replay
+            ref.tch[fd.node_off + (y0 + r) * fd.qw + (l - s_roff[r])] = klo == 0xffffu ? 0xffffffffu : klo | khi << 16;
         }
         for (int r = tid; r < nr; r += nt)
             if (s_link[r] && s_roff[r + 1] > s_roff[r]) pu_unite(A.par, s_roff[r + 1] - 1, L + r);
@@ -975,18 +980,25 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
         }
         for (int64_t e = tid; e < E + nnon; e += nt) A.key[e] = REF_KNONE;
         __syncthreads();
-        if (nf > 0)
-            for (int64_t j = tid; j < n0; j += nt) {
-                const uint64_t te = S.top_tl[j];
-                const uint32_t se = (uint32_t)te;
-                const uint8_t v = (uint8_t)(te >> 48);
-                const int64_t a0 = se & 0xffffu, a1 = se >> 16;
-                const uint32_t c = S.top_c[j];
+        const int64_t rt = fd.node_off + (int64_t)d0.x * fd.qw;
+        for (int64_t j = tid; j < n0; j += nt) {
+            const uint64_t te = S.top_tl[j];
+            const uint32_t se = (uint32_t)te;
+            const uint8_t v = (uint8_t)(te >> 48);
+            const int64_t a0 = se & 0xffffu, a1 = se >> 16;
+            const uint32_t c = S.top_c[j];
+            uint32_t klo = 0xffffu, khi = 0;
+            if (nf > 0)
                 for (uint32_t k = first_reaching(A.f_se, 0, (uint32_t)nf, a0);
                      k < nf && (int64_t)(A.f_se[k] & 0xffffu) <= a1 + 1; k++)
-                    if (A.f_v[k] == v && runs_touch(a0, a1, A.f_se[k] & 0xffffu, A.f_se[k] >> 16, v))
+                    if (A.f_v[k] == v && runs_touch(a0, a1, A.f_se[k] & 0xffffu, A.f_se[k] >> 16, v)) {
                         pu_unite(A.par, A.f_slot[k], (uint32_t)(m + c));
-            }
+                        if (klo == 0xffffu) klo = k;
+                        khi = k;
+                    }
+            // the runs above that this run touches, for the replay
+            ref.tch[rt + j] = klo == 0xffffu ? 0xffffffffu : klo | khi << 16;
+        }
         __syncthreads();
         for (int64_t e0 = 0; e0 < E; e0 += nt) {
             const int64_t e = e0 + tid;
@@ -1009,10 +1021,10 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
             atomicMin(&A.key[g], (uint32_t)j);
         }
         __syncthreads();
-        if (tid < 32) {
+        if (tid < 32) {  // one warp numbers them in run order
             uint32_t k0 = 0;
             for (int64_t i0 = 0; i0 < nbot; i0 += 32) {
-                const int64_t i = i0 + tid;
+                const int64_t i = i0 + lane;
                 uint32_t g = 0;
                 bool first = false;
                 if (i < nbot) {
@@ -1026,11 +1038,12 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
                     A.s_Z[k] = px;
                     A.key[g] = REF_KTOP | k;
                     if (boundary)
-                        ref.binfo[rb + k] = (uint64_t)px | (uint64_t)i << 32 | (uint64_t)(uint8_t)(S.bot_tl[i] >> 56) << 48;
+                        ref.binfo[rb + k] =
+                            (uint64_t)px | (uint64_t)i << 32 | (uint64_t)(uint8_t)(S.bot_tl[i] >> 56) << 48;
                 }
                 k0 += __popc(bal);
             }
-            if (tid == 0) {
+            if (lane == 0) {
                 s_m = k0;
                 if (boundary) ref.bm[fd.row0 + y1 - 1] = k0;
             }
@@ -1054,7 +1067,7 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
 }
 
 size_t ref_band_bytes(int64_t capr, bool staged) {
-    return ref_replay_bytes(capr) + (staged ? ref_align(8 * capr) : 0);
+    return ref_replay_bytes(capr) + (staged ? ref_align(8 * capr) + ref_align(4 * capr) : 0);
 }
 
 // The replay of one band, a warp each (the frame's bands taken in turn by
@@ -1064,8 +1077,7 @@ size_t ref_band_bytes(int64_t capr, bool staged) {
 // block) and rows are read in place, else each row's runs are staged while
 // the row above is replayed.
 __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrder ref, int64_t capr, uint32_t lo,
-                                                 uint32_t hi, uint8_t *scratch, size_t scratch_per_block,
-                                                 uint32_t *err) {
+                                                 uint32_t hi, uint8_t *scratch, size_t scratch_per_block) {
     extern __shared__ __align__(16) uint8_t s_mem[];
     const int f = blockIdx.y;
     if (!ref.need[f]) return;
@@ -1076,6 +1088,7 @@ __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrd
     const size_t rbytes =
         ref_carve(staged ? s_mem : scratch + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * scratch_per_block, capr, &A);
     uint64_t *stg = reinterpret_cast<uint64_t *>(s_mem + rbytes);
+    uint32_t *stg_t = reinterpret_cast<uint32_t *>(s_mem + rbytes + ref_align(8 * capr));
     uint32_t *fin = ref.fin + (int64_t)f * AT_REF_MAXT, *finb = ref.finb + (int64_t)f * AT_REF_MAXT;
     const uint32_t vbase = (uint32_t)(fd.node_off + (int64_t)fd.qw * fd.qh);
     const uint4 *desc = ref.desc + fd.row0 + f;
@@ -1091,7 +1104,10 @@ __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrd
         const uint32_t trl = lane < nr ? ref.trow[fd.row0 + y0 + lane] : 0u;
         if (staged) {
             const int64_t n = __shfl_sync(0xffffffffu, trl, 0) & 0x7fffffffu, rbase = fd.node_off + y0 * fd.qw;
-            for (int64_t j = lane; j < n; j += 32) cp_async8(stg + j, ref.tlist + rbase + j);
+            for (int64_t j = lane; j < n; j += 32) {
+                cp_async8(stg + j, ref.tlist + rbase + j);
+                cp_async4(stg_t + j, ref.tch + rbase + j);
+            }
             cp_async_commit();
         }
         RowState S{0, 0};
@@ -1113,39 +1129,41 @@ __global__ void __launch_bounds__(32) k_ref_band(const FrameDesc *frames, RefOrd
                 A.s_Z[k] = (uint32_t)bi;
                 A.s_t[k] = (uint8_t)(bi >> 48);
             }
-            S.m = ma;
-            S.np = na;
+            S.m = (int)ma;
+            S.np = (int)na;
         }
         for (int64_t y = y0; y < y1; y++) {
             const uint32_t tr = __shfl_sync(0xffffffffu, trl, (int)(y - y0));
-            const int64_t n = tr & 0x7fffffffu;
+            const int n = (int)(tr & 0x7fffffffu);
             const bool link = (tr >> 31) != 0;
             const int64_t rbase = fd.node_off + y * fd.qw;
             const uint64_t *src = ref.tlist + rbase;
+            const uint32_t *srct = ref.tch + rbase;
             if (staged) {
                 cp_async_wait_all();
                 src = stg;
+                srct = stg_t;
             }
             __syncwarp();
-            for (int64_t j = lane; j < n; j += 32) {
+            for (int j = lane; j < n; j += 32) {
                 const uint64_t e = src[j];
                 A.c_se[j] = (uint32_t)e;
                 A.c_v[j] = (uint8_t)(e >> 48);
                 A.c_j[j] = (uint16_t)(e >> 32);
                 A.c_t[j] = (uint8_t)(e >> 56);
+                A.c_tch[j] = srct[j];
             }
             __syncwarp();
             if (staged && y + 1 < y1) {
                 const uint32_t tn = __shfl_sync(0xffffffffu, trl, (int)(y + 1 - y0)) & 0x7fffffffu;
-                for (int64_t j = lane; j < tn; j += 32) cp_async8(stg + j, ref.tlist + rbase + fd.qw + j);
+                for (uint32_t j = lane; j < tn; j += 32) {
+                    cp_async8(stg + j, ref.tlist + rbase + fd.qw + j);
+                    cp_async4(stg_t + j, ref.tch + rbase + fd.qw + j);
+                }
                 cp_async_commit();
             }
             if (n == 0 && S.np == 0) continue;
-            if (!replay_row(A, S, n, link && n > 0, (uint32_t)rbase, vbase + (uint32_t)(y - 1), capr, fin, finb,
-                            (uint32_t)b, err)) {
-                cp_async_wait_all();
-                return;
-            }
+            replay_row(A, S, n, link && n > 0, (uint32_t)rbase, vbase + (uint32_t)(y - 1), fin, finb, (uint32_t)b);
         }
         // the roots of the sets at the band's last row, per slot of the
         // boundary below (through the slot's first run); after the last
@@ -1266,11 +1284,11 @@ void launch_ref_order(const Launch &L, const FrameDesc *frames, const uint8_t *t
     // bands of narrow rows, many blocks per SM; then the others
     const int64_t small = P.capr < REF_SMALLR ? P.capr : REF_SMALLR;
     k_ref_band<<<dim3(bands, (unsigned)L.nframes), 32, ref_band_bytes(small, true), L.stream>>>(
-        frames, ref, small, 0u, (uint32_t)small, nullptr, 0, err);
+        frames, ref, small, 0u, (uint32_t)small, nullptr, 0);
     if (P.capr > REF_SMALLR)
         k_ref_band<<<dim3(P.band_scratch ? REF_BAND_BLOCKS : bands, (unsigned)L.nframes), 32,
                      P.band_scratch ? 0 : ref_band_bytes(P.capr, true), L.stream>>>(
-            frames, ref, P.capr, (uint32_t)REF_SMALLR, 0xffffffffu, P.band_scratch, P.band_bytes, err);
+            frames, ref, P.capr, (uint32_t)REF_SMALLR, 0xffffffffu, P.band_scratch, P.band_bytes);
     k_ref_resolve<<<L.nframes, 256, 8 * (P.capr + 1), L.stream>>>(frames, ref, P.capr);
 }
 
