@@ -3,13 +3,15 @@
 //
 // The reference groups the boundary points by the pair of components they
 // lie between, each cluster's points in emission order (y, x, neighbour),
-// and orders the clusters. Here the points are never stored in emission
-// order; each is made from the threshold image and the labels where it is
-// needed, and written once, to its place in its cluster:
+// and orders the clusters. Here each point is made once, from the
+// threshold image and the labels, as a 4-byte record in its row's region;
+// the records are then placed, each at its place in its cluster:
 //
-//   k_pair_hash      a warp per row: the points' label pairs into an
-//                    open-addressing table, with each pair's point count and
-//                    the first and last row holding its points; the total.
+//   k_point_scan     a warp per row: the row's points, their label pairs
+//                    gathered in the warp's table (shared memory), the
+//                    records in emission order; at the row's end each pair
+//                    of the row into the frame's pair table (point count,
+//                    first and last row) and the row's pair list.
 //   k_cluster_collect (at_kernels.cu): the distinct pairs.
 //   -- the host reads the pair and point counts (its only wait here) --
 //   k_pair_frame, k_pair_scatter, k_pair_rank: the distinct pairs in order.
@@ -18,12 +20,13 @@
 //                    pairs are ranked among themselves.
 //   k_cluster_span   per cluster: count, frame, first row, rows spanned.
 //   scans            each cluster's first point; its row table's offset.
-//   k_seg_count      a warp per row: points per (cluster, row).
+//   k_seg_fill       a warp per row: its pairs' point counts into the
+//                    clusters' row tables.
 //   k_seg_scan       a warp per cluster: the counts of its rows become the
 //                    places of each row's first point of the cluster.
-//   k_point_place    a warp per row: every point to its place; points of a
-//                    row go in emission order, so a cluster's points keep
-//                    the reference's order.
+//   k_point_place    a warp per row: every record to its place; records of
+//                    a row are in emission order, so a cluster's points
+//                    keep the reference's order.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,71 +43,155 @@ __device__ __forceinline__ uint64_t point_key(const uint32_t *la, const uint32_t
     return hi << nb | lo;
 }
 
-__device__ __forceinline__ uint64_t point_value(const uint8_t *a, int64_t x, int64_t y, int j) {
-    const int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0;
-    const int dy = j == 0 ? 0 : 1;
-    const int g = a[x] == 0 ? 255 : -255;
-    const uint64_t px = (uint64_t)(2 * x + dx), py = (uint64_t)(2 * y + dy);
-    const uint64_t gx = (uint16_t)(int16_t)(dx * g), gy = (uint16_t)(int16_t)(dy * g);
-    return px | py << 16 | gx << 32 | gy << 48;
-}
-
-// The table slot of a key that is in the table.
-__device__ __forceinline__ uint32_t pair_slot(const PairTable &T, uint64_t k) {
-    uint32_t slot = ch_hash(k) & T.mask;
-    for (int p = 0; p < CH_PROBES && T.keys[slot] != k; p++) slot = (slot + 1) & T.mask;
-    return slot;
-}
-
 // Rows 1 .. qh-2 of each frame, a warp per row.
 #define ROW_WARPS_BEGIN                                                                              \
     const FrameDesc f = frames[blockIdx.y];                                                          \
     const int lane = threadIdx.x & 31;                                                               \
     const int64_t wpb = blockDim.x >> 5;                                                             \
-    for (int64_t y = 1 + blockIdx.x * wpb + (threadIdx.x >> 5); y + 1 < f.qh; y += gridDim.x * wpb) { \
-        const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;                                   \
-        const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+    for (int64_t y = 1 + blockIdx.x * wpb + (threadIdx.x >> 5); y + 1 < f.qh; y += gridDim.x * wpb) {
 #define ROW_WARPS_END }
 
-__global__ void __launch_bounds__(256) k_pair_hash(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
-                                                   int nb, PairTable T, uint32_t *full,
-                                                   unsigned long long *npoints) {
+// A warp's table of the pairs of its row: open addressing over 2 nd_cap
+// slots (key, index), and per index (the order pairs first appear in the
+// row) the key, the slot and the number of points.
+struct RowPairs {
+    uint64_t *tkey, *ikey;
+    uint32_t *icnt;
+    uint16_t *tpos, *islot;
+};
+__host__ __device__ inline size_t row_pairs_bytes(int nd_cap) { return (size_t)34 * nd_cap; }
+__device__ inline RowPairs row_pairs(uint8_t *base, int nd_cap) {
+    RowPairs W;
+    W.tkey = reinterpret_cast<uint64_t *>(base);
+    W.ikey = W.tkey + 2 * nd_cap;
+    W.icnt = reinterpret_cast<uint32_t *>(W.ikey + nd_cap);
+    W.tpos = reinterpret_cast<uint16_t *>(W.icnt + nd_cap);
+    W.islot = W.tpos + 2 * nd_cap;
+    return W;
+}
+
+// Point records: pair index in the row | neighbour j << 11 | (pixel is 0)
+// << 13 | x << 14.
+#define PREC_ID 0x7ffu
+
+// Every boundary point, once: its pair into the warp's row table, its
+// record (emission order) into the row's region; at the row's end each of
+// the row's pairs into the frame's pair table (count, first and last row)
+// and, with its points in the row, into the row's pair list. Any capacity
+// exceeded (pairs of a row, records of a row, probes of the pair table)
+// sets *full and the batch takes the sorting path instead.
+__global__ void __launch_bounds__(256) k_point_scan(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+                                                    int nb, PairTable T, PointRows P, uint32_t *full,
+                                                    unsigned long long *npoints) {
+    extern __shared__ __align__(16) uint8_t s_mem[];
+    const int nd_cap = P.nd_cap, rt = 2 * nd_cap;
+    RowPairs W = row_pairs(s_mem + (threadIdx.x >> 5) * row_pairs_bytes(nd_cap), nd_cap);
+    for (int i = threadIdx.x & 31; i < rt; i += 32) W.tkey[i] = CH_EMPTY;
+    __syncwarp();
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
+    uint64_t pts = 0;
     ROW_WARPS_BEGIN
-    uint32_t cnt = 0;
+    const uint8_t *a = thr + f.q_off + y * f.qw, *b = a + f.qw;
+    const uint32_t *la = lab + f.q_off + y * f.qw, *lb = la + f.qw;
+    uint32_t *rec = P.rec + 2 * (f.q_off + y * f.qw);
+    const uint32_t rcap = (uint32_t)(2 * f.qw);
+    uint32_t nd = 0, nrec = 0;
     for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
         const int64_t x = x0 + lane;
         const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
         if (!__any_sync(0xffffffffu, m != 0)) continue;
-        cnt += __popc(m);
+        uint32_t total;
+        const uint32_t o = warp_excl_scan(__popc(m), &total);
+        if (nrec + total > rcap) {
+            if (lane == 0) atomicOr(full, 1u);
+            return;
+        }
+        uint32_t id4[4];
+#pragma unroll
         for (int j = 0; j < 4; j++) {
             const uint64_t k = (m >> j & 1u) ? point_key(la, lb, x, j, nb) : CH_EMPTY;
             const uint32_t peers = __match_any_sync(0xffffffffu, k);
-            if (k == CH_EMPTY || lane != __ffs(peers) - 1) continue;
-            uint32_t slot = ch_hash(k) & T.mask;
-            int p = 0;
-            for (; p < CH_PROBES; p++) {
-                uint64_t cur = *(volatile uint64_t *)(T.keys + slot);
-                if (cur == CH_EMPTY) {
+            const int leader = __ffs(peers) - 1;
+            const bool lead = k != CH_EMPTY && lane == leader;
+            uint32_t h = 0;
+            bool added = false;
+            if (lead) {  // the distinct keys' leaders find or add them
+                h = ch_hash(k) & (uint32_t)(rt - 1);
+                for (int p = 0; p < rt; p++) {
                     const unsigned long long old =
-                        atomicCAS(reinterpret_cast<unsigned long long *>(T.keys + slot), CH_EMPTY, k);
-                    cur = old == CH_EMPTY ? k : old;
+                        atomicCAS(reinterpret_cast<unsigned long long *>(W.tkey + h), CH_EMPTY, k);
+                    if (old == CH_EMPTY) {
+                        added = true;
+                        break;
+                    }
+                    if (old == k) break;
+                    h = (h + 1) & (uint32_t)(rt - 1);
                 }
-                if (cur == k) break;
-                slot = (slot + 1) & T.mask;
             }
-            if (p == CH_PROBES) {
-                atomicOr(full, 1u);
-                continue;
+            const uint32_t nadd = __ballot_sync(0xffffffffu, added);
+            if (nd + __popc(nadd) > (uint32_t)nd_cap) {
+                if (lane == 0) atomicOr(full, 1u);
+                return;
             }
-            atomicAdd(T.count + slot, (uint32_t)__popc(peers));
+            uint32_t id = 0;
+            if (lead) {
+                if (added) {
+                    id = nd + __popc(nadd & lt);
+                    W.tpos[h] = (uint16_t)id;
+                    W.ikey[id] = k;
+                    W.islot[id] = (uint16_t)h;
+                    W.icnt[id] = (uint32_t)__popc(peers);
+                } else {
+                    id = W.tpos[h];
+                    W.icnt[id] += (uint32_t)__popc(peers);
+                }
+            }
+            nd += __popc(nadd);
+            id4[j] = __shfl_sync(0xffffffffu, id, leader);
+            __syncwarp();
+        }
+        // this lane's points, in emission order (x, then neighbour)
+        if (m) {
+            const uint32_t g = a[x] == 0 ? 1u : 0u;
+            uint32_t t = nrec + o;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (m >> j & 1u) rec[t++] = id4[j] | (uint32_t)j << 11 | g << 13 | (uint32_t)x << 14;
+        }
+        nrec += total;
+    }
+    __syncwarp();
+    // the row's pairs into the frame's pair table; the table cleared
+    uint32_t *ps = P.pslot + (f.row0 + y) * nd_cap, *pc = P.pcnt + (f.row0 + y) * nd_cap;
+    for (uint32_t i = lane; i < nd; i += 32) {
+        const uint64_t k = W.ikey[i];
+        uint32_t slot = ch_hash(k) & T.mask;
+        int p = 0;
+        for (; p < CH_PROBES; p++) {
+            uint64_t cur = *(volatile uint64_t *)(T.keys + slot);
+            if (cur == CH_EMPTY) {
+                const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(T.keys + slot), CH_EMPTY, k);
+                cur = old == CH_EMPTY ? k : old;
+            }
+            if (cur == k) break;
+            slot = (slot + 1) & T.mask;
+        }
+        if (p == CH_PROBES) {
+            atomicOr(full, 1u);
+        } else {
+            atomicAdd(T.count + slot, W.icnt[i]);
             atomicMin(T.ymin + slot, (uint32_t)y);
             atomicMax(T.ymax + slot, (uint32_t)y);
         }
+        ps[i] = slot;
+        pc[i] = W.icnt[i];
+        W.tkey[W.islot[i]] = CH_EMPTY;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if (lane == 0 && cnt) atomicAdd(npoints, (unsigned long long)cnt);
+    if (lane == 0) P.info[f.row0 + y] = make_uint2(nrec, nd);
+    pts += nrec;
+    __syncwarp();
     ROW_WARPS_END
+    if ((threadIdx.x & 31) == 0 && pts) atomicAdd(npoints, (unsigned long long)pts);
 }
 
 __device__ __forceinline__ int frame_of_node(const FrameDesc *frames, int nframes, int64_t node) {
@@ -287,27 +374,6 @@ __global__ void k_seg_zero(const uint32_t *spanoff, int64_t ncl, uint32_t *seg, 
         seg[i] = 0;
 }
 
-__global__ void __launch_bounds__(256) k_seg_count(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
-                                                   int nb, PairTable T, const uint32_t *rank_of_slot,
-                                                   const uint32_t *spanoff, const uint32_t *cy0, int64_t ncl,
-                                                   uint32_t *seg, int64_t cap) {
-    if (spanoff[ncl] > cap) return;
-    ROW_WARPS_BEGIN
-    for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
-        const int64_t x = x0 + lane;
-        const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
-        if (!__any_sync(0xffffffffu, m != 0)) continue;
-        for (int j = 0; j < 4; j++) {
-            uint32_t c = 0xffffffffu;
-            if (m >> j & 1u) c = rank_of_slot[pair_slot(T, point_key(la, lb, x, j, nb))];
-            const uint32_t peers = __match_any_sync(0xffffffffu, c);
-            if (c == 0xffffffffu || lane != __ffs(peers) - 1) continue;
-            atomicAdd(seg + spanoff[c] + ((uint32_t)y - cy0[c]), (uint32_t)__popc(peers));
-        }
-    }
-    ROW_WARPS_END
-}
-
 // A warp per cluster: seg[spanoff[c] + r] = the place of the cluster's
 // first point in row cy0[c] + r.
 __global__ void __launch_bounds__(256) k_seg_scan(const uint32_t *cstart, const uint32_t *spanoff,
@@ -330,56 +396,64 @@ __global__ void __launch_bounds__(256) k_seg_scan(const uint32_t *cstart, const 
     }
 }
 
-#define PLACE_STAGE 128  // points of 32 pixels, at most
-
-__global__ void __launch_bounds__(256) k_point_place(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
-                                                     int nb, PairTable T, const uint32_t *rank_of_slot,
-                                                     const uint32_t *spanoff, const uint32_t *cy0, int64_t ncl,
-                                                     uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts,
-                                                     uint32_t *err) {
-    __shared__ uint32_t s_c[8][PLACE_STAGE];
-    __shared__ uint64_t s_v[8][PLACE_STAGE];
+// Each row's pairs: their point counts into the row tables
+// (seg[spanoff[c] + y - cy0[c]] for the pair's cluster c).
+__global__ void __launch_bounds__(256) k_seg_fill(const FrameDesc *frames, PointRows P, const uint32_t *rank_of_slot,
+                                                  const uint32_t *spanoff, const uint32_t *cy0, int64_t ncl,
+                                                  uint32_t *seg, int64_t cap) {
     if (spanoff[ncl] > cap) return;
-    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
-    uint32_t *sc = s_c[threadIdx.x >> 5];
-    uint64_t *sv = s_v[threadIdx.x >> 5];
     ROW_WARPS_BEGIN
-    for (int64_t x0 = 0; x0 < f.qw; x0 += 32) {
-        const int64_t x = x0 + lane;
-        const uint32_t m = x < f.qw ? point_mask(a, b, la, lb, x, f.qw) : 0u;
-        if (!__any_sync(0xffffffffu, m != 0)) continue;
-        // this chunk's points in emission order (x, then neighbour)
-        uint32_t total;
-        uint32_t o = warp_excl_scan(__popc(m), &total);
-        for (int j = 0; j < 4; j++)
-            if (m >> j & 1u) {
-                sc[o] = rank_of_slot[pair_slot(T, point_key(la, lb, x, j, nb))];
-                sv[o] = point_value(a, x, y, j);
-                o++;
-            }
+    const uint32_t nd = P.info[f.row0 + y].y;
+    const uint32_t *ps = P.pslot + (f.row0 + y) * P.nd_cap, *pc = P.pcnt + (f.row0 + y) * P.nd_cap;
+    for (uint32_t i = lane; i < nd; i += 32) {
+        const uint32_t c = rank_of_slot[ps[i]];
+        seg[spanoff[c] + ((uint32_t)y - cy0[c])] = pc[i];
+    }
+    ROW_WARPS_END
+}
+
+// A warp per row: each record to its place, the row's first place of each
+// pair's cluster (seg, after the scan) plus the pair's points before it in
+// the row; the records are in emission order, so a cluster's points keep
+// the reference's order.
+__global__ void __launch_bounds__(256) k_point_place(const FrameDesc *frames, PointRows P,
+                                                     const uint32_t *rank_of_slot, const uint32_t *spanoff,
+                                                     const uint32_t *cy0, int64_t ncl, const uint32_t *seg, int64_t cap,
+                                                     uint64_t *out, int64_t npts, uint32_t *err) {
+    extern __shared__ __align__(16) uint32_t s_base[];
+    if (spanoff[ncl] > cap) return;
+    uint32_t *base = s_base + (threadIdx.x >> 5) * P.nd_cap;
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
+    ROW_WARPS_BEGIN
+    const uint2 inf = P.info[f.row0 + y];
+    const uint32_t *ps = P.pslot + (f.row0 + y) * P.nd_cap;
+    for (uint32_t i = lane; i < inf.y; i += 32) {
+        const uint32_t c = rank_of_slot[ps[i]];
+        base[i] = seg[spanoff[c] + ((uint32_t)y - cy0[c])];
+    }
+    __syncwarp();
+    const uint32_t *rec = P.rec + 2 * (f.q_off + y * f.qw);
+    for (uint32_t r0 = 0; r0 < inf.x; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        const bool valid = r < inf.x;
+        const uint32_t rc = valid ? rec[r] : 0u;
+        const uint32_t id = valid ? rc & PREC_ID : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, id);
+        const uint32_t at = valid ? base[id] + __popc(peers & lt) : 0u;
         __syncwarp();
-        // 32 at a time, in order: a point's place is its cluster's cursor
-        // for this row plus the cluster's points before it in the batch
-        for (uint32_t s0 = 0; s0 < total; s0 += 32) {
-            const uint32_t i = s0 + lane;
-            const bool valid = i < total;
-            const uint32_t c = valid ? sc[i] : 0xffffffffu;
-            const uint32_t peers = __match_any_sync(0xffffffffu, c);
-            const int leader = __ffs(peers) - 1;
-            uint32_t *cursor = valid ? seg + spanoff[c] + ((uint32_t)y - cy0[c]) : nullptr;
-            uint32_t base = 0;
-            if (valid && lane == leader) base = *cursor;
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (valid) {
-                const uint32_t at = base + __popc(peers & lt);
-                if (at < npts)  // always, unless the counts disagree: then an error, not a stray write
-                    out[at] = sv[i];
-                else
-                    atomicOr(err, AT_ERR_CAPACITY);
-                if (lane == leader) *cursor = base + __popc(peers);
-            }
-            __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) base[id] += __popc(peers);
+        if (valid) {
+            const uint32_t j = (rc >> 11) & 3u, x = rc >> 14;
+            const int dx = j == 0 || j == 3 ? 1 : j == 2 ? -1 : 0, dy = j == 0 ? 0 : 1;
+            const int g = (rc >> 13 & 1u) ? 255 : -255;
+            const uint64_t px = (uint64_t)(2 * (int64_t)x + dx), py = (uint64_t)(2 * y + dy);
+            const uint64_t gx = (uint16_t)(int16_t)(dx * g), gy = (uint16_t)(int16_t)(dy * g);
+            if (at < npts)  // always, unless the counts disagree: then an error, not a stray write
+                out[at] = px | py << 16 | gx << 32 | gy << 48;
+            else
+                atomicOr(err, AT_ERR_CAPACITY);
         }
+        __syncwarp();
     }
     ROW_WARPS_END
 }
@@ -397,9 +471,23 @@ static inline dim3 row_warps(const Launch &L) {
     return dim3((unsigned)(b < 1 ? 1 : b < 148 * 8 ? b : 148 * 8), (unsigned)L.nframes);
 }
 
-void launch_pair_hash(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
-                      const PairTable &T, uint32_t *full, unsigned long long *npoints) {
-    k_pair_hash<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, full, npoints);
+// Warps per block of the point scan: their row tables within 96 KB.
+static inline int scan_warps(int nd_cap) {
+    const int w = (int)((96 * 1024) / row_pairs_bytes(nd_cap));
+    return w < 1 ? 1 : w > 8 ? 8 : w;
+}
+
+bool point_scan_set_smem() {
+    return cudaFuncSetAttribute(k_point_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024) == cudaSuccess &&
+           cudaFuncSetAttribute(k_point_place, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) == cudaSuccess;
+}
+
+void launch_point_scan(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                       const PairTable &T, const PointRows &P, uint32_t *full, unsigned long long *npoints) {
+    const int w = scan_warps(P.nd_cap);
+    const int64_t b = (L.max_qh + w - 1) / w;
+    const dim3 grid((unsigned)(b < 1 ? 1 : b < 148 * 8 ? b : 148 * 8), (unsigned)L.nframes);
+    k_point_scan<<<grid, 32 * w, w * row_pairs_bytes(P.nd_cap), L.stream>>>(frames, thr, lab, nb, T, P, full, npoints);
 }
 
 void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *oslots, int64_t ncl, int nb,
@@ -424,15 +512,13 @@ void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *os
 
 int64_t pair_scan_blocks(int64_t ncl) { return (ncl + SCAN_ITEMS - 1) / SCAN_ITEMS + 1; }
 
-void launch_point_place(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
-                        const PairTable &T, const uint32_t *rank_of_slot, const uint32_t *cstart,
-                        const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0, int64_t ncl,
-                        uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err) {
+void launch_point_place(const Launch &L, const FrameDesc *frames, const PointRows &P, const uint32_t *rank_of_slot,
+                        const uint32_t *cstart, const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0,
+                        int64_t ncl, uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err) {
     if (ncl <= 0) return;
     k_seg_zero<<<flat_grid(cap, 256), 256, 0, L.stream>>>(spanoff, ncl, seg, cap, err);
-    k_seg_count<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, rank_of_slot, spanoff, cy0, ncl, seg,
-                                                    cap);
+    k_seg_fill<<<row_warps(L), 256, 0, L.stream>>>(frames, P, rank_of_slot, spanoff, cy0, ncl, seg, cap);
     k_seg_scan<<<flat_grid(ncl * 32, 256), 256, 0, L.stream>>>(cstart, spanoff, cspan, ncl, seg, cap);
-    k_point_place<<<row_warps(L), 256, 0, L.stream>>>(frames, thr, lab, nb, T, rank_of_slot, spanoff, cy0, ncl, seg,
-                                                      cap, out, npts, err);
+    k_point_place<<<row_warps(L), 256, 8 * P.nd_cap * 4, L.stream>>>(frames, P, rank_of_slot, spanoff, cy0, ncl, seg,
+                                                                    cap, out, npts, err);
 }

@@ -99,6 +99,7 @@ enum {
     B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
     B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RBWIDE, B_RDESC, B_RNBAND, B_RFSCR, B_RTCH, B_RLTOP, B_RLPX, B_RLBOT,
     B_RLPX2,
+    B_PREC, B_PPSLOT, B_PPCNT, B_PINFO,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -130,7 +131,8 @@ struct at_internal {
     // sizes of the last run (frame 0), for at_detector_diag
     int64_t last_qw = 0, last_qh = 0, last_npts = 0, last_ncl = 0, last_nq = 0;
     int64_t launches = 0;  // kernels of this library launched so far
-    size_t ref_smem = 0;   // the shared memory the replay kernel is allowed (set per device)
+    size_t ref_smem = 0;     // the shared memory the replay kernel is allowed (set per device)
+    bool scan_smem = false;  // the point scan's shared memory allowance is set
     int64_t seg_slack = 64;  // row-table entries per cluster beyond its points (grows on a shortfall)
 
     // A large batch is spread over up to `split` pipelines: this detector
@@ -485,7 +487,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     int64_t ncl = 0, nq = 0;
     uint64_t npts = 0;
     uint32_t hsize = 1u << 16;
-    while ((int64_t)hsize < qpx / 8 && hsize < (1u << 30)) hsize <<= 1;
+    while ((int64_t)hsize < qpx / 32 && hsize < (1u << 30)) hsize <<= 1;
     CK(B[B_HKEYS].ensure((size_t)hsize * 8));
     CK(B[B_HCOUNT].ensure((size_t)hsize * 4));
     CK(B[B_HYMIN].ensure((size_t)hsize * 4));
@@ -500,7 +502,25 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(cudaMemsetAsync(pt.ymin, 0xff, (size_t)hsize * 4, st));
     CK(cudaMemsetAsync(pt.ymax, 0, (size_t)hsize * 4, st));
     CK(cudaMemsetAsync(misc, 0, 32, st));
-    launch_pair_hash(L, dfr, thr, lab, nb, pt, misc, reinterpret_cast<unsigned long long *>(misc + 2));
+    // each row's points as records, its pairs gathered in shared memory
+    int64_t max_qw = 0;
+    for (auto &f : fd) max_qw = f.qw > max_qw ? f.qw : max_qw;
+    int32_t nd_cap = 64;
+    while (nd_cap < max_qw / 8 && nd_cap < 2048) nd_cap <<= 1;
+    CK(B[B_PREC].ensure(qpx * 8));
+    CK(B[B_PPSLOT].ensure(rows * nd_cap * 4));
+    CK(B[B_PPCNT].ensure(rows * nd_cap * 4));
+    CK(B[B_PINFO].ensure(rows * 8));
+    if (!in->scan_smem) {
+        if (!point_scan_set_smem()) {
+            set_error(in, 1, "cudaFuncSetAttribute for the point scan failed");
+            return false;
+        }
+        in->scan_smem = true;
+    }
+    const PointRows prow{B[B_PREC].as<uint32_t>(), B[B_PPSLOT].as<uint32_t>(), B[B_PPCNT].as<uint32_t>(),
+                         B[B_PINFO].as<uint2>(), nd_cap};
+    launch_point_scan(L, dfr, thr, lab, nb, pt, prow, misc, reinterpret_cast<unsigned long long *>(misc + 2));
     CK(B[B_HOKEYS].ensure((size_t)hsize * 8));
     CK(B[B_HOSLOTS].ensure((size_t)hsize * 4));
     launch_cluster_collect(st, pt.keys, hsize, B[B_HOKEYS].as<uint64_t>(), B[B_HOSLOTS].as<uint32_t>(), misc + 1);
@@ -537,7 +557,7 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                           B[B_HSKEYS].as<uint64_t>(), B[B_HSSLOTS].as<uint32_t>(), B[B_HRANK].as<uint32_t>(),
                           B[B_HCCOUNT].as<uint32_t>(), B[B_CSPAN].as<uint32_t>(), B[B_CY0].as<uint32_t>(),
                           B[B_CFRAME].as<int32_t>(), B[B_CSTART].as<uint32_t>(), B[B_SPANOFF].as<uint32_t>());
-        launch_point_place(L, dfr, thr, lab, nb, pt, B[B_HRANK].as<uint32_t>(), B[B_CSTART].as<uint32_t>(),
+        launch_point_place(L, dfr, prow, B[B_HRANK].as<uint32_t>(), B[B_CSTART].as<uint32_t>(),
                            B[B_SPANOFF].as<uint32_t>(), B[B_CSPAN].as<uint32_t>(), B[B_CY0].as<uint32_t>(), ncl,
                            B[B_SEG].as<uint32_t>(), segcap, B[B_VAL2].as<uint64_t>(), (int64_t)npts,
                            B[B_ERR].as<uint32_t>());

@@ -74,17 +74,28 @@ struct PairScratch {
     uint64_t *gkeys;
     uint32_t *gslots, *bsum_a, *bsum_b;
 };
-void launch_pair_hash(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
-                      const PairTable &T, uint32_t *full, unsigned long long *npoints);
+// The points of each row (rows 1 .. qh-2): records in emission order at
+// rec + 2 (q_off + y qw), at most 2 qw a row (pair index in the row |
+// neighbour << 11 | pixel is 0 << 13 | x << 14); the row's distinct pairs
+// (slot in the pair table, points) at (row0 + y) nd_cap; info[row0 + y] =
+// (records, pairs).
+struct PointRows {
+    uint32_t *rec;
+    uint32_t *pslot, *pcnt;
+    uint2 *info;
+    int32_t nd_cap;
+};
+bool point_scan_set_smem();
+void launch_point_scan(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
+                       const PairTable &T, const PointRows &P, uint32_t *full, unsigned long long *npoints);
 void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *oslots, int64_t ncl, int nb,
                        const FrameDesc *frames, int nframes, const PairTable &T, const PairScratch &P,
                        uint64_t *skeys, uint32_t *sslots, uint32_t *rank_of_slot, uint32_t *ccount, uint32_t *cspan,
                        uint32_t *cy0, int32_t *cframe, uint32_t *cstart, uint32_t *spanoff);
 int64_t pair_scan_blocks(int64_t ncl);
-void launch_point_place(const Launch &L, const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab, int nb,
-                        const PairTable &T, const uint32_t *rank_of_slot, const uint32_t *cstart,
-                        const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0, int64_t ncl,
-                        uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err);
+void launch_point_place(const Launch &L, const FrameDesc *frames, const PointRows &P, const uint32_t *rank_of_slot,
+                        const uint32_t *cstart, const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0,
+                        int64_t ncl, uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err);
 void launch_cluster_starts(cudaStream_t s, const uint64_t *key, const uint32_t *head, const uint32_t *head_scan,
                            int64_t n, int nb, const FrameDesc *frames, int nframes, uint32_t *cstart, int32_t *cframe,
                            uint64_t *ckey);
