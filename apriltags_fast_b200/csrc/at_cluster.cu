@@ -109,45 +109,64 @@ __global__ void __launch_bounds__(256) k_point_scan(const FrameDesc *frames, con
         uint32_t id4[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const uint64_t k = (m >> j & 1u) ? point_key(la, lb, x, j, nb) : CH_EMPTY;
-            const uint32_t peers = __match_any_sync(0xffffffffu, k);
-            const int leader = __ffs(peers) - 1;
-            const bool lead = k != CH_EMPTY && lane == leader;
-            uint32_t h = 0;
-            bool added = false;
-            if (lead) {  // the distinct keys' leaders find or add them
-                h = ch_hash(k) & (uint32_t)(rt - 1);
+            const bool has = (m >> j & 1u) != 0;
+            const uint64_t k = has ? point_key(la, lb, x, j, nb) : CH_EMPTY;
+            // the pair's index in the row, if the row has met it already
+            uint32_t id = 0xffffffffu;
+            if (has) {
+                uint32_t h = ch_hash(k) & (uint32_t)(rt - 1);
                 for (int p = 0; p < rt; p++) {
-                    const unsigned long long old =
-                        atomicCAS(reinterpret_cast<unsigned long long *>(W.tkey + h), CH_EMPTY, k);
-                    if (old == CH_EMPTY) {
-                        added = true;
+                    const uint64_t cur = W.tkey[h];
+                    if (cur == k) {
+                        id = W.tpos[h];
                         break;
                     }
-                    if (old == k) break;
+                    if (cur == CH_EMPTY) break;
                     h = (h + 1) & (uint32_t)(rt - 1);
                 }
             }
-            const uint32_t nadd = __ballot_sync(0xffffffffu, added);
-            if (nd + __popc(nadd) > (uint32_t)nd_cap) {
-                if (lane == 0) atomicOr(full, 1u);
-                return;
-            }
-            uint32_t id = 0;
-            if (lead) {
-                if (added) {
-                    id = nd + __popc(nadd & lt);
-                    W.tpos[h] = (uint16_t)id;
-                    W.ikey[id] = k;
-                    W.islot[id] = (uint16_t)h;
-                    W.icnt[id] = (uint32_t)__popc(peers);
-                } else {
-                    id = W.tpos[h];
-                    W.icnt[id] += (uint32_t)__popc(peers);
+            const bool miss = has && id == 0xffffffffu;
+            if (__any_sync(0xffffffffu, miss)) {
+                // pairs new to the row: each one's leader adds it
+                __syncwarp();
+                const uint64_t km = miss ? k : CH_EMPTY;
+                const uint32_t peers = __match_any_sync(0xffffffffu, km);
+                const int leader = __ffs(peers) - 1;
+                const bool lead = miss && lane == leader;
+                uint32_t h = 0;
+                bool added = false;
+                if (lead) {
+                    h = ch_hash(k) & (uint32_t)(rt - 1);
+                    for (int p = 0; p < rt; p++) {
+                        const unsigned long long old =
+                            atomicCAS(reinterpret_cast<unsigned long long *>(W.tkey + h), CH_EMPTY, k);
+                        if (old == CH_EMPTY) {
+                            added = true;
+                            break;
+                        }
+                        h = (h + 1) & (uint32_t)(rt - 1);
+                    }
                 }
+                const uint32_t nadd = __ballot_sync(0xffffffffu, added);
+                if (nd + __popc(nadd) > (uint32_t)nd_cap) {
+                    if (lane == 0) atomicOr(full, 1u);
+                    return;
+                }
+                uint32_t nid = 0;
+                if (added) {
+                    nid = nd + __popc(nadd & lt);
+                    W.tpos[h] = (uint16_t)nid;
+                    W.ikey[nid] = k;
+                    W.islot[nid] = (uint16_t)h;
+                    W.icnt[nid] = 0;
+                }
+                nd += __popc(nadd);
+                nid = __shfl_sync(0xffffffffu, nid, leader);
+                if (miss) id = nid;
+                __syncwarp();
             }
-            nd += __popc(nadd);
-            id4[j] = __shfl_sync(0xffffffffu, id, leader);
+            if (has) atomicAdd(W.icnt + id, 1u);
+            id4[j] = id;
             __syncwarp();
         }
         // this lane's points, in emission order (x, then neighbour)

@@ -628,19 +628,21 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
     __shared__ uint32_t s_se[UB_CAP];
     __shared__ uint32_t s_par[UB_CAP];
     __shared__ uint8_t s_v[UB_CAP];
+    __shared__ uint8_t s_row[UB_CAP];
     __shared__ uint32_t s_roff[UB_ROWS + 1];
+    static_assert(UB_ROWS <= 32, "one warp scans the band's row counts");
     const FrameDesc f = frames[blockIdx.y];
+    const int tid = threadIdx.x;
     const int nband = (f.qh + UB_ROWS - 1) / UB_ROWS;
     for (int b = blockIdx.x; b < nband; b += gridDim.x) {
         const int y0 = b * UB_ROWS, nr = min(UB_ROWS, f.qh - y0);
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for (int r = 0; r < nr; r++) {
-                s_roff[r] = acc;
-                acc += row_nruns[f.row0 + y0 + r];
-            }
-            s_roff[nr] = acc;
+        if (tid < 32) {
+            const uint32_t c = tid < nr ? row_nruns[f.row0 + y0 + tid] : 0u;
+            uint32_t total;
+            const uint32_t off = warp_excl_scan(c, &total);
+            if (tid < nr) s_roff[tid] = off;
+            if (tid == 0) s_roff[nr] = total;
         }
         __syncthreads();
         const uint32_t L = s_roff[nr];
@@ -649,7 +651,7 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
             for (int r = 1; r < nr; r++) {
                 const int64_t cur = f.node_off + (int64_t)(y0 + r) * f.qw, prev = cur - f.qw;
                 const int64_t ncur = s_roff[r + 1] - s_roff[r], nprev = s_roff[r] - s_roff[r - 1];
-                for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
+                for (int64_t i = tid; i < ncur; i += blockDim.x) {
                     const int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
                     const uint8_t v = runs.v[cur + i];
                     int64_t lo = 0, hi = nprev;
@@ -667,35 +669,40 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
             }
             continue;
         }
-        // stage the band's runs (local id = s_roff[row] + index)
-        for (int r = 0; r < nr; r++) {
-            const int64_t base = f.node_off + (int64_t)(y0 + r) * f.qw;
-            const uint32_t o = s_roff[r], n = s_roff[r + 1] - o;
-            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-                s_se[o + i] = (uint32_t)runs.start[base + i] | (uint32_t)runs.end[base + i] << 16;
-                s_v[o + i] = runs.v[base + i];
-                s_par[o + i] = o + i;
-            }
+        // stage the band's runs (local id l = s_roff[row] + index)
+        for (uint32_t l = tid; l < L; l += blockDim.x) {
+            int r = 0;
+            while (s_roff[r + 1] <= l) r++;
+            const int64_t node = f.node_off + (int64_t)(y0 + r) * f.qw + (l - s_roff[r]);
+            s_se[l] = (uint32_t)runs.start[node] | (uint32_t)runs.end[node] << 16;
+            s_v[l] = runs.v[node];
+            s_par[l] = l;
+            s_row[l] = (uint8_t)r;
         }
         __syncthreads();
         // the unions of rows 1.. of the band with the row above, in shared memory
-        for (uint32_t l = s_roff[1] + threadIdx.x; l < L; l += blockDim.x) {
-            int r = 1;
-            while (s_roff[r + 1] <= l) r++;
-            const uint32_t pb = s_roff[r - 1], np = s_roff[r] - pb;
-            const int64_t a0 = s_se[l] & 0xffffu, a1 = s_se[l] >> 16;
+        for (uint32_t l = s_roff[1] + tid; l < L; l += blockDim.x) {
+            const int r = s_row[l];
+            const uint32_t pb = s_roff[r - 1], pe = s_roff[r];
+            const int a0 = (int)(s_se[l] & 0xffffu), a1 = (int)(s_se[l] >> 16);
             const uint8_t v = s_v[l];
-            FOR_TOUCHING(s_se, s_v, pb, np, a0, a1, v, k, { lu_unite(s_par, l, (uint32_t)(pb + k)); })
+            uint32_t lo = pb, hi = pe;
+            while (lo < hi) {  // the first run above whose end reaches a0 - 1
+                const uint32_t mid = (lo + hi) >> 1;
+                if ((int)(s_se[mid] >> 16) + 1 < a0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            for (uint32_t k = lo; k < pe && (int)(s_se[k] & 0xffffu) <= a1 + 1; k++)
+                if (s_v[k] == v && runs_touch(a0, a1, s_se[k] & 0xffffu, s_se[k] >> 16, v)) lu_unite(s_par, l, k);
         }
         __syncthreads();
         // every node points at its local root (read-only walks)
-        for (uint32_t l = threadIdx.x; l < L; l += blockDim.x) {
+        for (uint32_t l = tid; l < L; l += blockDim.x) {
             uint32_t x = l;
             while (s_par[x] != x) x = s_par[x];
-            int r = 0;
-            while (s_roff[r + 1] <= l) r++;
-            int rr = 0;
-            while (s_roff[rr + 1] <= x) rr++;
+            const int r = s_row[l], rr = s_row[x];
             const int64_t node = f.node_off + (int64_t)(y0 + r) * f.qw + (l - s_roff[r]);
             const int64_t root = f.node_off + (int64_t)(y0 + rr) * f.qw + (x - s_roff[rr]);
             runs.parent[node] = (uint32_t)root;
@@ -774,13 +781,7 @@ __global__ void __launch_bounds__(256) k_row_sums(const FrameDesc *frames, RunAr
             if (r != (uint32_t)node) runs.parent[node] = r;
             const uint32_t px = i < n ? (uint32_t)(runs.end[node] - runs.start[node] + 1) : 1u;
             const uint32_t peers = __match_any_sync(live, r);
-            uint32_t sum = 0, mn = 0xffffffffu;
-            for (uint32_t m = peers; m; m &= m - 1) {
-                int src = __ffs(m) - 1;
-                sum += __shfl_sync(peers, px, src);
-                uint32_t o = __shfl_sync(peers, (uint32_t)node, src);
-                mn = o < mn ? o : mn;
-            }
+            const uint32_t sum = __reduce_add_sync(peers, px), mn = __reduce_min_sync(peers, (uint32_t)node);
             if (lane == __ffs(peers) - 1) {
                 atomicAdd(runs.px + r, sum);
                 atomicMin(runs.minid + r, mn);
