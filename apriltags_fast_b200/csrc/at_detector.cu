@@ -13,6 +13,10 @@
 #include <string.h>
 
 #include <cub/cub.cuh>
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -142,6 +146,7 @@ struct at_internal {
     int split = AT_BATCH_SPLIT_DEFAULT;
     at_detector *helper[AT_BATCH_SPLIT_MAX - 1] = {};
     uint64_t fam_gen = 0, helper_gen[AT_BATCH_SPLIT_MAX - 1] = {};
+    struct CopyChain *chain = nullptr;  // the order of the pipelines' host copies
 };
 
 // ---------------------------------------------------------------------------
@@ -313,8 +318,51 @@ template <class F> static bool cub_call(at_internal *in, F &&f) {
     return true;
 }
 
-static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *res) {
+// The pipelines of one split batch copy their host frames in pipeline
+// order: pipeline k's copies start on the device once pipeline k - 1's are
+// done, so the first pipeline computes while the later ones' frames are
+// still crossing the bus (copies issued together share it and all end late).
+struct CopyChain {
+    std::mutex m;
+    std::condition_variable cv;
+    int done = 0;  // the pipelines whose copies are issued (their events recorded)
+    cudaEvent_t ev[AT_BATCH_SPLIT_MAX] = {};
+};
+
+// A pipeline's turn in the chain; it is passed on when the pipeline's
+// copies are issued, or when the pipeline ends without them.
+struct CopyTurn {
+    CopyChain *c = nullptr;
+    int k = 0;
+    cudaStream_t st = nullptr;
+    bool passed = false;
+    void wait() {
+        if (!c || k == 0) return;
+        std::unique_lock<std::mutex> l(c->m);
+        // bounded: a pipeline that never passes its turn cannot stall this one
+        c->cv.wait_for(l, std::chrono::seconds(10), [&] { return c->done >= k; });
+        if (c->done >= k) cudaStreamWaitEvent(st, c->ev[k - 1], 0);
+    }
+    void pass() {
+        if (!c || passed) return;
+        passed = true;
+        cudaEventRecord(c->ev[k], st);
+        {
+            std::lock_guard<std::mutex> l(c->m);
+            c->done = std::max(c->done, k + 1);
+        }
+        c->cv.notify_all();
+    }
+    ~CopyTurn() { pass(); }
+};
+
+static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *res,
+                      CopyChain *chain = nullptr, int link = 0) {
     at_internal *in = td->in;
+    CopyTurn turn;
+    turn.c = chain;
+    turn.k = link;
+    turn.st = in->stream;
     cudaStream_t st = in->stream;
     CK(cudaSetDevice(in->device));
     if (td->qtp.max_nmaxima > AT_MAX_NMAXIMA || td->qtp.max_nmaxima < 0) {
@@ -432,11 +480,13 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
     CK(cudaEventRecord(in->ev[0], st));
     CK(cudaMemcpyAsync(B[B_FRAMES].p, in->h_frames.p, n * sizeof(FrameDesc), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(B[B_ERR].p, 0, 4, st));
+    turn.wait();
     for (int64_t i = 0; i < n; i++) {
         if (!copied[i]) continue;
         CK(cudaMemcpy2DAsync(const_cast<uint8_t *>(fd[i].img), fd[i].w, frames[i].pixels, frames[i].stride, fd[i].w,
                              fd[i].h, cudaMemcpyDefault, st));
     }
+    turn.pass();
     uint8_t *qim = B[B_QIM].as<uint8_t>(), *thr = B[B_THR].as<uint8_t>();
     // decimate 2 without blur: decimation and threshold in one pass (its
     // time is the threshold stage's, as when the reference fuses them)
@@ -882,6 +932,11 @@ void at_detector_destroy(at_detector *td) {
         for (void *p : in->fam_mem[i]) cudaFree(p);
     in->dfam.release();
     for (int k = 0; k < 12; k++) cudaEventDestroy(in->ev[k]);
+    if (in->chain) {
+        for (cudaEvent_t e : in->chain->ev)
+            if (e) cudaEventDestroy(e);
+        delete in->chain;
+    }
     cudaEventDestroy(in->fork);
     cudaEventDestroy(in->join);
     cudaEventDestroy(in->join2);
@@ -972,12 +1027,21 @@ static bool run_split(at_detector *td, const at_frame *frames, int64_t n, at_fra
     }
     std::vector<at_frame_result> part(n);
     bool ok[AT_BATCH_SPLIT_MAX] = {};
+    if (!in->chain) in->chain = new CopyChain;
+    CopyChain &chain = *in->chain;
+    for (int k = 0; k < P; k++)
+        if (!chain.ev[k] && cudaEventCreateWithFlags(&chain.ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            set_error(in, 1, "cudaEventCreate failed");
+            return false;
+        }
+    chain.done = 0;
     std::vector<std::thread> th;
     for (int k = 1; k < P; k++)
         th.emplace_back([&, k] {
-            ok[k] = run_batch(in->helper[k - 1], frames + cut[k], cut[k + 1] - cut[k], part.data() + cut[k]);
+            ok[k] = run_batch(in->helper[k - 1], frames + cut[k], cut[k + 1] - cut[k], part.data() + cut[k], &chain,
+                              k);
         });
-    ok[0] = run_batch(td, frames, cut[1], res);
+    ok[0] = run_batch(td, frames, cut[1], res, &chain, 0);
     for (auto &t : th) t.join();
     for (int k = 1; k < P; k++)
         if (!ok[k]) {

@@ -714,28 +714,65 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
 // the last-column links of every row (fast/unionfind.c:89-97), in global
 // memory: a block per band boundary row, then a thread per row for the
 // last column.
+#define BJ_CAP 4096  // runs of the two rows staged at once
 __global__ void __launch_bounds__(256) k_band_join(const FrameDesc *frames, const uint8_t *thr, RunArrays runs,
                                                    const uint32_t *row_nruns) {
+    __shared__ uint32_t s_se[BJ_CAP];
+    __shared__ uint8_t s_v[BJ_CAP];
     const FrameDesc f = frames[blockIdx.y];
+    const int tid = threadIdx.x;
     const int nband = (f.qh + UB_ROWS - 1) / UB_ROWS;
     for (int b = 1 + blockIdx.x; b < nband; b += gridDim.x) {
         const int64_t y = (int64_t)b * UB_ROWS;
         const int64_t cur = f.node_off + y * f.qw, prev = cur - f.qw;
-        const int64_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
-        for (int64_t i = threadIdx.x; i < ncur; i += blockDim.x) {
-            const int64_t a0 = runs.start[cur + i], a1 = runs.end[cur + i];
-            const uint8_t v = runs.v[cur + i];
-            int64_t lo = 0, hi = nprev;
+        const uint32_t ncur = row_nruns[f.row0 + y], nprev = row_nruns[f.row0 + y - 1];
+        const uint32_t L = ncur + nprev;  // staged: the row above [0, nprev), this row [nprev, L)
+        const bool staged = L <= BJ_CAP;
+        __syncthreads();
+        if (staged)
+            for (uint32_t l = tid; l < L; l += blockDim.x) {
+                const int64_t node = l < nprev ? prev + l : cur + (l - nprev);
+                s_se[l] = (uint32_t)runs.start[node] | (uint32_t)runs.end[node] << 16;
+                s_v[l] = runs.v[node];
+            }
+        __syncthreads();
+        auto se_at = [&](uint32_t l) -> uint32_t {
+            if (staged) return s_se[l];
+            const int64_t node = l < nprev ? prev + l : cur + (l - nprev);
+            return (uint32_t)runs.start[node] | (uint32_t)runs.end[node] << 16;
+        };
+        auto v_at = [&](uint32_t l) -> uint8_t {
+            if (staged) return s_v[l];
+            return runs.v[l < nprev ? prev + l : cur + (l - nprev)];
+        };
+        // each run of either row: the runs of the other row covering its
+        // start column and the column before (see k_band_union)
+        for (uint32_t l = tid; l < L; l += blockDim.x) {
+            const uint32_t se = se_at(l);
+            const int a0 = (int)(se & 0xffffu), a1 = (int)(se >> 16);
+            const uint8_t v = v_at(l);
+            const uint32_t ob = l < nprev ? nprev : 0, oe = l < nprev ? L : nprev;
+            uint32_t lo = ob, hi = oe;
             while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if ((int64_t)runs.end[prev + mid] + 1 < a0)
+                const uint32_t mid = (lo + hi) >> 1;
+                if ((int)(se_at(mid) & 0xffffu) <= a0)
                     lo = mid + 1;
                 else
                     hi = mid;
             }
-            for (int64_t k = lo; k < nprev && (int64_t)runs.start[prev + k] <= a1 + 1; k++)
-                if (runs.v[prev + k] == v && runs_touch(a0, a1, runs.start[prev + k], runs.end[prev + k], v))
-                    uf_unite(runs.parent, (uint32_t)(cur + i), (uint32_t)(prev + k));
+            if (lo == ob) continue;
+            const int64_t node = l < nprev ? prev + l : cur + (l - nprev);
+            // runs_touch as the reference calls it: this row's run, then the
+            // run above (it is not symmetric at column 0)
+            const bool upper = l < nprev;
+            for (uint32_t k = lo - 1, t = 0; t < 2; t++) {
+                const uint32_t sk = se_at(k);
+                const int b0 = (int)(sk & 0xffffu), b1 = (int)(sk >> 16);
+                if (v_at(k) == v && (upper ? runs_touch(b0, b1, a0, a1, v) : runs_touch(a0, a1, b0, b1, v)))
+                    uf_unite(runs.parent, (uint32_t)node, (uint32_t)(k < nprev ? prev + k : cur + (k - nprev)));
+                if ((int)(sk & 0xffffu) != a0 || k == ob) break;
+                k--;  // the run covering a0 - 1
+            }
         }
     }
     for (int64_t y = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; y < f.qh;
