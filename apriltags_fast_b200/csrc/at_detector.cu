@@ -1098,6 +1098,23 @@ at_detector *at_detector_clone(const at_detector *src) {
     return td;
 }
 
+int at_register_host_buffer(void *ptr, size_t bytes) {
+    if (!ptr || bytes == 0) return -1;
+    if (cudaHostRegister(ptr, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return 0;
+}
+
+int at_unregister_host_buffer(void *ptr) {
+    if (!ptr || cudaHostUnregister(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return 0;
+}
+
 int at_detector_set_batch_split(at_detector *td, int pipelines) {
     if (pipelines < 1 || pipelines > AT_BATCH_SPLIT_MAX) return -1;
     td->in->split = pipelines;

@@ -298,12 +298,8 @@ static void stamp_stages(timeprofile_t *tp, const at_timing *t) {
     }
 }
 
-zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig) {
-    zarray_t *detections = zarray_create(sizeof(apriltag_detection_t *));
-    if (zarray_size(td->tag_families) == 0) return detections;
-    if (im_orig->width < 8 || im_orig->height < 8) return detections;
-    if (td->families_changed) sync_families(td);
-
+/* The detector's parameters as the native detector takes them. */
+static void push_params(apriltag_detector_t *td) {
     at_detector *fd = td->fast;
     fd->nthreads = td->nthreads > 0 ? td->nthreads : 1;
     fd->quad_decimate = td->quad_decimate;
@@ -318,17 +314,15 @@ zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig)
     fd->qtp.max_line_fit_mse = td->qtp.max_line_fit_mse;
     fd->qtp.min_white_black_diff = td->qtp.min_white_black_diff;
     fd->qtp.deglitch = td->qtp.deglitch != 0;
+}
 
-    td->tp->utime = utime_now();
-    at_detect(fd, im_orig->buf, im_orig->width, im_orig->height, im_orig->stride);
-    stamp_stages(td->tp, &fd->timing);
-    td->nquads = (uint32_t)fd->nquads;
-    td->nedges = 0;
-    td->nsegments = 0;
-
-    zarray_ensure_capacity(detections, (int)fd->ndetections);
-    for (int64_t i = 0; i < fd->ndetections; i++) {
-        const at_detection *d = &fd->detections[i];
+/* Native detections [first, first + count) as upstream detections: each
+   its own allocation, its H a 3x3 matd, its family the detector's. */
+static zarray_t *to_upstream(apriltag_detector_t *td, const at_detection *dets, int64_t count) {
+    zarray_t *out = zarray_create(sizeof(apriltag_detection_t *));
+    zarray_ensure_capacity(out, (int)count);
+    for (int64_t i = 0; i < count; i++) {
+        const at_detection *d = &dets[i];
         apriltag_detection_t *det = (apriltag_detection_t *)calloc(1, sizeof(apriltag_detection_t));
         zarray_get(td->tag_families, d->family, &det->family);
         det->id = d->id;
@@ -338,9 +332,60 @@ zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig)
         det->c[0] = d->c[0];
         det->c[1] = d->c[1];
         memcpy(det->p, d->p, sizeof det->p);
-        zarray_add(detections, &det);
+        zarray_add(out, &det);
     }
-    return detections;
+    return out;
+}
+
+zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig) {
+    if (zarray_size(td->tag_families) == 0 || im_orig->width < 8 || im_orig->height < 8)
+        return zarray_create(sizeof(apriltag_detection_t *));
+    if (td->families_changed) sync_families(td);
+    push_params(td);
+    at_detector *fd = td->fast;
+    td->tp->utime = utime_now();
+    at_detect(fd, im_orig->buf, im_orig->width, im_orig->height, im_orig->stride);
+    stamp_stages(td->tp, &fd->timing);
+    td->nquads = (uint32_t)fd->nquads;
+    td->nedges = 0;
+    td->nsegments = 0;
+    return to_upstream(td, fd->detections, fd->ndetections);
+}
+
+void apriltag_detector_detect_batch(apriltag_detector_t *td, image_u8_t **ims, int n, zarray_t **results) {
+    if (n <= 0) return;
+    if (zarray_size(td->tag_families) == 0) {
+        for (int i = 0; i < n; i++) results[i] = zarray_create(sizeof(apriltag_detection_t *));
+        return;
+    }
+    if (td->families_changed) sync_families(td);
+    push_params(td);
+    at_detector *fd = td->fast;
+    at_frame *frames = (at_frame *)calloc((size_t)n, sizeof(at_frame));
+    at_frame_result *res = (at_frame_result *)calloc((size_t)n, sizeof(at_frame_result));
+    for (int i = 0; i < n; i++) {
+        /* a frame under 8 px a side is given no detections, as by the
+           single-frame call */
+        const int small = ims[i]->width < 8 || ims[i]->height < 8;
+        frames[i].pixels = ims[i]->buf;
+        frames[i].width = small ? 0 : ims[i]->width;
+        frames[i].height = small ? 0 : ims[i]->height;
+        frames[i].stride = ims[i]->stride;
+        frames[i].family_mask = 0;
+    }
+    td->tp->utime = utime_now();
+    at_detect_batch(fd, frames, n, res);
+    stamp_stages(td->tp, &fd->timing);
+    uint64_t nq = 0;
+    for (int i = 0; i < n; i++) {
+        results[i] = to_upstream(td, fd->detections + res[i].first, res[i].count);
+        nq += (uint64_t)res[i].nquads;
+    }
+    td->nquads = (uint32_t)nq;
+    td->nedges = 0;
+    td->nsegments = 0;
+    free(frames);
+    free(res);
 }
 
 void apriltag_detection_destroy(apriltag_detection_t *det) {

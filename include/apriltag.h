@@ -100,6 +100,12 @@ void apriltag_detector_clear_families(apriltag_detector_t *td);
 void apriltag_detector_destroy(apriltag_detector_t *td);
 /* apriltag.c:152-208: a zarray of apriltag_detection_t *, sorted by id. */
 zarray_t *apriltag_detector_detect(apriltag_detector_t *td, image_u8_t *im_orig);
+/* Not in apriltag.c: n images through one batched pass on the GPU;
+   results[i] gets image i's detections exactly as apriltag_detector_detect
+   would return them (the caller destroys each with
+   apriltag_detections_destroy). td->nquads is the batch's total and td->tp
+   holds the batch's stage times. */
+void apriltag_detector_detect_batch(apriltag_detector_t *td, image_u8_t **ims, int n, zarray_t **results);
 /* apriltag.c:210-229 */
 void apriltag_detection_destroy(apriltag_detection_t *det);
 void apriltag_detections_destroy(zarray_t *detections);

@@ -162,6 +162,15 @@ typedef struct at_frame_result {
    detections, frame by frame; td->ndetections their total. */
 void at_detect_batch(at_detector *td, const at_frame *frames, int64_t n, at_frame_result *results);
 
+/* Page-locks a caller's host buffer for the GPU (cudaHostRegister): frames
+   in it are then copied to the device by DMA straight from it, instead of
+   through the driver's staging of pageable memory. Returns 0, or -1 when
+   the buffer cannot be registered (it is then used as before). A buffer
+   stays registered until at_unregister_host_buffer, which must come before
+   the buffer is freed. */
+int at_register_host_buffer(void *ptr, size_t bytes);
+int at_unregister_host_buffer(void *ptr);
+
 /* How many pipelines at_detect_batch spreads a large batch over (1 to 4;
    3 by default). Each pipeline takes a run of consecutive frames (at least
    10, with about equal pixel counts): the first runs on this detector, the

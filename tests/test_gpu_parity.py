@@ -313,7 +313,16 @@ def test_upstream_api_equals_native(tmp_path, family, bits):
         up = [l[2:] for l in lines if l.startswith("U ")]
         nat = [l[2:] for l in lines if l.startswith("N ")]
         assert up == nat and len(up) > 0
+        # the batch call: each copy of the image gives the single call's
+        # detections, the crop none; the quad count is the batch's total
+        for k in (0, 2, 3):
+            assert [l[3:] for l in lines if l.startswith(f"B{k} ")] == up
+        assert not [l for l in lines if l.startswith("B1 ")]
         nq = [l for l in lines if l.startswith("nquads")][0].split()
+        assert int([l for l in lines if l.startswith("batch nquads")][0].split()[2]) == 3 * int(nq[1])
+        # a page-locked buffer: the same detections
+        assert [l[2:] for l in lines if l.startswith("R ")] == nat
+        assert "registered 0 unregistered 0" in lines
         assert nq[1] == [l for l in lines if l.startswith("native nquads")][0].split()[2]
         assert nq[3] == "9"
         assert "after clear 0" in lines

@@ -2,7 +2,9 @@
    native API (apriltag_fast.h) of the library and prints both detection
    lists in the same exact (%a) form, one line per detection, so that the
    GPU test can compare them; also exercises detections_copy, the family
-   create/destroy pair, remove/clear families and apriltag_to_image.
+   create/destroy pair, remove/clear families, apriltag_to_image, the batch
+   call (the image three times and a crop too small to hold a tag) and a
+   page-locked image buffer.
    usage: upstream_detect image.pgm family bits */
 #include <stdio.h>
 #include <string.h>
@@ -52,6 +54,22 @@ int main(int argc, char **argv) {
         print_det("U", d->id, d->hamming, d->decision_margin, d->H->data, d->c, (const double (*)[2])d->p);
     }
     printf("nquads %u stamps %d\n", td->nquads, zarray_size(td->tp->stamps));
+    /* the same image three times and a 4x4 crop through the batch call */
+    image_u8_t tiny = {4, 4, im->stride, im->buf};
+    image_u8_t *batch[4] = {im, &tiny, im, im};
+    zarray_t *bres[4];
+    apriltag_detector_detect_batch(td, batch, 4, bres);
+    for (int k = 0; k < 4; k++) {
+        for (int i = 0; i < zarray_size(bres[k]); i++) {
+            apriltag_detection_t *d;
+            zarray_get(bres[k], i, &d);
+            char tag[8];
+            snprintf(tag, sizeof tag, "B%d", k);
+            print_det(tag, d->id, d->hamming, d->decision_margin, d->H->data, d->c, (const double (*)[2])d->p);
+        }
+        apriltag_detections_destroy(bres[k]);
+    }
+    printf("batch nquads %u\n", td->nquads);
     apriltag_detections_destroy(copy);
     apriltag_detections_destroy(dets);
     apriltag_detector_clear_families(td);
@@ -67,6 +85,14 @@ int main(int argc, char **argv) {
         print_det("N", d->id, d->hamming, d->decision_margin, d->H, d->c, d->p);
     }
     printf("native nquads %lld\n", (long long)fd->nquads);
+    /* the image's buffer page-locked: the same detections */
+    const int reg = at_register_host_buffer(im->buf, (size_t)im->stride * im->height);
+    at_detect(fd, im->buf, im->width, im->height, im->stride);
+    for (int64_t i = 0; i < fd->ndetections; i++) {
+        const at_detection *d = &fd->detections[i];
+        print_det("R", d->id, d->hamming, d->decision_margin, d->H, d->c, d->p);
+    }
+    printf("registered %d unregistered %d\n", reg, at_unregister_host_buffer(im->buf));
 
     image_u8_t *tagim = apriltag_to_image(fam, 0);
     printf("tag image %d %d\n", tagim->width, tagim->height);
