@@ -214,10 +214,13 @@ def run_reference(args):
 
 # the kernels of each stage (one launch of each per batch)
 STAGE_KERNELS = {
+    "threshold": "threshold stage: k_decimate_threshold (decimate 2, tile max/min and threshold fused)",
+    "unionfind": "unionfind stage: k_row_runs, k_band_union, k_band_join, k_row_sums, k_labels_w",
+    "clusters": "clusters stage: k_point_scan, k_cluster_collect, k_pair_*, k_cluster_span, k_scan2_*, "
+                "k_seg_zero/fill/scan, k_point_place",
     "fit_quads": "fit_quads stage: k_fit_classify, k_fit_order, k_fit_warp<4/8/16>, k_fit_quads<128/512>",
-    "clusters": "clusters stage: k_point_count, k_point_emit, k_cluster_hash/collect/rank/assign, radix sort",
-    "unionfind": "unionfind stage: k_row_runs, k_row_union, k_row_sums, k_labels",
     "decode": "decode stage: k_refine, k_quad_homography, k_decode",
+    "reconcile": "reconcile stage: k_ref_targets/mark/cut/local/frontier/band/resolve, k_finalize, k_output_*",
 }
 
 
@@ -480,8 +483,9 @@ def main():
     alg = {
         "decimate": 0,                                 # fused into the threshold stage at decimate 2
         "threshold": B * (W * H + 2 * qpx),            # read the frame; write the quad and threshold images
-        "unionfind": B * (qpx + 13 * qpx // 4),        # threshold image + runs and nodes (13 B a node)
-        "clusters": int(pts * (8 + 8 + 2 * 16)),       # points written, then sorted (key + value)
+        "unionfind": B * 5 * qpx,                      # read the threshold image; write the labels (4 B)
+        "clusters": B * 5 * qpx + int(pts * 16),       # read threshold and labels; a 4-byte record per
+                                                       # point written and read, the 8-byte point written
         "fit_quads": int(pts * 8),                     # each boundary point read once
         "decode": B * 24 * 4 * 64 * 25 * 8,            # refine samples along the quads' edges
         "reconcile": B * 24 * 168,
