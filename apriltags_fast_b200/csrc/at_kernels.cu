@@ -230,55 +230,69 @@ __global__ void __launch_bounds__(DT_THREADS) k_decimate_threshold(const FrameDe
     for (int i = threadIdx.x; i < npair * ntr; i += DT_THREADS) {
         const int r = i / npair, tp = px0 + 2 * (i - r * npair);
         const int ty = ty0 + r;
-        uint32_t q[2][4][4];  // [tile][row][col]
+        uint32_t qw4[2][4];  // [tile][row]: the tile row's 4 quad pixels as bytes of a word
+        if (al16 && tp + 1 < tw && 4 * tp + 8 <= xv) {
+            // 16 input bytes of two rows give 8 quad pixels: the byte average
+            // of the rows, then of even and odd columns (the reference's two
+            // rounded averages of its AVX2 path)
 #pragma unroll
-        for (int dy = 0; dy < 4; dy++) {
-            const uint8_t *r0 = img + (int64_t)(8 * ty + 2 * dy) * st + 8 * tp, *r1 = r0 + st;
-            uint32_t a[4], b[4];  // 16 input bytes of each row, as words
-            if (al16 && tp + 1 < tw) {
-                const uint4 u = *reinterpret_cast<const uint4 *>(r0), v = *reinterpret_cast<const uint4 *>(r1);
-                a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w;
-                b[0] = v.x, b[1] = v.y, b[2] = v.z, b[3] = v.w;
-            } else {
-                const int nb = tp + 1 < tw ? 16 : 8;
-#pragma unroll
-                for (int w = 0; w < 4; w++) {
-                    a[w] = b[w] = 0;
-#pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        if (4 * w + k < nb) {
-                            a[w] |= (uint32_t)r0[4 * w + k] << (8 * k);
-                            b[w] |= (uint32_t)r1[4 * w + k] << (8 * k);
-                        }
-                }
+            for (int dy = 0; dy < 4; dy++) {
+                const uint8_t *r0 = img + (int64_t)(8 * ty + 2 * dy) * st + 8 * tp;
+                const uint4 u = *reinterpret_cast<const uint4 *>(r0), v = *reinterpret_cast<const uint4 *>(r0 + st);
+                const uint32_t a0 = __vavgu4(u.x, v.x), a1 = __vavgu4(u.y, v.y), a2 = __vavgu4(u.z, v.z),
+                               a3 = __vavgu4(u.w, v.w);
+                qw4[0][dy] = __vavgu4(__byte_perm(a0, a1, 0x6420), __byte_perm(a0, a1, 0x7531));
+                qw4[1][dy] = __vavgu4(__byte_perm(a2, a3, 0x6420), __byte_perm(a2, a3, 0x7531));
             }
+        } else {
 #pragma unroll
-            for (int o = 0; o < 8; o++) {  // quad pixel 4 tp + o of row 4 ty + dy
-                const uint32_t w0 = a[o >> 1], w1 = b[o >> 1];
-                const int sh = 16 * (o & 1);
-                q[o >> 2][dy][o & 3] = box2(4 * tp + o, xv, (w0 >> sh) & 255, (w0 >> (sh + 8)) & 255,
-                                            (w1 >> sh) & 255, (w1 >> (sh + 8)) & 255);
+            for (int dy = 0; dy < 4; dy++) {
+                const uint8_t *r0 = img + (int64_t)(8 * ty + 2 * dy) * st + 8 * tp, *r1 = r0 + st;
+                uint32_t a[4], b[4];  // 16 input bytes of each row, as words
+                if (al16 && tp + 1 < tw) {
+                    const uint4 u = *reinterpret_cast<const uint4 *>(r0), v = *reinterpret_cast<const uint4 *>(r1);
+                    a[0] = u.x, a[1] = u.y, a[2] = u.z, a[3] = u.w;
+                    b[0] = v.x, b[1] = v.y, b[2] = v.z, b[3] = v.w;
+                } else {
+                    const int nb = tp + 1 < tw ? 16 : 8;
+#pragma unroll
+                    for (int w = 0; w < 4; w++) {
+                        a[w] = b[w] = 0;
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if (4 * w + k < nb) {
+                                a[w] |= (uint32_t)r0[4 * w + k] << (8 * k);
+                                b[w] |= (uint32_t)r1[4 * w + k] << (8 * k);
+                            }
+                    }
+                }
+                qw4[0][dy] = qw4[1][dy] = 0;
+#pragma unroll
+                for (int o = 0; o < 8; o++) {  // quad pixel 4 tp + o of row 4 ty + dy
+                    const uint32_t w0 = a[o >> 1], w1 = b[o >> 1];
+                    const int sh = 16 * (o & 1);
+                    qw4[o >> 2][dy] |= box2(4 * tp + o, xv, (w0 >> sh) & 255, (w0 >> (sh + 8)) & 255, (w1 >> sh) & 255,
+                                            (w1 >> (sh + 8)) & 255)
+                                       << (8 * (o & 3));
+                }
             }
         }
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const int tx = tp + k;
             if (tx < tx0 || tx > tx1) continue;
-            uint32_t hi = 0, lo = 255;
+            uint32_t mx = qw4[k][0], mn = qw4[k][0];
 #pragma unroll
-            for (int dy = 0; dy < 4; dy++)
-#pragma unroll
-                for (int dx = 0; dx < 4; dx++) {
-                    hi = max(hi, q[k][dy][dx]);
-                    lo = min(lo, q[k][dy][dx]);
-                }
-            s_tmax[ty - ty0][tx - tx0] = (uint8_t)hi;
-            s_tmin[ty - ty0][tx - tx0] = (uint8_t)lo;
+            for (int dy = 1; dy < 4; dy++) {
+                mx = __vmaxu4(mx, qw4[k][dy]);
+                mn = __vminu4(mn, qw4[k][dy]);
+            }
+            s_tmax[ty - ty0][tx - tx0] = (uint8_t)max(max(mx & 255u, mx >> 8 & 255u), max(mx >> 16 & 255u, mx >> 24));
+            s_tmin[ty - ty0][tx - tx0] = (uint8_t)min(min(mn & 255u, mn >> 8 & 255u), min(mn >> 16 & 255u, mn >> 24));
             if (ty >= cy0 && ty < cy1 && tx >= cx0 && tx < cx1) {
 #pragma unroll
                 for (int dy = 0; dy < 4; dy++)
-                    *reinterpret_cast<uint32_t *>(&s_q[4 * (ty - cy0) + dy][4 * (tx - cx0)]) =
-                        q[k][dy][0] | q[k][dy][1] << 8 | q[k][dy][2] << 16 | q[k][dy][3] << 24;
+                    *reinterpret_cast<uint32_t *>(&s_q[4 * (ty - cy0) + dy][4 * (tx - cx0)]) = qw4[k][dy];
             }
         }
     }
@@ -307,6 +321,22 @@ __global__ void __launch_bounds__(DT_THREADS) k_decimate_threshold(const FrameDe
         const int y = y0 + i / nseg, xs = x0 + 16 * (i % nseg);
         const int n = min(16, x1 - xs);
         const bool whole_tiles = y < 4 * th;
+        if (st16 && n == 16 && whole_tiles && xs + 16 <= 4 * tw) {
+            // 16 pixels of 4 cells, 4 at a time: above the cell's threshold
+            // 255, else 0; a flat cell 127
+            const uint4 q = *reinterpret_cast<const uint4 *>(&s_q[y - y0][xs - x0]);
+            const uint32_t qa[4] = {q.x, q.y, q.z, q.w};
+            uint32_t t4[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t c = s_cell[(y >> 2) - cy0][(xs >> 2) - cx0 + k];
+                t4[k] = (c & 256u) ? 0x7f7f7f7fu : __vcmpgtu4(qa[k], (c & 255u) * 0x01010101u);
+            }
+            const int64_t o = f.q_off + (int64_t)y * qw + xs;
+            *reinterpret_cast<uint4 *>(qim + o) = q;
+            *reinterpret_cast<uint4 *>(thr + o) = make_uint4(t4[0], t4[1], t4[2], t4[3]);
+            continue;
+        }
         uint32_t qv[4] = {0, 0, 0, 0}, tv[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int o = 0; o < 16; o++) {
