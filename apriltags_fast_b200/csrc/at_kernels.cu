@@ -938,14 +938,16 @@ __global__ void __launch_bounds__(LAB_THREADS) k_labels(const FrameDesc *frames,
 
 // The same labels with a warp per row (8 rows a block, for batches large
 // enough to fill the GPU that way): the run starting at each column staged
-// in the warp's slice of shared memory, a max-scan 32 columns at a time
-// (carried across chunks), and each pixel's label read through its run's
-// root (the L1 cache holds the few roots of a row). Rows wider than
+// in the warp's slice of shared memory, then 128 columns at a time, 4 a
+// lane: a max-scan gives each column its run (carried across chunks), the
+// label is read through the run's root (the L1 cache holds the few roots of
+// a row; a lane's 4 pixels usually share one run), and a pixel that no
+// stored run covers is a 127 of the threshold image. Rows wider than
 // LW_CAP columns search the runs per pixel instead.
 #define LW_CAP 2048
-__global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const RunArrays runs,
+__global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const uint8_t *thr, const RunArrays runs,
                                                   const uint32_t *row_nruns, uint32_t *lab, int32_t min_px) {
-    __shared__ uint16_t s_run[8][LW_CAP];
+    __shared__ __align__(16) uint16_t s_run[8][LW_CAP + 8];
     const FrameDesc f = frames[blockIdx.y];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int qw = (int)f.qw, W = qw - 1;
@@ -954,6 +956,7 @@ __global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const
         const int64_t base = f.node_off + (int64_t)y * qw;
         const int nr = (int)row_nruns[f.row0 + y];
         uint32_t *out = lab + f.q_off + (int64_t)y * qw;
+        const uint8_t *row = thr + f.q_off + (int64_t)y * qw;
         auto label_of = [&](int i) -> uint32_t {
             const uint32_t r = runs.parent[base + i];
             return (int64_t)runs.px[r] >= min_px ? runs.minid[r] : AT_NOK;
@@ -976,22 +979,53 @@ __global__ void __launch_bounds__(256) k_labels_w(const FrameDesc *frames, const
             }
             continue;
         }
-        for (int x = lane; x < W; x += 32) sr[x] = 0;
+        const int Wp = (W + 3) & ~3;
+        for (int x = lane; x < Wp; x += 32) sr[x] = 0;
         __syncwarp();
         for (int i = lane; i < nr; i += 32) sr[runs.start[base + i]] = (uint16_t)(i + 1);
         __syncwarp();
+        // 16-byte stores when the row and the label array allow
+        const bool v4 = ((((uintptr_t)out) | ((uintptr_t)row)) & 15) == 0;
         uint32_t carry = 0;
-        for (int x0 = 0; x0 < W; x0 += 32) {
-            const int x = x0 + lane;
-            uint32_t v = x < W ? sr[x] : 0u;
+        for (int x0 = 0; x0 < W; x0 += 128) {
+            const int x = x0 + 4 * lane;
+            const uint2 pr = x < Wp ? *reinterpret_cast<const uint2 *>(sr + x) : make_uint2(0, 0);
+            uint32_t m[4] = {pr.x & 0xffffu, pr.x >> 16, pr.y & 0xffffu, pr.y >> 16};
+            m[1] = max(m[1], m[0]);
+            m[2] = max(m[2], m[1]);
+            m[3] = max(m[3], m[2]);
+            uint32_t incl = m[3];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v = max(v, t);
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl = max(incl, t);
             }
-            v = max(v, carry);
-            carry = __shfl_sync(0xffffffffu, v, 31);
-            if (x < W) out[x] = v && x <= (int)runs.end[base + v - 1] ? label_of((int)v - 1) : AT_NOK;
+            uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) excl = 0;
+            excl = max(excl, carry);
+            carry = max(carry, __shfl_sync(0xffffffffu, incl, 31));
+            uint32_t l4[4];
+            uint32_t prev_run = 0, prev_lab = AT_NOK;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t v = max(m[k], excl);
+                uint32_t l = AT_NOK;
+                if (x + k < W && v) {
+                    if (v != prev_run) {
+                        prev_run = v;
+                        prev_lab = label_of((int)v - 1);
+                    }
+                    l = row[x + k] != 127 ? prev_lab : AT_NOK;
+                }
+                l4[k] = l;
+            }
+            if (v4 && x + 4 <= W) {
+                *reinterpret_cast<uint4 *>(out + x) = make_uint4(l4[0], l4[1], l4[2], l4[3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (x + k < W) out[x + k] = l4[k];
+            }
         }
         __syncwarp();
     }
@@ -3891,7 +3925,7 @@ int launch_segment(const Launch &L, const FrameDesc *frames, const uint8_t *thr,
         frames, thr, runs, row_nruns);
     k_row_sums<<<rg, 256, 0, L.stream>>>(frames, runs, row_nruns);
     if (warp_rows(L))
-        k_labels_w<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
+        k_labels_w<<<row_warp_grid(L), 256, 0, L.stream>>>(frames, thr, runs, row_nruns, lab, min_px);
     else
         k_labels<<<rg, LAB_THREADS, 0, L.stream>>>(frames, runs, row_nruns, lab, min_px);
     return 5;
