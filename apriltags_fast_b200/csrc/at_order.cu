@@ -858,7 +858,7 @@ __global__ void __launch_bounds__(256) k_ref_local(const FrameDesc *frames, RefO
 // of one band's summaries (two of them, the next band's copies landing
 // while this band is worked on).
 struct FrontArrays {
-    uint32_t *f_se, *s_Z, *par, *Z, *tot, *key, *bk;
+    uint32_t *f_se, *s_Z, *par, *Z, *tot, *key, *bk, *cmin, *trng;
     uint16_t *f_slot;
     uint8_t *f_v;
 };
@@ -883,6 +883,8 @@ __host__ __device__ inline size_t ref_front_carve(uint8_t *base, int64_t capr, F
     a.tot = (uint32_t *)take(4 * cape);
     a.key = (uint32_t *)take(4 * (cape + capr + 1));
     a.bk = (uint32_t *)take(4 * capr);
+    a.cmin = (uint32_t *)take(4 * (capr + 1));
+    a.trng = (uint32_t *)take(4 * capr);
     a.f_slot = (uint16_t *)take(2 * capr);
     a.f_v = take(capr);
     if (A) *A = a;
@@ -979,7 +981,11 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
             A.Z[e] = e < m ? A.s_Z[e] : S.px[e - m];
         }
         for (int64_t e = tid; e < E + nnon; e += nt) A.key[e] = REF_KNONE;
+        for (int64_t c = tid; c < ntop; c += nt) A.cmin[c] = 0xffffffffu;
         __syncthreads();
+        // each top run's touching runs above (first and last; the runs of
+        // its value between them touch it too), and each band component's
+        // smallest touching slot
         const int64_t rt = fd.node_off + (int64_t)d0.x * fd.qw;
         for (int64_t j = tid; j < n0; j += nt) {
             const uint64_t te = S.top_tl[j];
@@ -987,17 +993,32 @@ __global__ void __launch_bounds__(128) k_ref_frontier(const FrameDesc *frames, R
             const uint8_t v = (uint8_t)(te >> 48);
             const int64_t a0 = se & 0xffffu, a1 = se >> 16;
             const uint32_t c = S.top_c[j];
-            uint32_t klo = 0xffffu, khi = 0;
+            uint32_t klo = 0xffffu, khi = 0, smin = 0xffffffffu;
             if (nf > 0)
                 for (uint32_t k = first_reaching(A.f_se, 0, (uint32_t)nf, a0);
                      k < nf && (int64_t)(A.f_se[k] & 0xffffu) <= a1 + 1; k++)
                     if (A.f_v[k] == v && runs_touch(a0, a1, A.f_se[k] & 0xffffu, A.f_se[k] >> 16, v)) {
-                        pu_unite(A.par, A.f_slot[k], (uint32_t)(m + c));
+                        smin = min(smin, (uint32_t)A.f_slot[k]);
                         if (klo == 0xffffu) klo = k;
                         khi = k;
                     }
-            // the runs above that this run touches, for the replay
-            ref.tch[rt + j] = klo == 0xffffu ? 0xffffffffu : klo | khi << 16;
+            if (smin != 0xffffffffu) atomicMin(A.cmin + c, smin);
+            const uint32_t r = klo == 0xffffu ? 0xffffffffu : klo | khi << 16;
+            A.trng[j] = r;
+            ref.tch[rt + j] = r;  // for the replay
+        }
+        __syncthreads();
+        // a component hangs under its smallest slot; the other slots it
+        // reaches are joined to that one (the only unions left)
+        for (int64_t c = tid; c < ntop; c += nt)
+            if (A.cmin[c] != 0xffffffffu) A.par[m + c] = A.cmin[c];
+        for (int64_t j = tid; j < n0; j += nt) {
+            const uint32_t r = A.trng[j];
+            if (r == 0xffffffffu) continue;
+            const uint32_t s0 = A.cmin[S.top_c[j]];
+            const uint8_t v = (uint8_t)(S.top_tl[j] >> 48);
+            for (uint32_t k = r & 0xffffu; k <= (r >> 16); k++)
+                if (A.f_v[k] == v && A.f_slot[k] != s0) pu_unite(A.par, A.f_slot[k], s0);
         }
         __syncthreads();
         for (int64_t e0 = 0; e0 < E; e0 += nt) {
