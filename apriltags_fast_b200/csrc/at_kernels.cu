@@ -1546,12 +1546,13 @@ __device__ double block_select_desc(const double *e, int64_t n, uint32_t r, uint
 
 // Two size classes of clusters, one kernel template: 128 threads for
 // clusters of at most FIT_SMALL points (everything staged in shared
-// memory), 512 threads for the larger ones (dynamic shared memory; sorts
+// memory), FIT_LARGE_NT threads for the larger ones (dynamic shared memory; sorts
 // beyond FIT_LARGE_SORT points fall back to global scratch).
 #define FIT_SMALL 1024
-#define FIT_LARGE_SORT 14336
+#define FIT_LARGE_SORT 6144
 #define FIT_CHUNK_SMALL 256
-#define FIT_CHUNK_LARGE 1024
+#define FIT_CHUNK_LARGE 512
+#define FIT_LARGE_NT 256  // threads of the largest class's blocks (two blocks an SM)
 
 // dynamic shared memory of one block of the fit kernel
 // Shared memory of the block fit kernel for clusters of up to sort_cap
@@ -1669,7 +1670,7 @@ extern "C" int at_fit_prof_copy(void *dst, int n) {
 #endif
 
 template <int NT>
-__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : 1)) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
+__global__ void __launch_bounds__(NT, (NT <= 128 ? 4 : NT <= 256 ? 2 : 1)) k_fit_quads(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
                                                    const uint64_t *pts, const uint32_t *cstart,
                                                    const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                    FitScratch scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err,
@@ -3989,9 +3990,9 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
                       int64_t npoints, const FitScratch &scr, GpuQuad *quads, uint32_t *quad_ok, uint32_t *err) {
     if (nclusters <= 0) return;
     const size_t small = fit_smem_bytes(FIT_SMALL, FIT_CHUNK_SMALL, 128 / 32),
-                 large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE, 512 / 32);
+                 large = fit_smem_bytes(FIT_LARGE_SORT, FIT_CHUNK_LARGE, FIT_LARGE_NT / 32);
     cudaFuncSetAttribute(k_fit_quads<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small);
-    cudaFuncSetAttribute(k_fit_quads<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
+    cudaFuncSetAttribute(k_fit_quads<FIT_LARGE_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)large);
     cudaFuncSetAttribute(k_fit_order, cudaFuncAttributeMaxDynamicSharedMemorySize, FIT_ORDER_CAP * 8);
     const int mm = prm.max_nmaxima > 4 ? prm.max_nmaxima : 4;
     // the size classes' lists, the two block classes' largest first
@@ -4009,8 +4010,9 @@ void launch_fit_quads(cudaStream_t s, cudaStream_t side, cudaStream_t side2, cud
     cudaStreamWaitEvent(side3, fork, 0);
     k_fit_order<<<1, 1024, FIT_ORDER_CAP * 8, side>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 4);
     k_fit_order<<<1, 1024, FIT_ORDER_CAP * 8, side2>>>(cstart, nclusters, npoints, scr.lists, scr.counts, 3);
-    const unsigned nbig = (unsigned)(nclusters < 148 ? nclusters : 148);
-    k_fit_quads<512><<<nbig, 512, large, side>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
+    // two blocks an SM: one cluster's serial steps overlap the other's
+    const unsigned nbig = (unsigned)(nclusters < 2 * 148 ? nclusters : 2 * 148);
+    k_fit_quads<FIT_LARGE_NT><<<nbig, FIT_LARGE_NT, large, side>>>(frames, prm, qim, pts, cstart, cframe, nclusters, npoints, scr,
                                                  quads, quad_ok, err, scr.lists + 4 * nclusters, scr.counts + 4,
                                                  scr.counts + FIT_NCLASS + 4, FIT_LARGE_SORT, FIT_CHUNK_LARGE);
     cudaEventRecord(join, side);
