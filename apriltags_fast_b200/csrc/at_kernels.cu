@@ -625,7 +625,8 @@ __global__ void __launch_bounds__(256) k_row_union(const FrameDesc *frames, cons
 // same pairs are joined as by k_row_union, so the partition is the same. A
 // band with more than UB_CAP runs joins its rows in global memory instead.
 #define UB_ROWS 8
-#define UB_CAP 4608
+#define UB_CAP 3072
+#define UB_PAIRS 3072  // touching pairs listed per band, at most
 
 __device__ __forceinline__ uint32_t lu_find(volatile uint32_t *par, uint32_t x) {
     uint32_t p = par[x];
@@ -660,7 +661,10 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
     __shared__ uint8_t s_v[UB_CAP];
     __shared__ uint8_t s_row[UB_CAP];
     __shared__ uint32_t s_roff[UB_ROWS + 1];
+    __shared__ uint32_t s_pair[UB_PAIRS];  // touching pairs: run | run above << 16
+    __shared__ uint32_t s_npair;
     static_assert(UB_ROWS <= 32, "one warp scans the band's row counts");
+    static_assert(UB_CAP <= 65536, "band-local run ids fit 16 bits");
     const FrameDesc f = frames[blockIdx.y];
     const int tid = threadIdx.x;
     const int nband = (f.qh + UB_ROWS - 1) / UB_ROWS;
@@ -710,7 +714,13 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
             s_row[l] = (uint8_t)r;
         }
         __syncthreads();
-        // the unions of rows 1.. of the band with the row above, in shared memory
+        // the unions of rows 1.. of the band with the row above, in shared
+        // memory: the touching pairs listed first (a thread per run), then
+        // one union per pair, the pairs spread evenly over the threads (a
+        // run touching many runs above no longer holds its warp); a band
+        // with more pairs than the list holds unites them where found
+        if (tid == 0) s_npair = 0;
+        __syncthreads();
         for (uint32_t l = s_roff[1] + tid; l < L; l += blockDim.x) {
             const int r = s_row[l];
             const uint32_t pb = s_roff[r - 1], pe = s_roff[r];
@@ -725,8 +735,17 @@ __global__ void __launch_bounds__(256) k_band_union(const FrameDesc *frames, Run
                     hi = mid;
             }
             for (uint32_t k = lo; k < pe && (int)(s_se[k] & 0xffffu) <= a1 + 1; k++)
-                if (s_v[k] == v && runs_touch(a0, a1, s_se[k] & 0xffffu, s_se[k] >> 16, v)) lu_unite(s_par, l, k);
+                if (s_v[k] == v && runs_touch(a0, a1, s_se[k] & 0xffffu, s_se[k] >> 16, v)) {
+                    const uint32_t p = atomicAdd(&s_npair, 1u);
+                    if (p < UB_PAIRS)
+                        s_pair[p] = l | k << 16;
+                    else
+                        lu_unite(s_par, l, k);
+                }
         }
+        __syncthreads();
+        const uint32_t np = min(s_npair, (uint32_t)UB_PAIRS);
+        for (uint32_t p = tid; p < np; p += blockDim.x) lu_unite(s_par, s_pair[p] & 0xffffu, s_pair[p] >> 16);
         __syncthreads();
         // every node points at its local root (read-only walks)
         for (uint32_t l = tid; l < L; l += blockDim.x) {
