@@ -531,6 +531,20 @@ void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *os
 
 int64_t pair_scan_blocks(int64_t ncl) { return (ncl + SCAN_ITEMS - 1) / SCAN_ITEMS + 1; }
 
+// An exclusive scan of n u32 values into out (n + 1 entries, the total
+// last) with the two-array kernels above, the second array the first
+// again; scratch: scan_u32_scratch(n) values.
+int64_t scan_u32_scratch(int64_t n) { return 2 * ((n + SCAN_ITEMS - 1) / SCAN_ITEMS + 1) + n + 1; }
+
+void launch_scan_u32(cudaStream_t s, const uint32_t *a, int64_t n, uint32_t *out, uint32_t *scratch) {
+    if (n <= 0) return;
+    const int64_t nblk = (n + SCAN_ITEMS - 1) / SCAN_ITEMS;
+    uint32_t *sa = scratch, *sb = scratch + nblk + 1, *ob = scratch + 2 * (nblk + 1);
+    k_scan2_sums<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(a, a, n, sa, sb);
+    k_scan2_top<<<1, 1024, 0, s>>>(sa, sb, nblk);
+    k_scan2_apply<<<(unsigned)nblk, SCAN_THREADS, 0, s>>>(a, a, n, sa, sb, nblk, out, ob);
+}
+
 void launch_point_place(const Launch &L, const FrameDesc *frames, const PointRows &P, const uint32_t *rank_of_slot,
                         const uint32_t *cstart, const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0,
                         int64_t ncl, uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err) {

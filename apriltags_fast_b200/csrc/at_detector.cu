@@ -103,7 +103,7 @@ enum {
     B_QCL, B_CKEY, B_RNEED, B_RNT, B_RTLAB, B_RTPX, B_RTROOT, B_RTLIST, B_RTROW, B_RPRE, B_ROKEY, B_RIDX2, B_RSCR,
     B_RFIN, B_RFINB, B_RBSLOT, B_RBINFO, B_ROUTROOT, B_RBM, B_RBSTART, B_RBWIDE, B_RDESC, B_RNBAND, B_RFSCR, B_RTCH, B_RLTOP, B_RLPX, B_RLBOT,
     B_RLPX2,
-    B_PREC, B_PPSLOT, B_PPCNT, B_PINFO,
+    B_PREC, B_PPSLOT, B_PPCNT, B_PINFO, B_QSCR,
     B_CUB, B_ERR, B_NBUF
 };
 
@@ -670,7 +670,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
         CK(B[B_SMXI].ensure(npts * 4));
         CK(B[B_QUADS].ensure(ncl * sizeof(GpuQuad)));
         CK(B[B_QOK].ensure(ncl * 4));
-        CK(B[B_QSCAN].ensure(ncl * 4));
+        CK(B[B_QSCAN].ensure((ncl + 1) * 4));
+        CK(B[B_QSCR].ensure(scan_u32_scratch(ncl) * 4));
         CK(B[B_FLIST].ensure(ncl * 4 * 5));
         CK(B[B_FCNT].ensure(64));
         FitScratch scr{B[B_SKEYS].as<uint64_t>(), B[B_SSKEY].as<uint64_t>(), B[B_SSVAL].as<uint32_t>(),
@@ -684,10 +685,8 @@ static bool run_batch(at_detector *td, const at_frame *frames, int64_t n, at_fra
                          (int64_t)npts, scr, B[B_QUADS].as<GpuQuad>(), qok, B[B_ERR].as<uint32_t>());
         in->launches += 8;
         CK(cudaGetLastError());
-        if (!cub_call(in, [&](void *t, size_t &b) {
-                return cub::DeviceScan::ExclusiveSum(t, b, qok, qscan, ncl, st);
-            }))
-            return false;
+        launch_scan_u32(st, qok, ncl, qscan, B[B_QSCR].as<uint32_t>());
+        in->launches += 3;
         // the quads in cluster order (grouped by frame), their count and each
         // frame's first quad stay on the device: decode is sized by ncl
         CK(B[B_QUADSC].ensure(ncl * sizeof(GpuQuad)));

@@ -93,6 +93,8 @@ void launch_pair_order(cudaStream_t s, const uint64_t *okeys, const uint32_t *os
                        uint64_t *skeys, uint32_t *sslots, uint32_t *rank_of_slot, uint32_t *ccount, uint32_t *cspan,
                        uint32_t *cy0, int32_t *cframe, uint32_t *cstart, uint32_t *spanoff);
 int64_t pair_scan_blocks(int64_t ncl);
+int64_t scan_u32_scratch(int64_t n);
+void launch_scan_u32(cudaStream_t s, const uint32_t *a, int64_t n, uint32_t *out, uint32_t *scratch);
 void launch_point_place(const Launch &L, const FrameDesc *frames, const PointRows &P, const uint32_t *rank_of_slot,
                         const uint32_t *cstart, const uint32_t *spanoff, const uint32_t *cspan, const uint32_t *cy0,
                         int64_t ncl, uint32_t *seg, int64_t cap, uint64_t *out, int64_t npts, uint32_t *err);
