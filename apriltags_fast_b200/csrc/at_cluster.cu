@@ -80,7 +80,7 @@ __device__ inline RowPairs row_pairs(uint8_t *base, int nd_cap) {
 // and, with its points in the row, into the row's pair list. Any capacity
 // exceeded (pairs of a row, records of a row, probes of the pair table)
 // sets *full and the batch takes the sorting path instead.
-__global__ void __launch_bounds__(256) k_point_scan(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
+__global__ void __launch_bounds__(256, 5) k_point_scan(const FrameDesc *frames, const uint8_t *thr, const uint32_t *lab,
                                                     int nb, PairTable T, PointRows P, uint32_t *full,
                                                     unsigned long long *npoints) {
     extern __shared__ __align__(16) uint8_t s_mem[];
