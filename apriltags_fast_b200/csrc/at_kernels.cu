@@ -2433,7 +2433,7 @@ __device__ void warp_radix_sort32(uint32_t *ka, uint16_t *va, uint32_t *kb, uint
 }
 
 template <int R>
-__global__ void __launch_bounds__(FIT_WPB * 32) k_fit_warp(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
+__global__ void __launch_bounds__(FIT_WPB * 32, 12) k_fit_warp(const FrameDesc *frames, GpuParams prm, const uint8_t *qim,
                                                           const uint64_t *pts, const uint32_t *cstart,
                                                           const int32_t *cframe, int64_t nclusters, int64_t npoints,
                                                           const uint32_t *list, const uint32_t *count,
