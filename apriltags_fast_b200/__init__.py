@@ -424,3 +424,162 @@ def _image_arg(img, stride):
         a = np.ascontiguousarray(a)
     h, w = a.shape
     return C.c_void_p(a.ctypes.data), w, h, int(stride or a.strides[0])
+
+
+# --------------------------------------------------------------------------
+# JPEG input (csrc/at_jpeg.cu): baseline JPEG decoded on the GPU, pixels and
+# error codes as the reference's common/pjpeg.c gives them.
+
+PJPEG_MJPEG = 2
+JPEG_ERRORS = ("OKAY", "FILE", "DQT", "SOF", "DHT", "SOS", "MISSING_DHT", "DRI", "RESET", "EOF", "UNSUPPORTED")
+
+
+class _PJComponent(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("stride", C.c_uint32),
+                ("data", C.POINTER(C.c_uint8)), ("id", C.c_uint8), ("hv", C.c_uint8), ("scalex", C.c_uint8),
+                ("scaley", C.c_uint8), ("tq", C.c_uint8), ("tda", C.c_uint8)]
+
+
+class _PJ(C.Structure):
+    _fields_ = [("error", C.c_int), ("width", C.c_uint32), ("height", C.c_uint32), ("ncomponents", C.c_int),
+                ("components", C.POINTER(_PJComponent))]
+
+
+class _ImageU8x3(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("stride", C.c_int32), ("buf", C.POINTER(C.c_uint8))]
+
+
+_jpeg_bound = False
+
+
+def _jpeg_lib():
+    global _jpeg_bound
+    L = lib()
+    if not _jpeg_bound:
+        L.at_jpeg_create.restype = C.c_void_p
+        L.at_jpeg_destroy.argtypes = [C.c_void_p]
+        L.at_jpeg_info.argtypes = [C.c_char_p, C.c_int64, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_int32)]
+        L.at_jpeg_info.restype = C.c_int
+        L.at_jpeg_decode_gray.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_int64),
+                                          C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_int32,
+                                          C.POINTER(C.c_int32)]
+        L.at_jpeg_decode_gray.restype = C.c_int
+        L.at_jpeg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.at_jpeg_set_sub_bits.argtypes = [C.c_void_p, C.c_int32]
+        L.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
+        L.pjpeg_create_from_buffer.restype = C.POINTER(_PJ)
+        L.pjpeg_destroy.argtypes = [C.POINTER(_PJ)]
+        L.pjpeg_to_u8x3_baseline.argtypes = [C.POINTER(_PJ)]
+        L.pjpeg_to_u8x3_baseline.restype = C.POINTER(_ImageU8x3)
+        L.image_u8x3_destroy.argtypes = [C.POINTER(_ImageU8x3)]
+        _jpeg_bound = True
+    return L
+
+
+def jpeg_info(buf: bytes, flags: int = 0):
+    """(error, width, height, components) of the gray frame a decode gives."""
+    L = _jpeg_lib()
+    w, h, n = C.c_int32(), C.c_int32(), C.c_int32()
+    e = L.at_jpeg_info(buf, len(buf), flags, C.byref(w), C.byref(h), C.byref(n))
+    return e, w.value, h.value, n.value
+
+
+class JpegDecoder:
+    """Decodes batches of baseline JPEGs on the GPU into gray frames
+    (component 0 cropped to the image, as pjpeg_to_u8_baseline gives it)."""
+
+    def __init__(self, sub_bits: int | None = None):
+        self._L = _jpeg_lib()
+        self._d = self._L.at_jpeg_create()
+        if not self._d:
+            raise RuntimeError("at_jpeg_create failed (no CUDA device?)")
+        if sub_bits is not None and self._L.at_jpeg_set_sub_bits(self._d, sub_bits):
+            raise ValueError("sub_bits must be a multiple of 32 in [64, 65536]")
+
+    def _call(self, bufs, dsts, strides, on_device, flags):
+        n = len(bufs)
+        cb = (C.c_char_p * n)(*bufs)
+        cl = (C.c_int64 * n)(*[len(b) for b in bufs])
+        cd = (C.c_void_p * n)(*dsts)
+        cs = (C.c_int64 * n)(*strides)
+        errs = (C.c_int32 * n)()
+        r = self._L.at_jpeg_decode_gray(self._d, n, cb, cl, flags, cd, cs, int(on_device), errs)
+        if r < 0:
+            raise RuntimeError("at_jpeg_decode_gray: CUDA error")
+        return list(errs)
+
+    def decode(self, bufs, flags: int = 0):
+        """Host numpy frames (None where an image failed) and error codes."""
+        infos = [jpeg_info(b, flags) for b in bufs]
+        outs = [np.zeros((max(h, 1), max(w, 1)), np.uint8) if e == 0 else np.zeros((1, 1), np.uint8)
+                for e, w, h, _ in infos]
+        errs = self._call(bufs, [o.ctypes.data for o in outs], [o.strides[0] for o in outs], False, flags)
+        res = [o[:h, :w] if e == 0 else None for o, e, (_, w, h, _) in zip(outs, errs, infos)]
+        return res, errs
+
+    def decode_device(self, bufs, flags: int = 0, pad: int = 0):
+        """torch.uint8 CUDA frames (rows padded by `pad` bytes) and error codes."""
+        import torch
+        infos = [jpeg_info(b, flags) for b in bufs]
+        outs = [torch.zeros((max(h, 1), max(w, 1) + pad), dtype=torch.uint8, device="cuda") for _, w, h, _ in infos]
+        errs = self._call(bufs, [o.data_ptr() for o in outs], [o.stride(0) for o in outs], True, flags)
+        return [o[:h, :w] if e == 0 else None for o, e, (_, w, h, _) in zip(outs, errs, infos)], errs
+
+    def last_stats(self) -> dict:
+        a = (C.c_double * 8)()
+        self._L.at_jpeg_last_stats(self._d, a)
+        return dict(parse_ms=a[0], copy_in_ms=a[1], sync_ms=a[2], write_ms=a[3], copy_out_ms=a[4],
+                    substreams=int(a[5]), extra_passes=int(a[6]), entropy_bytes=int(a[7]))
+
+    def close(self):
+        if self._d:
+            self._L.at_jpeg_destroy(self._d)
+            self._d = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pjpeg_decode(buf: bytes, flags: int = 0):
+    """Through the pjpeg.h drop-in: (error, width, height, [planes])."""
+    L = _jpeg_lib()
+    err = C.c_int(0)
+    pj = L.pjpeg_create_from_buffer(buf, len(buf), flags, C.byref(err))
+    if not pj:
+        return err.value, 0, 0, []
+    try:
+        p = pj.contents
+        planes = []
+        for i in range(p.ncomponents):
+            c = p.components[i]
+            n = c.height * c.stride
+            planes.append(np.ctypeslib.as_array(c.data, shape=(n,)).reshape(c.height, c.stride).copy()
+                          if n else np.zeros((c.height, c.stride), np.uint8))
+        return err.value, p.width, p.height, planes
+    finally:
+        L.pjpeg_destroy(pj)
+
+
+def pjpeg_rgb(buf: bytes, flags: int = 0):
+    """pjpeg_to_u8x3_baseline of the drop-in: (h, w, 3) array or None."""
+    L = _jpeg_lib()
+    err = C.c_int(0)
+    pj = L.pjpeg_create_from_buffer(buf, len(buf), flags, C.byref(err))
+    if not pj:
+        return None
+    try:
+        im = L.pjpeg_to_u8x3_baseline(pj)
+        if not im:
+            return None
+        try:
+            m = im.contents
+            a = np.ctypeslib.as_array(m.buf, shape=(m.height * m.stride,)).reshape(m.height, m.stride)
+            return a[:, :3 * m.width].reshape(m.height, m.width, 3).copy()
+        finally:
+            L.image_u8x3_destroy(im)
+    finally:
+        L.pjpeg_destroy(pj)

@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 CUFLAGS = ARCH + FP + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                        "-I", os.path.join(ROOT, "include"), "-I", CSRC]
-SOURCES = ["at_kernels.cu", "at_cluster.cu", "at_order.cu", "at_detector.cu", "at_noalloc.cu", "at_server.cu", "at_pose.cu"]
+SOURCES = ["at_kernels.cu", "at_cluster.cu", "at_order.cu", "at_detector.cu", "at_noalloc.cu", "at_server.cu", "at_pose.cu", "at_jpeg.cu"]
 C_SOURCES = ["at_upstream.c"]
 
 

@@ -301,6 +301,46 @@ int at_estimate_poses(const at_detector *td, double tagsize, double fx, double f
 int at_threshold_noalloc(const uint8_t *image, int64_t width, int64_t height, int32_t min_white_black_diff,
                          uint8_t *out, void *stream);
 
+/* ---- JPEG input: baseline JPEG decoded on the GPU into 8-bit frames ----
+   The pixels are those of the reference's decoder (common/pjpeg.c:
+   pjpeg_create_from_buffer then pjpeg_to_u8_baseline, component 0 cropped
+   to the image), byte for byte, and so are its error codes (PJPEG_ERR_* of
+   common/pjpeg.h). The reference decodes on one CPU core; here the host
+   reads the headers and cuts each scan at its restart markers, and the
+   entropy decoding and the IDCT run on the GPU. pjpeg.h's calls are
+   provided too, over the same decoder. No counterpart in the reference's
+   native API. */
+typedef struct at_jpeg at_jpeg;
+
+/* A decoder with its own CUDA stream and memory on the current device. */
+at_jpeg *at_jpeg_create(void);
+void at_jpeg_destroy(at_jpeg *dec);
+
+/* The size of the gray frame a decode of buf gives (the image's width and
+   height, its component count). Returns 0 or the error the decode would
+   return from its headers (PJPEG_ERR_*). */
+int at_jpeg_info(const uint8_t *buf, int64_t len, uint32_t flags, int32_t *width, int32_t *height,
+                 int32_t *ncomponents);
+
+/* Decodes n JPEGs (bufs[i], lens[i] bytes, host memory) in one pass on the
+   GPU into gray frames: frame i goes to dst[i], rows of strides[i] bytes,
+   width x height as at_jpeg_info gives; dst is device memory when
+   on_device is non-zero, host memory otherwise. flags: PJPEG_MJPEG.
+   errors[i] receives each image's PJPEG_ERR_* (0: written). Returns the
+   number of images that failed, or -1 for a CUDA error (message on
+   stderr). Returns when every frame is written. */
+int at_jpeg_decode_gray(at_jpeg *dec, int32_t n, const uint8_t *const *bufs, const int64_t *lens, uint32_t flags,
+                        uint8_t *const *dst, const int64_t *strides, int32_t on_device, int32_t *errors);
+
+/* Figures of the last decode: [0] host parse ms, [1] copy in ms, [2] sync
+   pass ms, [3] write pass ms, [4] copy out ms (CUDA events), [5] sub-
+   streams, [6] sync passes beyond the first, [7] entropy-coded bytes. */
+int at_jpeg_last_stats(const at_jpeg *dec, double *out8);
+
+/* Bits of entropy-coded data per sub-stream (one GPU thread each),
+   default 512; a multiple of 32 from 64 to 65536. Returns 0 or 1. */
+int at_jpeg_set_sub_bits(at_jpeg *dec, int32_t bits);
+
 #ifdef __cplusplus
 }
 #endif

@@ -300,3 +300,131 @@ def ref_detect(img: np.ndarray, family_names, bits, params: Params | None = None
         return [det_tuple(d.detections[i]) for i in range(d.ndetections)], int(d.nquads)
     finally:
         R.at_detector_destroy(td)
+
+
+# --------------------------------------------------------------------------
+# JPEG input path (oracle/at_jpeg.c; the reference's common/pjpeg.c)
+
+JPEG_MJPEG = 2
+JPEG_OPTIMIZE, JPEG_NO_DHT, JPEG_MARKERS, JPEG_ONE_DQT = 1, 2, 4, 8
+
+
+class _OJPlane(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("stride", C.c_uint32),
+                ("data", C.POINTER(C.c_uint8)), ("id", C.c_uint8), ("hv", C.c_uint8), ("scalex", C.c_uint8),
+                ("scaley", C.c_uint8), ("tq", C.c_uint8), ("tda", C.c_uint8)]
+
+
+class _OJImage(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("ncomponents", C.c_int),
+                ("comp", _OJPlane * 3)]
+
+
+class _PJPEG(C.Structure):
+    """The reference's pjpeg_t (common/pjpeg.h:64-72); its component type
+    has the oracle's plane layout (common/pjpeg.h:38-62)."""
+
+    _fields_ = [("error", C.c_int), ("width", C.c_uint32), ("height", C.c_uint32), ("ncomponents", C.c_int),
+                ("components", C.POINTER(_OJPlane))]
+
+
+def _planes(comps, n):
+    out = []
+    for i in range(n):
+        c = comps[i]
+        a = np.ctypeslib.as_array(c.data, shape=(c.height * c.stride,)).reshape(c.height, c.stride) \
+            if c.height * c.stride else np.zeros((c.height, c.stride), np.uint8)
+        out.append(a.copy())
+    return out
+
+
+def jpeg_encode(img: np.ndarray, quality: int = 90, sampling=(1, 1), restart: int = 0, flags: int = 0) -> bytes:
+    """Baseline JPEG of a gray (h, w) or RGB (h, w, 3) u8 image (test inputs)."""
+    L = lib()
+    L.oj_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
+                            C.c_int, C.c_int, C.c_void_p, C.c_int64]
+    L.oj_encode.restype = C.c_int64
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape[:2]
+    nc = 1 if img.ndim == 2 else 3
+    cap = 4 * w * h * nc + 65536
+    out = np.empty(cap, np.uint8)
+    n = L.oj_encode(img.ctypes.data, w, h, img.strides[0], nc, sampling[0], sampling[1], quality, restart, flags,
+                    out.ctypes.data, cap)
+    if n < 0:
+        raise ValueError("oj_encode refused its arguments")
+    return out[:n].tobytes()
+
+
+def jpeg_decode(buf: bytes, flags: int = 0):
+    """The oracle's decode: (error, width, height, [component planes])."""
+    L = lib()
+    L.oj_decode.argtypes = [C.c_char_p, C.c_int64, C.c_uint32, C.POINTER(_OJImage)]
+    L.oj_decode.restype = C.c_int
+    L.oj_free.argtypes = [C.POINTER(_OJImage)]
+    im = _OJImage()
+    e = L.oj_decode(buf, len(buf), flags, C.byref(im))
+    if e:
+        return e, 0, 0, []
+    try:
+        return 0, im.width, im.height, _planes(im.comp, im.ncomponents)
+    finally:
+        L.oj_free(C.byref(im))
+
+
+def ref_jpeg_decode(buf: bytes, flags: int = 0):
+    """The reference's own pjpeg (oracle/_ref), same return as jpeg_decode."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref not built (make -C oracle ref)")
+    R.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
+    R.pjpeg_create_from_buffer.restype = C.POINTER(_PJPEG)
+    R.pjpeg_destroy.argtypes = [C.POINTER(_PJPEG)]
+    err = C.c_int(0)
+    pj = R.pjpeg_create_from_buffer(buf, len(buf), flags, C.byref(err))
+    if not pj:
+        return err.value, 0, 0, []
+    try:
+        p = pj.contents
+        return err.value, p.width, p.height, _planes(p.components, p.ncomponents)
+    finally:
+        R.pjpeg_destroy(pj)
+
+
+def gray_of(width: int, height: int, planes) -> np.ndarray:
+    """Component 0 cropped to the image (pjpeg_to_u8_baseline)."""
+    return np.ascontiguousarray(planes[0][:height, :width])
+
+
+def ref_jpeg_rgb(buf: bytes, flags: int = 0):
+    """The reference's pjpeg_to_u8x3_baseline (oracle/_ref): (h, w, 3) or None."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref not built (make -C oracle ref)")
+
+    class U8x3(C.Structure):
+        _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("stride", C.c_int32),
+                    ("buf", C.POINTER(C.c_uint8))]
+
+    R.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
+    R.pjpeg_create_from_buffer.restype = C.POINTER(_PJPEG)
+    R.pjpeg_destroy.argtypes = [C.POINTER(_PJPEG)]
+    R.pjpeg_to_u8x3_baseline.argtypes = [C.POINTER(_PJPEG)]
+    R.pjpeg_to_u8x3_baseline.restype = C.POINTER(U8x3)
+    R.image_u8x3_destroy.argtypes = [C.POINTER(U8x3)]
+    err = C.c_int(0)
+    pj = R.pjpeg_create_from_buffer(buf, len(buf), flags, C.byref(err))
+    if not pj:
+        return None
+    try:
+        if pj.contents.ncomponents != 3:
+            return None
+        im = R.pjpeg_to_u8x3_baseline(pj)
+        try:
+            m = im.contents
+            a = np.ctypeslib.as_array(m.buf, shape=(m.height * m.stride,)).reshape(m.height, m.stride)
+            return a[:, :3 * m.width].reshape(m.height, m.width, 3).copy()
+        finally:
+            R.image_u8x3_destroy(im)
+    finally:
+        R.pjpeg_destroy(pj)

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "apriltag_fast.h")
 UPSTREAM_HEADERS = [os.path.join(ROOT, "include", h) for h in (
     "apriltag.h", "apriltag_pose.h", "common/matd.h", "common/image_u8.h", "tag16h5.h", "tag25h9.h", "tag36h10.h", "tag36h11.h",
-    "tagCircle21h7.h", "tagCircle49h12.h", "tagCustom48h12.h", "tagStandard41h12.h", "tagStandard52h13.h")]
+    "tagCircle21h7.h", "tagCircle49h12.h", "tagCustom48h12.h", "tagStandard41h12.h", "tagStandard52h13.h",
+    "common/pjpeg.h", "common/image_u8x3.h")]
 
 
 def declared_functions(path=HEADER, prefix=r"at_\w+"):
@@ -37,9 +38,9 @@ def test_library_exports_the_upstream_api():
     L = C.CDLL(AT.LIB_PATH)
     names = []
     for h in UPSTREAM_HEADERS:
-        names += declared_functions(h, r"(?:apriltag|matd|image_u8|tag|estimate)\w+")
+        names += declared_functions(h, r"(?:apriltag|matd|image_u8|tag|estimate|pjpeg)\w+")
     assert "apriltag_detector_detect" in names and "tag36h11_create" in names and len(names) >= 38
-    assert "estimate_tag_pose" in names
+    assert "estimate_tag_pose" in names and "pjpeg_to_u8_baseline" in names and "image_u8x3_create" in names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 
@@ -62,6 +63,10 @@ def test_upstream_struct_layouts_match_reference(tmp_path):
     assert out[2] == "detection 112 family 0 id 8 hamming 12 dm 16 H 24 c 32 p 48"
     assert out[3] == "qtp 28 zarray 24 matd 16 image_u8 24 timeprofile 16"
     assert out[4] == "info 48 det 0 tagsize 8 fx 16 fy 24 cx 32 cy 40 pose 16 R 0 t 8"
+    # common/pjpeg.h and common/image_types.h of the reference
+    assert out[5] == ("pjpeg 24 error 0 width 4 height 8 nc 12 comps 16 component 32 w 0 h 4 stride 8 data 16 "
+                      "id 24 hv 25 sx 26 sy 27 tq 28 tda 29 u8x3 24")
+    assert out[6] == "errors 1 6 8 10 flags 1 2"
 
 
 def test_struct_layouts_match_reference():

@@ -4,6 +4,7 @@
 #include <stddef.h>
 #include "apriltag.h"
 #include "apriltag_pose.h"
+#include "common/pjpeg.h"
 int main(void) {
     printf("family %zu ncodes %zu codes %zu wab %zu tw %zu rb %zu nbits %zu bx %zu by %zu h %zu name %zu impl %zu\n",
         sizeof(apriltag_family_t), offsetof(apriltag_family_t, ncodes), offsetof(apriltag_family_t, codes), offsetof(apriltag_family_t, width_at_border),
@@ -23,5 +24,12 @@ int main(void) {
         offsetof(apriltag_detection_info_t, det), offsetof(apriltag_detection_info_t, tagsize), offsetof(apriltag_detection_info_t, fx),
         offsetof(apriltag_detection_info_t, fy), offsetof(apriltag_detection_info_t, cx), offsetof(apriltag_detection_info_t, cy),
         sizeof(apriltag_pose_t), offsetof(apriltag_pose_t, R), offsetof(apriltag_pose_t, t));
+    printf("pjpeg %zu error %zu width %zu height %zu nc %zu comps %zu component %zu w %zu h %zu stride %zu data %zu id %zu hv %zu sx %zu sy %zu tq %zu tda %zu u8x3 %zu\n",
+        sizeof(pjpeg_t), offsetof(pjpeg_t, error), offsetof(pjpeg_t, width), offsetof(pjpeg_t, height), offsetof(pjpeg_t, ncomponents),
+        offsetof(pjpeg_t, components), sizeof(pjpeg_component_t), offsetof(pjpeg_component_t, width), offsetof(pjpeg_component_t, height),
+        offsetof(pjpeg_component_t, stride), offsetof(pjpeg_component_t, data), offsetof(pjpeg_component_t, id), offsetof(pjpeg_component_t, hv),
+        offsetof(pjpeg_component_t, scalex), offsetof(pjpeg_component_t, scaley), offsetof(pjpeg_component_t, tq), offsetof(pjpeg_component_t, tda),
+        sizeof(image_u8x3_t));
+    printf("errors %d %d %d %d flags %d %d\n", PJPEG_ERR_FILE, PJPEG_ERR_MISSING_DHT, PJPEG_ERR_RESET, PJEPG_ERR_UNSUPPORTED, PJPEG_STRICT, PJPEG_MJPEG);
     return 0;
 }
