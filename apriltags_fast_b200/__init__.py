@@ -467,6 +467,7 @@ def _jpeg_lib():
         L.at_jpeg_decode_gray.restype = C.c_int
         L.at_jpeg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.at_jpeg_set_sub_bits.argtypes = [C.c_void_p, C.c_int32]
+        L.at_jpeg_set_threads.argtypes = [C.c_void_p, C.c_int32]
         L.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
         L.pjpeg_create_from_buffer.restype = C.POINTER(_PJ)
         L.pjpeg_destroy.argtypes = [C.POINTER(_PJ)]
@@ -489,13 +490,15 @@ class JpegDecoder:
     """Decodes batches of baseline JPEGs on the GPU into gray frames
     (component 0 cropped to the image, as pjpeg_to_u8_baseline gives it)."""
 
-    def __init__(self, sub_bits: int | None = None):
+    def __init__(self, sub_bits: int | None = None, threads: int = 0):
         self._L = _jpeg_lib()
         self._d = self._L.at_jpeg_create()
         if not self._d:
             raise RuntimeError("at_jpeg_create failed (no CUDA device?)")
         if sub_bits is not None and self._L.at_jpeg_set_sub_bits(self._d, sub_bits):
             raise ValueError("sub_bits must be a multiple of 32 in [64, 65536]")
+        if self._L.at_jpeg_set_threads(self._d, threads):
+            raise ValueError("threads must be in [0, 256]")
 
     def _call(self, bufs, dsts, strides, on_device, flags):
         n = len(bufs)

@@ -341,6 +341,10 @@ int at_jpeg_last_stats(const at_jpeg *dec, double *out8);
    default 512; a multiple of 32 from 64 to 65536. Returns 0 or 1. */
 int at_jpeg_set_sub_bits(at_jpeg *dec, int32_t bits);
 
+/* Host threads that parse the images of a batch (0, the default: up to
+   16). Returns 0 or 1. */
+int at_jpeg_set_threads(at_jpeg *dec, int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif
