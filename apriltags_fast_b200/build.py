@@ -17,6 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libapriltag_b200.so")
+SYNTH_JPEG_LIB = os.path.join(PKG, "libsynthjpeg.so")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -70,6 +71,10 @@ def build(force: bool = False) -> str:
         objs.append(o)
     if force or _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm"])
+    # the synthetic-input JPEG encoder (bench and tests; not the detector)
+    sj = os.path.join(CSRC, "synth_jpeg.c")
+    if force or _newer(SYNTH_JPEG_LIB, [sj]):
+        _run(["gcc", "-O2", "-fPIC", "-std=gnu11", "-shared", "-o", SYNTH_JPEG_LIB, sj, "-lm"])
     return LIB
 
 

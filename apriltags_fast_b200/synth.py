@@ -262,3 +262,42 @@ def tables_from(lookup, names):
     """name -> table for `names`, with lookup(name) giving an at_family
     struct (for example the reference library's at_family_by_name)."""
     return {n: table_of(lookup(n)) for n in names}
+
+
+# --------------------------------------------------------------------------
+# JPEG versions of frames (csrc/synth_jpeg.c, built beside the package)
+
+JPEG_OPTIMIZE, JPEG_NO_DHT, JPEG_MARKERS, JPEG_ONE_DQT = 1, 2, 4, 8
+_sj = None
+
+
+def encode_jpeg(img, quality: int = 90, sampling=(1, 1), restart: int = 0, flags: int = 0) -> bytes:
+    """Baseline JPEG of a gray (h, w) or RGB (h, w, 3) u8 image: luma
+    sampling (h, v) in {1, 2}, chroma 1x1; quality 1-100 on the IJG scale
+    of the Annex K tables; a restart marker every `restart` MCUs; flags:
+    JPEG_OPTIMIZE (per-image optimal Huffman tables), JPEG_NO_DHT (no
+    Huffman tables in the file), JPEG_MARKERS (APP0, APP13, COM),
+    JPEG_ONE_DQT (one DQT segment)."""
+    import ctypes as C
+    import os
+
+    global _sj
+    if _sj is None:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsynthjpeg.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m apriltags_fast_b200.build`")
+        L = C.CDLL(path)
+        L.sj_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_void_p, C.c_int64]
+        L.sj_encode.restype = C.c_int64
+        _sj = L
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape[:2]
+    nc = 1 if img.ndim == 2 else 3
+    cap = 4 * w * h * nc + 65536
+    out = np.empty(cap, np.uint8)
+    n = _sj.sj_encode(img.ctypes.data, w, h, img.strides[0], nc, sampling[0], sampling[1], quality, restart, flags,
+                      out.ctypes.data, cap)
+    if n < 0:
+        raise ValueError("encode_jpeg: arguments out of range")
+    return out[:n].tobytes()

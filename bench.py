@@ -22,6 +22,11 @@ With torchrun (N > 1) each rank runs its own detector on its own frames
 (frames are independent: no collective on the data path); `value` is all
 ranks' frames over the slowest rank's time.
 
+`jpeg` times the JPEG input path on the same frames encoded as baseline
+JPEGs: one at_jpeg_decode_gray call for B frames (host JPEG bytes to device
+frames), and that call followed by at_detect_batch on its frames, with the
+reference's own decoder (pjpeg) on the host threads beside it.
+
 --impl reference times the reference's own CPU detector (compiled from its
 sources into oracle/_ref) with all host threads on the same frames.
 """
@@ -157,6 +162,106 @@ def cpu_reference_fps(pool, nthreads: int, seconds: float):
     dt = time.perf_counter() - t0
     R.at_detector_destroy(td)
     return n / dt, n
+
+
+def jpeg_cpu_fps(bufs, nthreads: int, seconds: float):
+    """The reference's own decoder (common/pjpeg.c, compiled into
+    oracle/_ref) on host threads: JPEG frames/s over a bounded sample."""
+    from oracle import oracle as O
+
+    R = O.ref_lib()
+    if R is None:
+        return None, 0
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    R.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
+    R.pjpeg_create_from_buffer.restype = C.c_void_p
+    R.pjpeg_destroy.argtypes = [C.c_void_p]
+    t0 = time.perf_counter()
+
+    def work(k):
+        n = 0
+        while time.perf_counter() - t0 < seconds:
+            err = C.c_int(0)
+            b = bufs[(k + n) % len(bufs)]
+            R.pjpeg_destroy(R.pjpeg_create_from_buffer(b, len(b), 0, C.byref(err)))
+            n += 1
+        return n
+
+    with ThreadPoolExecutor(nthreads) as ex:
+        n = sum(ex.map(work, range(nthreads)))
+    return n / (time.perf_counter() - t0), n
+
+
+def jpeg_bench(pool, B: int, steps: int, warmup: int, cpu: bool):
+    """The JPEG input path: B frames of the pool as baseline JPEGs (quality
+    90, Annex K tables, gray, as a camera's encoder writes them) decoded by
+    one at_jpeg_decode_gray call into device frames (headers parsed on host
+    threads, entropy decoding and IDCT on the GPU); then the same call
+    followed by at_detect_batch on those device frames (JPEG bytes in host
+    memory to detections). Wall-clock time per call (the call returns when
+    its frames are written); kernel times from the decoder's CUDA events."""
+    import ctypes as C
+
+    import torch
+
+    import apriltags_fast_b200 as AT
+    from apriltags_fast_b200 import synth
+
+    bufs = [synth.encode_jpeg(pool[i % len(pool)], 90) for i in range(B)]
+    dec = AT.JpegDecoder()
+    L = AT._jpeg_lib()
+    frames = [torch.empty((H, W), dtype=torch.uint8, device="cuda") for _ in range(B)]
+    cb = (C.c_char_p * B)(*bufs)
+    cl = (C.c_int64 * B)(*[len(b) for b in bufs])
+    cd = (C.c_void_p * B)(*[f.data_ptr() for f in frames])
+    cs = (C.c_int64 * B)(*[W] * B)
+    errs = (C.c_int32 * B)()
+
+    def decode():
+        if L.at_jpeg_decode_gray(dec._d, B, cb, cl, 0, cd, cs, 1, errs) != 0:
+            raise RuntimeError("JPEG decode failed")
+
+    for _ in range(warmup):
+        decode()
+    wall, st = [], []
+    for _ in range(steps):
+        t = time.perf_counter()
+        decode()
+        wall.append(time.perf_counter() - t)
+        st.append(dec.last_stats())
+    ms = 1e3 * float(np.median(wall))
+    kern = {k: float(np.median([x[k] for x in st])) for k in ("parse_ms", "copy_in_ms", "sync_ms", "write_ms")}
+    det = AT.Detector(["tag36h11"], 2)
+    for _ in range(warmup):
+        decode()
+        det.detect_batch(frames, as_arrays=True)
+    both = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        decode()
+        det.detect_batch(frames, as_arrays=True)
+        both.append(time.perf_counter() - t)
+    ms_both = 1e3 * float(np.median(both))
+    ent = float(np.median([x["entropy_bytes"] for x in st]))
+    out = {"workload": f"{B} x 1920x1080 gray JPEG, quality 90, Annex K tables, "
+                       f"{sum(map(len, bufs)) / B / 1e3:.0f} KB a frame",
+           "unit": "frames/s", "frames_per_call": B, "fps": B / ms * 1e3, "ms_per_call": ms,
+           "stage_ms": kern, "substreams": int(st[-1]["substreams"]), "extra_sync_passes": int(st[-1]["extra_passes"]),
+           "entropy_gbs_in_kernels": ent / ((kern["sync_ms"] + kern["write_ms"]) * 1e-3) / 1e9,
+           "jpeg_to_detections_fps": B / ms_both * 1e3, "gpu_launches_per_call": 3}
+    if cpu:
+        cores = os.cpu_count() or 1
+        fa, na = jpeg_cpu_fps(bufs, cores, 5.0)
+        f1, n1 = jpeg_cpu_fps(bufs, 1, 3.0)
+        if fa is not None:
+            out["cpu_baseline"] = {"value": fa, "unit": "frames/s", "cores": cores, "kind": "reference",
+                                   "sample": f"{na} decodes of the {B} JPEGs by pjpeg_create_from_buffer "
+                                             f"at {cores} threads, ~5 s",
+                                   "value_1thread": f1, "sample_1thread": f"{n1} decodes, ~3 s"}
+    dec.close()
+    return out
 
 
 def run_reference(args):
@@ -343,6 +448,7 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--no-jpeg", action="store_true", help="skip the JPEG-input measurement")
     ap.add_argument("--profile-step", action="store_true",
                     help="warm up, then run one batched step between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
@@ -549,6 +655,8 @@ def main():
     }
     if not args.no_served:
         line["served"] = served(det)
+    if not args.no_jpeg and rank == 0:
+        line["jpeg"] = jpeg_bench(pool, B, 10, 3, not args.no_cpu_baseline)
     if not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         fps_all, n_all = cpu_reference_fps(pool, cores, 10.0)

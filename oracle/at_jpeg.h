@@ -7,12 +7,9 @@
    end of the buffer), the same Huffman code space, the same restart check
    (which zeroes the DC predictor of the scan's first component only), the
    same component planes. It is pinned to the reference compiled from its
-   own sources (oracle/_ref) by the CPU tests.
-
-   oj_encode is a small baseline JPEG encoder that makes the test inputs
-   (gray or YCbCr, any luma sampling up to 2x2, restart intervals, the
-   Annex K tables or per-image optimal Huffman tables). Neither is linked
-   into the product library. */
+   own sources (oracle/_ref) by the CPU tests. Not linked into the product
+   library. (The test inputs come from the package's synthetic-input
+   encoder, apriltags_fast_b200/csrc/synth_jpeg.c.) */
 #ifndef AT_JPEG_ORACLE_H
 #define AT_JPEG_ORACLE_H
 
@@ -50,22 +47,6 @@ void oj_free(oj_image *im);
 /* Component 0 cropped to width x height, rows of `stride` bytes
    (pjpeg_to_u8_baseline). Returns 0, or -1 when the plane is smaller. */
 int oj_gray(const oj_image *im, uint8_t *dst, int64_t stride);
-
-/* Encoder options. */
-enum {
-    OJ_ENC_OPTIMIZE = 1,   /* per-image optimal Huffman tables */
-    OJ_ENC_NO_DHT = 2,     /* leave the Huffman tables out (Annex K ones used) */
-    OJ_ENC_MARKERS = 4,    /* add APP0, APP13 and COM segments */
-    OJ_ENC_ONE_DQT = 8,    /* both quantisation tables in one DQT segment */
-};
-
-/* Encodes an 8-bit image: nc 1 (gray, rows of `stride` bytes) or 3 (RGB
-   interleaved). Luma sampling hs x vs (1 or 2 each; chroma 1x1), quality
-   1-100 on the IJG scale of the Annex K tables, a restart marker every
-   `restart` MCUs (0: none). Returns the byte count, or -1 if `cap` is too
-   small or an argument is out of range. */
-int64_t oj_encode(const uint8_t *img, int w, int h, int64_t stride, int nc, int hs, int vs, int quality,
-                  int restart, int flags, uint8_t *out, int64_t cap);
 
 #ifdef __cplusplus
 }

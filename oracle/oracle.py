@@ -339,21 +339,10 @@ def _planes(comps, n):
 
 
 def jpeg_encode(img: np.ndarray, quality: int = 90, sampling=(1, 1), restart: int = 0, flags: int = 0) -> bytes:
-    """Baseline JPEG of a gray (h, w) or RGB (h, w, 3) u8 image (test inputs)."""
-    L = lib()
-    L.oj_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
-                            C.c_int, C.c_int, C.c_void_p, C.c_int64]
-    L.oj_encode.restype = C.c_int64
-    img = np.ascontiguousarray(img, dtype=np.uint8)
-    h, w = img.shape[:2]
-    nc = 1 if img.ndim == 2 else 3
-    cap = 4 * w * h * nc + 65536
-    out = np.empty(cap, np.uint8)
-    n = L.oj_encode(img.ctypes.data, w, h, img.strides[0], nc, sampling[0], sampling[1], quality, restart, flags,
-                    out.ctypes.data, cap)
-    if n < 0:
-        raise ValueError("oj_encode refused its arguments")
-    return out[:n].tobytes()
+    """Test inputs: the package's synthetic-input encoder (synth.encode_jpeg)."""
+    from apriltags_fast_b200 import synth
+
+    return synth.encode_jpeg(img, quality, sampling, restart, flags)
 
 
 def jpeg_decode(buf: bytes, flags: int = 0):
