@@ -14,10 +14,9 @@
 
    Every stage of at_detect runs as sm_100a CUDA kernels on the current
    device; there is no CPU path. The detections are bit-identical to the
-   reference built with -ffp-contract=off; detections that share an id keep
-   the order of their quads, which here is the order of their boundary
-   clusters by component label (see at_detector_last_error below for the
-   error model). */
+   reference built with -ffp-contract=off, in the reference's order (same-id
+   detections too: the order its union-find roots give their quads). See
+   at_detector_last_error below for the error model. */
 #ifndef APRILTAG_FAST_H
 #define APRILTAG_FAST_H
 
