@@ -468,6 +468,7 @@ def _jpeg_lib():
         L.at_jpeg_last_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.at_jpeg_set_sub_bits.argtypes = [C.c_void_p, C.c_int32]
         L.at_jpeg_set_threads.argtypes = [C.c_void_p, C.c_int32]
+        L.at_jpeg_set_run_in.argtypes = [C.c_void_p, C.c_int32]
         L.pjpeg_create_from_buffer.argtypes = [C.c_char_p, C.c_int, C.c_uint32, C.POINTER(C.c_int)]
         L.pjpeg_create_from_buffer.restype = C.POINTER(_PJ)
         L.pjpeg_destroy.argtypes = [C.POINTER(_PJ)]
@@ -490,7 +491,7 @@ class JpegDecoder:
     """Decodes batches of baseline JPEGs on the GPU into gray frames
     (component 0 cropped to the image, as pjpeg_to_u8_baseline gives it)."""
 
-    def __init__(self, sub_bits: int | None = None, threads: int = 0):
+    def __init__(self, sub_bits: int | None = None, threads: int = 0, run_in: int | None = None):
         self._L = _jpeg_lib()
         self._d = self._L.at_jpeg_create()
         if not self._d:
@@ -499,6 +500,8 @@ class JpegDecoder:
             raise ValueError("sub_bits must be a multiple of 32 in [64, 65536]")
         if self._L.at_jpeg_set_threads(self._d, threads):
             raise ValueError("threads must be in [0, 256]")
+        if run_in is not None and self._L.at_jpeg_set_run_in(self._d, run_in):
+            raise ValueError("run_in must be in [0, 2**20]")
 
     def _call(self, bufs, dsts, strides, on_device, flags):
         n = len(bufs)
@@ -530,10 +533,11 @@ class JpegDecoder:
         return [o[:h, :w] if e == 0 else None for o, e, (_, w, h, _) in zip(outs, errs, infos)], errs
 
     def last_stats(self) -> dict:
-        a = (C.c_double * 8)()
+        a = (C.c_double * 10)()
         self._L.at_jpeg_last_stats(self._d, a)
         return dict(parse_ms=a[0], copy_in_ms=a[1], sync_ms=a[2], write_ms=a[3], copy_out_ms=a[4],
-                    substreams=int(a[5]), extra_passes=int(a[6]), entropy_bytes=int(a[7]))
+                    substreams=int(a[5]), extra_passes=int(a[6]), entropy_bytes=int(a[7]),
+                    cta_rounds=int(a[8]))
 
     def close(self):
         if self._d:

@@ -40,6 +40,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -50,8 +52,13 @@
 
 namespace {
 
-constexpr int JSUB_DEFAULT = 512;   // bits per sub-stream
-constexpr int JBACK_DEFAULT = 1024; // bits a speculative decode starts before its sub-stream
+// Bits per sub-stream, by job: short sub-streams give one image more
+// threads (latency), long ones spend less of a large batch on run-ins.
+uint32_t jsub_for(int64_t stream_bytes) {
+    uint32_t b = 256;
+    while (b < 1024 && (uint64_t)stream_bytes * 8 / b > 65536) b *= 2;
+    return b;
+}
 constexpr int JMAX_BPM = 64;        // blocks per MCU (the standard allows 10)
 constexpr int JSYNC_THREADS = 128;
 constexpr int JWRITE_THREADS = 128;
@@ -384,7 +391,10 @@ __global__ void __launch_bounds__(JSYNC_THREADS, 8) k_jpeg_sync(JJob J, uint32_t
             J.used[i] = in;
             for (int k = 0; k < 4; k++) J.cnt[4 * (size_t)i + k] = c4[k];
         }
-        if (!__syncthreads_or(any)) break;
+        if (!__syncthreads_or(any)) {
+            if (threadIdx.x == 0 && round) atomicMax(&J.changed[J.max_passes + 1], (int)round);
+            break;
+        }
         if (round > 2 * per + 2) {  // the CTA's entry kept moving: settle it over the grid
             edge = true;
             break;
@@ -1177,6 +1187,7 @@ struct HJob {
     size_t staging = 0;
     uint32_t max_seg_subs = 0;
     uint32_t nblocks = 0;  // blocks of the planes written
+    uint32_t sub_bits = 512, back_bits = 1024;
 };
 
 JTab make_tab(const HTab &t, std::vector<uint8_t> &pool) {
@@ -1305,6 +1316,63 @@ void add_image(HJob &J, const HImage &im, int64_t s_base, uint32_t sub_bits, uns
 
 }  // namespace
 
+// Host threads that parse a batch's images, kept for the decoder's life
+// (starting threads for every call cost more than the parse of a batch).
+struct JPool {
+    std::vector<std::thread> th;
+    std::mutex m;
+    std::condition_variable go, fin;
+    const std::function<void(int)> *fn = nullptr;
+    int n = 0, busy = 0;
+    uint64_t gen = 0;
+    bool stop = false;
+    std::atomic<int> next{0};
+    void start(int nthreads) {
+        for (int t = 0; t < nthreads; t++)
+            th.emplace_back([this] {
+                uint64_t seen = 0;
+                while (true) {
+                    const std::function<void(int)> *f;
+                    int cnt;
+                    {
+                        std::unique_lock<std::mutex> lk(m);
+                        go.wait(lk, [&] { return stop || gen != seen; });
+                        if (stop) return;
+                        seen = gen;
+                        f = fn;
+                        cnt = n;
+                    }
+                    for (int k; (k = next.fetch_add(1)) < cnt;) (*f)(k);
+                    std::lock_guard<std::mutex> lk(m);
+                    if (--busy == 0) fin.notify_all();
+                }
+            });
+    }
+    // runs f(0 .. n-1) on the workers and the calling thread
+    void run(int cnt, const std::function<void(int)> &f) {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            fn = &f;
+            n = cnt;
+            next = 0;
+            busy = (int)th.size();
+            gen++;
+        }
+        go.notify_all();
+        for (int k; (k = next.fetch_add(1)) < cnt;) f(k);
+        std::unique_lock<std::mutex> lk(m);
+        fin.wait(lk, [&] { return busy == 0; });
+    }
+    ~JPool() {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            stop = true;
+        }
+        go.notify_all();
+        for (auto &t : th) t.join();
+    }
+};
+
 struct at_jpeg {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1313,11 +1381,13 @@ struct at_jpeg {
     size_t h_cap = 0;
     uint8_t *d_arena = nullptr;
     size_t d_cap = 0;
-    uint32_t sub_bits = JSUB_DEFAULT;
-    uint32_t back_bits = JBACK_DEFAULT;
+    uint32_t sub_bits = 0;   // 0: chosen per job (jsub_for)
+    uint32_t back_bits = 0;  // 0: chosen per job
     int threads = 0;  // host threads parsing a batch (0: up to 16)
+    JPool *pool = nullptr;
+    int pool_threads = 0;
     int grid_max = 0;
-    double stats[8] = {};
+    double stats[10] = {};
     std::mutex mu;
 };
 
@@ -1425,7 +1495,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         JJ.nplanes = (uint32_t)J.planes.size();
         JJ.nblocks = J.nblocks;
         JJ.nsub = nsub;
-        JJ.sub_bits = d->sub_bits;
+        JJ.sub_bits = J.sub_bits;
         JJ.max_passes = max_passes;
         JJ.exitst = (unsigned long long *)(D + o_exit);
         JJ.used = (unsigned long long *)(D + o_used);
@@ -1433,7 +1503,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         JJ.excl = (uint32_t *)(D + o_excl);
         JJ.totals = (uint32_t *)(D + o_tot);
         JJ.seg_stuck = (uint32_t *)(D + o_stuck);
-        JJ.back_bits = d->back_bits;
+        JJ.back_bits = J.back_bits;
         JJ.bar = (unsigned int *)(D + o_bar);
         JJ.changed = (int *)(D + o_chg);
         JJ.err = (int *)(D + o_err);
@@ -1453,9 +1523,12 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         }
         ok = ok && jcheck(cudaMemcpyAsync(hres, D + o_err, 4, cudaMemcpyDeviceToHost, s), "copy out");
         ok = ok && jcheck(cudaMemcpyAsync(hres + 1, D + o_chg, 4, cudaMemcpyDeviceToHost, s), "copy out");
+        ok = ok && jcheck(cudaMemcpyAsync(hres + 2, D + o_chg + 4 * (size_t)(max_passes + 1), 4,
+                                          cudaMemcpyDeviceToHost, s),
+                          "copy out");
     } else if (ok) {
         ok = jcheck(cudaEventRecord(d->ev[2], s), "event");
-        hres[0] = hres[1] = 0;
+        hres[0] = hres[1] = hres[2] = 0;
     }
     ok = ok && jcheck(cudaEventRecord(d->ev[3], s), "event");
     for (const HOut &o : J.outs) {
@@ -1475,6 +1548,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
     for (int k = 1; k < 5; k++)
         if (cudaEventElapsedTime(&ms, d->ev[k - 1], d->ev[k]) == cudaSuccess) d->stats[k] = ms;
     d->stats[6] = nsub ? hres[1] : 0;
+    d->stats[8] = nsub ? hres[2] : 0;
     return 0;
 }
 
@@ -1515,6 +1589,7 @@ void at_jpeg_destroy(at_jpeg *d) {
     if (d->stream) cudaStreamDestroy(d->stream);
     if (d->d_arena) cudaFree(d->d_arena);
     if (d->h_stage) cudaFreeHost(d->h_stage);
+    delete d->pool;
     delete d;
 }
 
@@ -1576,13 +1651,14 @@ static int decode_group(at_jpeg *dec, int32_t a, int32_t b, const uint8_t *const
     if (nt <= 1) {
         for (int k = 0; k < m; k++) parse_one(k, dec->h_stage + base[k], cap[a + k]);
     } else {
-        std::atomic<int> next(0);
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nt; t++)
-            pool.emplace_back([&] {
-                for (int k; (k = next.fetch_add(1)) < m;) parse_one(k, dec->h_stage + base[k], cap[a + k]);
-            });
-        for (auto &th : pool) th.join();
+        if (!dec->pool || dec->pool_threads != nt - 1) {
+            delete dec->pool;
+            dec->pool = new JPool();
+            dec->pool->start(nt - 1);
+            dec->pool_threads = nt - 1;
+        }
+        const std::function<void(int)> f = [&](int k) { parse_one(k, dec->h_stage + base[k], cap[a + k]); };
+        dec->pool->run(m, f);
     }
     int64_t tail = base[m];
     for (int k = 0; k < m; k++) {
@@ -1595,6 +1671,11 @@ static int decode_group(at_jpeg *dec, int32_t a, int32_t b, const uint8_t *const
     }
     HJob J;
     J.stream_n = tail;
+    int64_t total = 0;
+    for (int k = 0; k < m; k++)
+        if (!errs[k]) total += used[k];
+    J.sub_bits = dec->sub_bits ? dec->sub_bits : jsub_for(total);
+    J.back_bits = dec->back_bits ? dec->back_bits : std::max(512u, J.sub_bits);
     int failed = 0;
     for (int k = 0; k < m; k++) {
         const int32_t i = a + k;
@@ -1604,7 +1685,7 @@ static int decode_group(at_jpeg *dec, int32_t a, int32_t b, const uint8_t *const
             continue;
         }
         const HImage &im = ims[k];
-        add_image(J, im, base[k], dec->sub_bits, 1u, [&](int, JPlaneDev &P) -> size_t {
+        add_image(J, im, base[k], J.sub_bits, 1u, [&](int, JPlaneDev &P) -> size_t {
             P.ow = im.w;
             P.oh = im.h;
             if (on_device) {
@@ -1642,9 +1723,15 @@ int at_jpeg_decode_gray(at_jpeg *dec, int32_t n, const uint8_t *const *bufs, con
     return failed;
 }
 
-int at_jpeg_last_stats(const at_jpeg *dec, double *out8) {
-    if (!dec || !out8) return 1;
-    memcpy(out8, dec->stats, sizeof dec->stats);
+int at_jpeg_last_stats(const at_jpeg *dec, double *out10) {
+    if (!dec || !out10) return 1;
+    memcpy(out10, dec->stats, sizeof dec->stats);
+    return 0;
+}
+
+int at_jpeg_set_run_in(at_jpeg *dec, int32_t bits) {
+    if (!dec || bits < 0 || bits > (1 << 20)) return 1;
+    dec->back_bits = (uint32_t)bits;
     return 0;
 }
 
@@ -1655,7 +1742,7 @@ int at_jpeg_set_threads(at_jpeg *dec, int32_t threads) {
 }
 
 int at_jpeg_set_sub_bits(at_jpeg *dec, int32_t bits) {
-    if (!dec || bits < 64 || bits > 65536 || bits % 32) return 1;
+    if (!dec || (bits && (bits < 64 || bits > 65536 || bits % 32))) return 1;
     dec->sub_bits = (uint32_t)bits;
     return 0;
 }
@@ -1709,7 +1796,9 @@ pjpeg_t *pjpeg_create_from_buffer(uint8_t *buf, int buflen, uint32_t flags, int 
             o.data = (uint8_t *)calloc((size_t)h.ph * h.pstride + 1, 1);
         }
     }
-    add_image(J, im, 0, JSUB_DEFAULT, 7u, [&](int c, JPlaneDev &P) -> size_t {
+    J.sub_bits = jsub_for(sk.n);
+    J.back_bits = std::max(512u, J.sub_bits);
+    add_image(J, im, 0, J.sub_bits, 7u, [&](int c, JPlaneDev &P) -> size_t {
         const pjpeg_component_t &o = pj->components[c];
         P.ow = o.width;
         P.oh = o.height;

@@ -449,6 +449,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--no-jpeg", action="store_true", help="skip the JPEG-input measurement")
+    ap.add_argument("--jpeg-only", action="store_true",
+                    help="only the JPEG-input measurement (B frames a call), as its own JSON line")
     ap.add_argument("--profile-step", action="store_true",
                     help="warm up, then run one batched step between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
@@ -476,6 +478,9 @@ def main():
     import apriltags_fast_b200 as AT
 
     pool = make_pool(rank)
+    if args.jpeg_only:
+        print(json.dumps({"jpeg": jpeg_bench(pool, args.batch, args.steps, args.warmup, not args.no_cpu_baseline)}))
+        return
     dev = [torch.from_numpy(f).cuda() for f in pool]
     pinned = [torch.from_numpy(f).pin_memory() for f in pool]
     det = AT.Detector(["tag36h11"], 2)

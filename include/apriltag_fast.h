@@ -332,13 +332,21 @@ int at_jpeg_decode_gray(at_jpeg *dec, int32_t n, const uint8_t *const *bufs, con
                         uint8_t *const *dst, const int64_t *strides, int32_t on_device, int32_t *errors);
 
 /* Figures of the last decode: [0] host parse ms, [1] copy in ms, [2] sync
-   pass ms, [3] write pass ms, [4] copy out ms (CUDA events), [5] sub-
-   streams, [6] sync passes beyond the first, [7] entropy-coded bytes. */
-int at_jpeg_last_stats(const at_jpeg *dec, double *out8);
+   pass ms, [3] write and IDCT ms, [4] copy out ms (CUDA events), [5] sub-
+   streams, [6] sync passes beyond the first, [7] entropy-coded bytes, [8]
+   the most repeats a CTA needed within a pass, [9] unused. */
+int at_jpeg_last_stats(const at_jpeg *dec, double *out10);
 
-/* Bits of entropy-coded data per sub-stream (one GPU thread each),
-   default 512; a multiple of 32 from 64 to 65536. Returns 0 or 1. */
+/* Bits of entropy-coded data per sub-stream (one GPU thread each); by
+   default chosen per call from 256 to 1024 by the data's size (0 restores
+   that); a multiple of 32 from 64 to 65536. Returns 0 or 1. */
 int at_jpeg_set_sub_bits(at_jpeg *dec, int32_t bits);
+
+/* Bits a sub-stream's first, speculative decode starts before the
+   sub-stream (by default the larger of 512 and the sub-stream; 0 restores
+   that): longer run-ins fall into step with the true decode more often, at
+   the cost of decoding them. Returns 0 or 1. */
+int at_jpeg_set_run_in(at_jpeg *dec, int32_t bits);
 
 /* Host threads that parse the images of a batch (0, the default: up to
    16). Returns 0 or 1. */
