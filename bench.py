@@ -201,7 +201,9 @@ def jpeg_bench(pool, B: int, steps: int, warmup: int, cpu: bool):
     threads, entropy decoding and IDCT on the GPU); then the same call
     followed by at_detect_batch on those device frames (JPEG bytes in host
     memory to detections). Wall-clock time per call (the call returns when
-    its frames are written); kernel times from the decoder's CUDA events."""
+    its frames are written); kernel times from the decoder's CUDA events.
+    Also pipelined: the decode of the next call on one host thread while
+    the detector works on the previous call's frames."""
     import ctypes as C
 
     import torch
@@ -244,13 +246,42 @@ def jpeg_bench(pool, B: int, steps: int, warmup: int, cpu: bool):
         det.detect_batch(frames, as_arrays=True)
         both.append(time.perf_counter() - t)
     ms_both = 1e3 * float(np.median(both))
+    # pipelined: the decode of call k+1 (decoder's stream, one host thread)
+    # overlaps the detection of call k (detector's streams, another), two
+    # sets of device frames
+    from concurrent.futures import ThreadPoolExecutor
+
+    frames2 = [torch.empty((H, W), dtype=torch.uint8, device="cuda") for _ in range(B)]
+    cd2 = (C.c_void_p * B)(*[f.data_ptr() for f in frames2])
+    errs2 = (C.c_int32 * B)()
+    sets = [(cd, errs, frames), (cd2, errs2, frames2)]
+
+    def decode_into(k):
+        d_ptrs, e, _ = sets[k % 2]
+        if L.at_jpeg_decode_gray(dec._d, B, cb, cl, 0, d_ptrs, cs, 1, e) != 0:
+            raise RuntimeError("JPEG decode failed")
+
+    n_pipe = steps * 2
+    with ThreadPoolExecutor(1) as ex:
+        for _ in range(2):  # warm-up of the pipeline
+            decode_into(0)
+            det.detect_batch(sets[0][2], as_arrays=True)
+        t = time.perf_counter()
+        nxt = ex.submit(decode_into, 0)
+        for k in range(n_pipe):
+            nxt.result()
+            if k + 1 < n_pipe:
+                nxt = ex.submit(decode_into, k + 1)
+            det.detect_batch(sets[k % 2][2], as_arrays=True)
+        ms_pipe = 1e3 * (time.perf_counter() - t) / n_pipe
     ent = float(np.median([x["entropy_bytes"] for x in st]))
     out = {"workload": f"{B} x 1920x1080 gray JPEG, quality 90, Annex K tables, "
                        f"{sum(map(len, bufs)) / B / 1e3:.0f} KB a frame",
            "unit": "frames/s", "frames_per_call": B, "fps": B / ms * 1e3, "ms_per_call": ms,
            "stage_ms": kern, "substreams": int(st[-1]["substreams"]), "extra_sync_passes": int(st[-1]["extra_passes"]),
            "entropy_gbs_in_kernels": ent / ((kern["sync_ms"] + kern["write_ms"]) * 1e-3) / 1e9,
-           "jpeg_to_detections_fps": B / ms_both * 1e3, "gpu_launches_per_call": 3}
+           "jpeg_to_detections_fps": B / ms_both * 1e3,
+           "jpeg_to_detections_pipelined_fps": B / ms_pipe * 1e3, "gpu_launches_per_call": 3}
     if cpu:
         cores = os.cpu_count() or 1
         fa, na = jpeg_cpu_fps(bufs, cores, 5.0)
