@@ -116,7 +116,8 @@ _lib = None
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("workers", C.c_int32), ("max_batch", C.c_int32), ("memory_budget", C.c_int64)]
+    _fields_ = [("workers", C.c_int32), ("max_batch", C.c_int32), ("memory_budget", C.c_int64),
+                ("device_mask", C.c_uint32)]
 
 
 class ServerResult(C.Structure):
@@ -169,6 +170,8 @@ def lib():
         L.at_server_free_result.argtypes = [C.POINTER(ServerResult)]
         L.at_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         L.at_server_destroy.argtypes = [C.c_void_p]
+        L.at_server_worker_device.argtypes = [C.c_void_p, C.c_int32]
+        L.at_server_worker_device.restype = C.c_int
         L.at_family_by_name.argtypes = [C.c_char_p]
         L.at_family_by_name.restype = C.POINTER(Family)
         for n in FAMILY_NAMES:
@@ -353,11 +356,17 @@ class Server:
     from `detector` (its parameters and families). submit() returns a ticket
     (0: rejected); the image must stay alive and unchanged until its result
     has been polled. poll() returns finished results as dicts with the
-    detections as a numpy record array (DETECTION_DTYPE)."""
+    detections as a numpy record array (DETECTION_DTYPE). `devices`: the
+    GPUs to deal the workers out over (one detector replica per worker;
+    None: the current GPU)."""
 
-    def __init__(self, detector: "Detector", workers: int = 2, max_batch: int = 16, memory_budget: int = 24 << 30):
+    def __init__(self, detector: "Detector", workers: int = 2, max_batch: int = 16, memory_budget: int = 24 << 30,
+                 devices=None):
         self._L = lib()
-        cfg = ServerConfig(workers, max_batch, memory_budget)
+        mask = 0
+        for d in devices or ():
+            mask |= 1 << int(d)
+        cfg = ServerConfig(workers, max_batch, memory_budget, mask)
         self._s = self._L.at_server_create(detector._td, C.byref(cfg))
         if not self._s:
             raise RuntimeError("at_server_create failed")
@@ -370,6 +379,10 @@ class Server:
         if t:
             self._keep[t] = img
         return t
+
+    def worker_device(self, worker: int) -> int:
+        """The GPU of worker `worker` (a result's "worker"), or -1."""
+        return int(self._L.at_server_worker_device(self._s, int(worker)))
 
     def cancel(self, ticket: int) -> bool:
         """Cancel a request still in the queue (its result comes back with

@@ -42,7 +42,7 @@ struct Request {
 
 struct at_server {
     at_server_config cfg;
-    int device = 0;
+    std::vector<int> dev_of;  // each worker's GPU
     std::vector<at_detector *> dets;
     std::vector<std::thread> threads;
     std::mutex mu;
@@ -57,7 +57,7 @@ struct at_server {
 };
 
 static void worker(at_server *s, int w) {
-    cudaSetDevice(s->device);
+    cudaSetDevice(s->dev_of[w]);
     at_detector *td = s->dets[w];
     const int64_t share = s->cfg.memory_budget / (s->cfg.workers > 0 ? s->cfg.workers : 1);
     std::vector<Request> batch;
@@ -139,9 +139,29 @@ at_server *at_server_create(const at_detector *params, const at_server_config *c
         if (cfg->max_batch > 0) c.max_batch = cfg->max_batch;
         if (cfg->memory_budget > 0) c.memory_budget = cfg->memory_budget;
     }
+    // the GPUs: the current one, or those of the mask (one detector replica
+    // per worker, workers dealt out over the GPUs in turn; frames are
+    // independent, so nothing passes between the replicas)
+    int cur = 0, ndev = 0;
+    cudaGetDevice(&cur);
+    cudaGetDeviceCount(&ndev);
+    std::vector<int> devs;
+    const uint32_t mask = cfg ? cfg->device_mask : 0u;
+    if (mask == 0) devs.push_back(cur);
+    for (int d = 0; d < 32 && d < ndev; d++)
+        if (mask & (1u << d)) devs.push_back(d);
+    if (devs.empty()) {
+        delete s;
+        return nullptr;
+    }
+    c.device_mask = mask;
     s->cfg = c;
-    cudaGetDevice(&s->device);
-    for (int w = 0; w < c.workers; w++) s->dets.push_back(at_detector_clone(params));
+    for (int w = 0; w < c.workers; w++) {
+        s->dev_of.push_back(devs[w % devs.size()]);
+        cudaSetDevice(s->dev_of[w]);
+        s->dets.push_back(at_detector_clone(params));
+    }
+    cudaSetDevice(cur);
     for (int w = 0; w < c.workers; w++) s->threads.emplace_back(worker, s, w);
     return s;
 }
@@ -165,6 +185,11 @@ uint64_t at_server_submit(at_server *s, const at_frame *frame, uint64_t user) {
     s->st.admitted++;
     s->cv_work.notify_one();
     return r.ticket;
+}
+
+int at_server_worker_device(const at_server *s, int32_t worker) {
+    if (s == nullptr || worker < 0 || worker >= (int32_t)s->dev_of.size()) return -1;
+    return s->dev_of[worker];
 }
 
 int at_server_cancel(at_server *s, uint64_t ticket) {
@@ -228,7 +253,13 @@ void at_server_destroy(at_server *s) {
     }
     s->cv_work.notify_all();
     for (auto &t : s->threads) t.join();
-    for (auto *d : s->dets) at_detector_destroy(d);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (size_t w = 0; w < s->dets.size(); w++) {  // each replica on its own GPU
+        cudaSetDevice(s->dev_of[w]);
+        at_detector_destroy(s->dets[w]);
+    }
+    cudaSetDevice(cur);
     for (auto &r : s->done) free(r.detections);
     delete s;
 }

@@ -199,6 +199,7 @@ typedef struct at_server_config {
     int32_t workers;       /* concurrent batches (default 2) */
     int32_t max_batch;     /* frames per batch (default 16) */
     int64_t memory_budget; /* device bytes for all workers' frames (default 24 GiB) */
+    uint32_t device_mask;  /* bit d: workers on GPU d, dealt out in turn (0: the current GPU) */
 } at_server_config;
 #define AT_SERVER_CANCELLED (-1) /* at_server_result.status of a cancelled request */
 typedef struct at_server_result {
@@ -229,6 +230,8 @@ int at_server_cancel(at_server *s, uint64_t ticket);
 int64_t at_server_poll(at_server *s, at_server_result *out, int64_t max, int32_t wait_ms);
 void at_server_free_result(at_server_result *r);
 void at_server_get_stats(at_server *s, at_server_stats *out);
+/* The GPU that worker w runs on (at_server_result.worker), or -1. */
+int at_server_worker_device(const at_server *s, int32_t worker);
 /* Finishes the queued frames, stops the workers, frees everything. */
 void at_server_destroy(at_server *s);
 

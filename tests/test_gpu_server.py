@@ -204,3 +204,31 @@ def test_server_rejects_when_queued_bytes_exceed_budget():
         assert st["rejected"] == len(tickets) - len(admitted)
     finally:
         srv.close()
+
+
+def test_server_over_a_device_list():
+    """Workers dealt out over a list of GPUs (one detector replica each; this
+    box has one GPU, listed for both workers): each worker reports its GPU
+    and every result equals the frame alone, from host frames and from
+    device frames. A mask that names no GPU of this machine is refused."""
+    import torch
+
+    frames = synth.serve_mix(4, 5)
+    det = AT.Detector(["tag36h11"], 2)
+    alone = _alone(det, frames)
+    dev = [torch.from_numpy(np.ascontiguousarray(f)).cuda() for f in frames]
+    srv = AT.Server(det, workers=2, max_batch=4, devices=[0])
+    try:
+        assert [srv.worker_device(w) for w in range(3)] == [0, 0, -1]
+        tickets = [srv.submit(f, user=i) for i, f in enumerate(frames)]
+        tickets += [srv.submit(f, user=i) for i, f in enumerate(dev)]
+        assert all(t > 0 for t in tickets)
+        res = _drain(srv, len(tickets))
+        assert sorted(r["ticket"] for r in res) == sorted(tickets)
+        for r in res:
+            assert r["status"] == 0 and srv.worker_device(r["worker"]) == 0
+            assert (r["detections"].tobytes(), r["nquads"]) == alone[r["user"]]
+    finally:
+        srv.close()
+    with pytest.raises(RuntimeError):
+        AT.Server(det, workers=1, devices=[31])
