@@ -16,15 +16,17 @@
 // is on the device:
 //
 //  * k_jpeg_sync (cooperative, one launch): every segment is cut into
-//    sub-streams of JSUB bits, one thread each. Pass 0 decodes each
-//    sub-stream from its first bit as if a block started there; pass k
-//    re-decodes a sub-stream from the exit state (bit, coefficient,
-//    block of the MCU) of its predecessor whenever that changed. Huffman
-//    codes resynchronise within a few codes, so the exit states settle in
-//    one or two passes; a segment's first sub-stream starts exactly, so
-//    the passes end by construction (at worst after one per sub-stream).
-//    The same launch then scans, over the sub-streams, the block counts
-//    and the DC-difference sums of each component.
+//    sub-streams of 256 to 1024 bits (by the call's data size), one thread
+//    each. Pass 0 decodes each sub-stream from a run-in before its first
+//    bit, as if a block started there; later passes re-decode a sub-stream
+//    from the exit state (bit, coefficient, block of the MCU) of its
+//    predecessor whenever that changed, a CTA repeating over its own
+//    sub-streams until they settle. Huffman codes fall back into step
+//    within a few codes, so the exits mostly settle in one or two passes;
+//    a segment's first sub-stream starts exactly, so the passes end by
+//    construction (at worst after one per sub-stream). The same launch
+//    then scans, over the sub-streams, the block counts and the DC
+//    differences of each scan component.
 //  * k_jpeg_write: each sub-stream decodes again from its exact entry and
 //    owns the blocks whose DC code lies inside it; it gathers each in
 //    shared memory and stores its quantised coefficients whole, with its
@@ -47,7 +49,6 @@
 #include <vector>
 
 #include "apriltag_fast.h"
-#include "at_kernels.h"
 #include "common/pjpeg.h"
 
 namespace {
