@@ -34,8 +34,11 @@
 //  * k_jpeg_idct: 8 lanes per block dequantise, run the IDCT (rows, then
 //    columns) and store the 8x8 pixels.
 #include <cuda_runtime.h>
-#include <emmintrin.h>
 #include <stdint.h>
+#if defined(__x86_64__) || defined(__i386__)
+#include <emmintrin.h>
+#define JSINK_STREAM 1
+#endif
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -858,12 +861,16 @@ struct JSink {
         const int64_t k = n - flushed;  // == sizeof buf
         if (flushed + k <= cap) {
             uint8_t *d = p + flushed;
+#ifdef JSINK_STREAM
             if (!((uintptr_t)d & 15)) {
                 for (int64_t o = 0; o < k; o += 16)
                     _mm_stream_si128((__m128i *)(d + o), _mm_load_si128((const __m128i *)(buf + o)));
             } else {
                 memcpy(d, buf, (size_t)k);
             }
+#else
+            memcpy(d, buf, (size_t)k);  // hosts without SSE2 streaming stores
+#endif
         } else {
             over = true;
         }
@@ -897,7 +904,9 @@ struct JSink {
             else over = true;
         }
         flushed = n;
+#ifdef JSINK_STREAM
         _mm_sfence();
+#endif
     }
 };
 

@@ -326,8 +326,8 @@ int at_jpeg_info(const uint8_t *buf, int64_t len, uint32_t flags, int32_t *width
 
 /* Decodes n JPEGs (bufs[i], lens[i] bytes, host memory) in one pass on the
    GPU into gray frames: frame i goes to dst[i], rows of strides[i] bytes,
-   width x height as at_jpeg_info gives; dst is device memory when
-   on_device is non-zero, host memory otherwise. flags: PJPEG_MJPEG.
+   width x height as at_jpeg_info gives; dst is device memory of the
+   decoder's GPU when on_device is non-zero, host memory otherwise. flags: PJPEG_MJPEG.
    errors[i] receives each image's PJPEG_ERR_* (0: written). Returns the
    number of images that failed, or -1 for a CUDA error (message on
    stderr). Returns when every frame is written. */
