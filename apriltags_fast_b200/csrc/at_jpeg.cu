@@ -136,6 +136,7 @@ struct JJob {
     uint32_t *excl;              // 4 per sub-stream: exclusive scans of cnt
     uint32_t *totals;            // 4 per CTA
     uint32_t *seg_stuck;         // per segment: its first sub-stream whose decode stops moving (~0: none)
+    uint32_t *seg_endbit;        // per segment: the bit where its last block ends (~0: not reached)
     unsigned int *bar;           // grid barrier: count, generation
     int *changed;                // per pass
     int *err;
@@ -573,7 +574,7 @@ struct JWriter {
     JReader R;
     const JScanDev *S;
     const JPlaneDev *P;   // plane of the block in progress (nullptr: not written)
-    uint32_t end, rel, nblk, mcu;
+    uint32_t seg, end, rel, nblk, mcu;
     int32_t pred0, pred1, pred2;  // DC predictors of the scan components
     bool last, own, done;
 };
@@ -586,6 +587,7 @@ __host__ __device__ __forceinline__ void jwriter_init(JWriter &w, const JJob &J,
     if (J.seg_stuck[seg] < i) return;  // dead: the segment's decode stopped before it
     const JScanDev &S = J.scans[G.scan];
     w.S = &S;
+    w.seg = seg;
     const unsigned long long in = i == G.sub0 ? jpack(G.start, 0, 0) : J.exitst[i - 1];
     w.last = i == G.sub0 + G.nsub - 1;
     w.end = min(G.end, G.start + (i - G.sub0 + 1) * J.sub_bits);
@@ -664,7 +666,9 @@ __host__ __device__ __forceinline__ void jwriter_run(JWriter &w, const JJob &J, 
                 }
             }
             s.z = 0;
-            w.rel++;
+            // where the segment's decode ends: the reference looks for the
+            // next restart marker from there
+            if (++w.rel == w.nblk) J.seg_endbit[w.seg] = s.p;
             if (++s.b == (int)S.bpm) {
                 s.b = 0;
                 w.mcu++;
@@ -1226,7 +1230,27 @@ struct HJob {
     uint32_t max_seg_subs = 0;
     uint32_t nblocks = 0;  // blocks of the planes written
     uint32_t sub_bits = 512, back_bits = 1024;
+    std::vector<int> scan_image;    // per scan: the index of its image in the call
+    std::vector<uint32_t> seg_end;  // per segment after the decode: the bit its last block ends at
 };
+
+// The reference's restart check (common/pjpeg.c:494-518): after a
+// segment's last block it reads on from the next byte boundary to the
+// first FF, which must begin the expected restart marker; a damaged
+// segment whose decode ends elsewhere fails there with PJPEG_ERR_RESET.
+// Returns, per image of the call, whether one of its segments fails.
+std::vector<char> restart_failures(const HJob &J, const uint8_t *stream, int nimages) {
+    std::vector<char> bad((size_t)nimages, 0);
+    for (size_t g = 0; g + 1 < J.segs.size(); g++) {
+        const JSegDev &G = J.segs[g];
+        if (J.segs[g + 1].scan != G.scan) continue;  // a scan's last segment ends at no marker
+        const uint32_t e = J.seg_end[g];
+        const uint64_t b0 = ((uint64_t)e + 7) / 8, m = G.end / 8;  // m: the marker's FF
+        const bool ok = e != 0xffffffffu && b0 <= m && !memchr(stream + b0, 0xff, (size_t)(m - b0));
+        if (!ok) bad[(size_t)J.scan_image[G.scan]] = 1;
+    }
+    return bad;
+}
 
 JTab make_tab(const HTab &t, std::vector<uint8_t> &pool) {
     JTab d;
@@ -1263,7 +1287,7 @@ JTab make_tab(const HTab &t, std::vector<uint8_t> &pool) {
 // components to write (bit c); place(c, P) fills the output of component
 // c (pointer, stride, clip) and returns its staging size (0: in place).
 template <class Place>
-void add_image(HJob &J, const HImage &im, int64_t s_base, uint32_t sub_bits, unsigned want, Place place) {
+void add_image(HJob &J, const HImage &im, int img, int64_t s_base, uint32_t sub_bits, unsigned want, Place place) {
     int plane_of[3] = {-1, -1, -1};
     for (int c = 0; c < im.ncomp; c++) {
         if (!(want & (1u << c)) || im.comp[c].scan < 0) continue;
@@ -1333,6 +1357,7 @@ void add_image(HJob &J, const HImage &im, int64_t s_base, uint32_t sub_bits, uns
         for (int i = sc.ns; i < 3; i++) D.plane[i] = -1;
         const uint32_t scan_id = (uint32_t)J.scans.size();
         J.scans.push_back(D);
+        J.scan_image.push_back(img);
         const uint32_t per = sc.restart ? sc.restart : (uint32_t)nmcu;
         for (size_t g = 0; g < sc.seg_start.size(); g++) {
             JSegDev G;
@@ -1485,6 +1510,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
     const size_t o_excl = put((size_t)nsub * 16);
     const size_t o_tot = put((size_t)grid * 16);
     const size_t o_stuck = put(J.segs.size() * 4);
+    const size_t o_endbit = put(J.segs.size() * 4);
     const size_t o_zero = off;  // zeroed: barrier, error, pass flags
     const size_t o_bar = put(8);
     const size_t o_err = put(4);
@@ -1500,7 +1526,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         if (!jcheck(cudaMalloc(&d->d_arena, off + off / 4), "cudaMalloc")) return -1;
         d->d_cap = off + off / 4;
     }
-    if (!grow_host(d, in_bytes + 64, J.stream_src ? 0 : (size_t)J.stream_n)) return -1;
+    if (!grow_host(d, in_bytes + 64 + J.segs.size() * 4, J.stream_src ? 0 : (size_t)J.stream_n)) return -1;
     uint8_t *D = d->d_arena, *H = d->h_stage;
     for (size_t p = 0; p < J.planes.size(); p++)
         if (J.plane_stage[p] != SIZE_MAX) J.planes[p].out = D + o_stage + J.plane_stage[p];
@@ -1518,6 +1544,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
     ok = ok && jcheck(cudaMemcpyAsync(D, H, in_bytes, cudaMemcpyHostToDevice, s), "copy in");
     ok = ok && jcheck(cudaMemsetAsync(D + o_zero, 0, zero_bytes, s), "memset");
     ok = ok && jcheck(cudaMemsetAsync(D + o_stuck, 0xff, J.segs.size() * 4, s), "memset");
+    ok = ok && jcheck(cudaMemsetAsync(D + o_endbit, 0xff, J.segs.size() * 4, s), "memset");
     ok = ok && jcheck(cudaEventRecord(d->ev[1], s), "event");
     if (ok && nsub) {
         JJob JJ;
@@ -1541,6 +1568,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         JJ.excl = (uint32_t *)(D + o_excl);
         JJ.totals = (uint32_t *)(D + o_tot);
         JJ.seg_stuck = (uint32_t *)(D + o_stuck);
+        JJ.seg_endbit = (uint32_t *)(D + o_endbit);
         JJ.back_bits = J.back_bits;
         JJ.bar = (unsigned int *)(D + o_bar);
         JJ.changed = (int *)(D + o_chg);
@@ -1564,6 +1592,8 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
         ok = ok && jcheck(cudaMemcpyAsync(hres + 2, D + o_chg + 4 * (size_t)(max_passes + 1), 4,
                                           cudaMemcpyDeviceToHost, s),
                           "copy out");
+        ok = ok && jcheck(cudaMemcpyAsync(hres + 16, D + o_endbit, J.segs.size() * 4, cudaMemcpyDeviceToHost, s),
+                          "copy out");
     } else if (ok) {
         ok = jcheck(cudaEventRecord(d->ev[2], s), "event");
         hres[0] = hres[1] = hres[2] = 0;
@@ -1585,6 +1615,7 @@ int run_job(at_jpeg *d, HJob &J, double parse_ms) {
     float ms;
     for (int k = 1; k < 5; k++)
         if (cudaEventElapsedTime(&ms, d->ev[k - 1], d->ev[k]) == cudaSuccess) d->stats[k] = ms;
+    J.seg_end.assign((const uint32_t *)(hres + 16), (const uint32_t *)(hres + 16) + J.segs.size());
     d->stats[6] = nsub ? hres[1] : 0;
     d->stats[8] = nsub ? hres[2] : 0;
     return 0;
@@ -1723,7 +1754,7 @@ static int decode_group(at_jpeg *dec, int32_t a, int32_t b, const uint8_t *const
             continue;
         }
         const HImage &im = ims[k];
-        add_image(J, im, base[k], J.sub_bits, 1u, [&](int, JPlaneDev &P) -> size_t {
+        add_image(J, im, k, base[k], J.sub_bits, 1u, [&](int, JPlaneDev &P) -> size_t {
             P.ow = im.w;
             P.oh = im.h;
             if (on_device) {
@@ -1737,6 +1768,12 @@ static int decode_group(at_jpeg *dec, int32_t a, int32_t b, const uint8_t *const
         });
     }
     if (run_job(dec, J, now_ms() - t0) != 0) return -1;
+    const std::vector<char> bad = restart_failures(J, dec->h_stage, m);
+    for (int k = 0; k < m; k++)
+        if (bad[k] && errors[a + k] == PJPEG_OKAY) {
+            errors[a + k] = PJPEG_ERR_RESET;  // its frame's pixels mean nothing
+            failed++;
+        }
     return failed;
 }
 
@@ -1836,7 +1873,7 @@ pjpeg_t *pjpeg_create_from_buffer(uint8_t *buf, int buflen, uint32_t flags, int 
     }
     J.sub_bits = jsub_for(sk.n);
     J.back_bits = std::max(512u, J.sub_bits);
-    add_image(J, im, 0, J.sub_bits, 7u, [&](int c, JPlaneDev &P) -> size_t {
+    add_image(J, im, 0, 0, J.sub_bits, 7u, [&](int c, JPlaneDev &P) -> size_t {
         const pjpeg_component_t &o = pj->components[c];
         P.ow = o.width;
         P.oh = o.height;
@@ -1846,14 +1883,16 @@ pjpeg_t *pjpeg_create_from_buffer(uint8_t *buf, int buflen, uint32_t flags, int 
         return (size_t)o.stride * o.height + 16;
     });
     int rc;
+    bool reset = false;
     {
         std::lock_guard<std::mutex> lk(g_pjpeg_mu);
         if (!g_pjpeg_dec) g_pjpeg_dec = at_jpeg_create();
         rc = g_pjpeg_dec ? run_job(g_pjpeg_dec, J, now_ms() - t0) : -1;
+        if (rc == 0) reset = restart_failures(J, g_pjpeg_dec->h_stage, 1)[0] != 0;
     }
-    if (rc != 0) {
+    if (rc != 0 || reset) {
         pjpeg_destroy(pj);
-        if (error) *error = PJPEG_ERR_FILE;
+        if (error) *error = rc != 0 ? PJPEG_ERR_FILE : PJPEG_ERR_RESET;
         return nullptr;
     }
     return pj;

@@ -131,3 +131,41 @@ def test_detect_on_a_decoded_jpeg(dec):
     got = [d.key() for d in det.detect(frames[0])]
     want = O.detect(host, [H.oracle_family("tag36h11")], [2], O.default_params(), order=O.ORDER_REF).dets
     assert got == want and len(got) >= 3
+
+
+def _flip_entropy(buf, rng, nflips):
+    """Random bytes of the entropy-coded data changed, none of them an FF,
+    next to an FF, or made into one (the markers stay where they were)."""
+    b = bytearray(buf)
+    sos = buf.find(b"\xff\xda")
+    lo = sos + 2 + (buf[sos + 2] << 8 | buf[sos + 3])
+    hi = len(buf) - 2
+    done = 0
+    while done < nflips:
+        i = int(rng.integers(lo + 1, hi - 1))
+        if 0xFF in (b[i - 1], b[i], b[i + 1]):
+            continue
+        v = int(rng.integers(0, 255))  # never 0xFF
+        if v == b[i]:
+            continue
+        b[i] = v
+        done += 1
+    return bytes(b)
+
+
+def test_damaged_entropy_data_equals_the_oracle(dec):
+    """Damaged scans decode as the oracle decodes them (codes that match
+    nothing, runs past the last coefficient, decodes that stop moving),
+    gray, 4:2:0 with restart markers, and 4:4:4, with no fault."""
+    rng = np.random.default_rng(42)
+    cfg = synth.Config(640, 480)
+    img = synth.make_frame(cfg, 9)[0]
+    rgb = np.stack([img, np.roll(img, 5, 0), 255 - img], -1)
+    bases = [O.jpeg_encode(img, 90), O.jpeg_encode(rgb, 80, (2, 2), 6), O.jpeg_encode(rgb, 95, (1, 1))]
+    cases = []
+    for k, base in enumerate(bases):
+        for n in (1, 3, 8, 40):
+            for rep in range(3):
+                cases.append((f"base{k} flips{n} #{rep}", _flip_entropy(base, rng, n), 0))
+    check_batch(dec, cases)
+    check_batch(dec, cases[::5], device=True, pad=3)
