@@ -83,3 +83,15 @@ def test_host_header_walk_matches_the_oracle():
             assert (iw, ih) == (w, h), name
         else:
             assert e in (RESET, MISSING_DHT, SOS, SOF), (name, e)  # found in or after the first scan
+
+
+def test_oracle_equals_reference_on_1080p_frames():
+    """Frames of the benchmark's size: gray and 4:2:0 with restart markers."""
+    need_ref()
+    from apriltags_fast_b200 import synth
+
+    cfg = synth.Config(1920, 1080, ntags=(24, 24), side=(30, 220), tilt_deg=60.0, noise=4.0, distractors=200)
+    img = synth.make_frame(cfg, 3)[0]
+    rgb = np.stack([img, np.roll(img, 4, 1), 255 - img], -1)
+    for buf in (O.jpeg_encode(img, 90), O.jpeg_encode(rgb, 85, (2, 2), 30, O.JPEG_OPTIMIZE)):
+        assert same(O.jpeg_decode(buf), O.ref_jpeg_decode(buf))
