@@ -95,3 +95,16 @@ def test_oracle_equals_reference_on_1080p_frames():
     rgb = np.stack([img, np.roll(img, 4, 1), 255 - img], -1)
     for buf in (O.jpeg_encode(img, 90), O.jpeg_encode(rgb, 85, (2, 2), 30, O.JPEG_OPTIMIZE)):
         assert same(O.jpeg_decode(buf), O.ref_jpeg_decode(buf))
+
+
+def test_decoder_fails_loudly_without_a_gpu():
+    """No CPU fallback: without a CUDA device the decoder cannot be made and
+    the pjpeg.h drop-in reports PJPEG_ERR_FILE instead of decoding."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    with pytest.raises(RuntimeError):
+        AT.JpegDecoder()
+    g = (np.arange(64 * 48) % 251).astype(np.uint8).reshape(48, 64)
+    assert AT.pjpeg_decode(O.jpeg_encode(g, 90))[0] == 1
