@@ -509,8 +509,12 @@ def main():
     import apriltags_fast_b200 as AT
 
     pool = make_pool(rank)
-    if args.jpeg_only:
-        print(json.dumps({"jpeg": jpeg_bench(pool, args.batch, args.steps, args.warmup, not args.no_cpu_baseline)}))
+    if args.jpeg_only:  # rank 0 alone (frames are independent: nothing to combine)
+        if rank == 0:
+            print(json.dumps({"jpeg": jpeg_bench(pool, args.batch, args.steps, args.warmup,
+                                                 not args.no_cpu_baseline)}))
+        if dist:
+            dist.destroy_process_group()
         return
     dev = [torch.from_numpy(f).cuda() for f in pool]
     pinned = [torch.from_numpy(f).pin_memory() for f in pool]
